@@ -1,0 +1,254 @@
+"""cugmres_b200 -- B200-native GMRES for A = I - G diag(c) on an N x N grid.
+
+G is the symmetric block-Toeplitz-Toeplitz-block Green's-function matrix of
+the 2D Helmholtz Lippmann-Schwinger (GFIEM) equation and c = k0^2 chi the
+scaled contrast.  The solver is hand-written sm_100a CUDA behind the C-ABI in
+include/cugmres.h (libcugmres.so); this module is the Python front-end:
+
+* ``Solver`` -- a context with an operator, ``matvec``, ``residual``, ``solve``.
+* PyGMRES-compatible helpers with the signatures of the reference's NumPy
+  module (PyGMRES/GMRES.py:13-69): ``get_plane_wave``, ``get_green_matrix``, ``get_toeplitz_mat``, ``get_eps_from_mask``,
+  ``matvec`` -- the operator application runs on the GPU.
+* ``fast_gmres`` -- the reference's Fast_GMRES_with_CUDA semantics
+  (CUDA_GMRES/GMRES.cuh:22-35) in complex64.
+
+Inputs may be NumPy arrays (host) or contiguous torch tensors (host or CUDA);
+the C library detects device pointers itself.  There is no CPU fallback: a
+missing library or a failing CUDA call raises.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import CugmresError, check
+from .problems import green_block, helmholtz, reference_cylinder
+
+__all__ = ["Solver", "CugmresError", "green_block", "helmholtz", "reference_cylinder", "matvec",
+           "get_plane_wave", "get_green_matrix", "get_toeplitz_mat", "get_eps_from_mask",
+           "fast_gmres", "gmres"]
+
+_PREC = {"fp64": _lib.CG_PREC_FP64, "mixed": _lib.CG_PREC_MIXED, "fp32": _lib.CG_PREC_MIXED}
+_GIV = {"unitary": _lib.CG_GIVENS_UNITARY, "reference": _lib.CG_GIVENS_REFERENCE}
+
+
+def _is_torch(a):
+    return type(a).__module__.split(".")[0] == "torch"
+
+
+def _np_dtype_name(dt):
+    return {np.complex128: "complex128", np.complex64: "complex64", np.float64: "float64",
+            np.float32: "float32", np.uint8: "uint8"}[dt]
+
+
+def _arg(a, dtype, copy=False):
+    """(c_void_p, keepalive) for a NumPy array or a contiguous torch tensor."""
+    if _is_torch(a):
+        name = _np_dtype_name(dtype)
+        if str(a.dtype) != "torch." + name:
+            raise TypeError(f"expected torch.{name}, got {a.dtype}")
+        if not a.is_contiguous():
+            raise TypeError("tensor must be contiguous")
+        return ctypes.c_void_p(a.data_ptr()), a
+    arr = np.array(a, dtype=dtype, order="C", copy=True) if copy else np.ascontiguousarray(a, dtype=dtype)
+    return arr.ctypes.data_as(ctypes.c_void_p), arr
+
+
+class Solver:
+    """One solver context (device workspace + CUDA stream) on ``device``."""
+
+    def __init__(self, device=0):
+        self._ctx = ctypes.c_void_p()
+        check(_lib.lib().cugmres_create(ctypes.byref(self._ctx), int(device)), "cugmres_create")
+        self.N = None
+        self.L = None
+
+    def close(self):
+        if self._ctx:
+            _lib.lib().cugmres_destroy(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _grid(self):
+        N, L = ctypes.c_int(0), ctypes.c_int(0)
+        check(_lib.lib().cugmres_grid_size(self._ctx, ctypes.byref(N), ctypes.byref(L)), "grid_size")
+        self.N, self.L = N.value, L.value
+
+    def set_stream(self, stream):
+        """Run on a caller's cudaStream_t (an int handle, e.g. torch's stream.cuda_stream)."""
+        check(_lib.lib().cugmres_set_stream(self._ctx, ctypes.c_void_p(int(stream))), "set_stream")
+
+    def synchronize(self):
+        check(_lib.lib().cugmres_synchronize(self._ctx), "synchronize")
+
+    def set_operator(self, g_block, chi, chi_scale=1.0):
+        """A = I - G diag(chi_scale * chi); g_block[d1, d2] is G at offset (d1, d2)."""
+        N = int(g_block.shape[0])
+        gp, gk = _arg(g_block, np.complex128)
+        cp, ck = _arg(chi, np.float64)
+        check(_lib.lib().cugmres_set_operator(self._ctx, N, gp, cp, float(chi_scale)), "set_operator")
+        self._grid()
+        return self
+
+    def set_operator_circulant(self, g_prep, chi, chi_scale=1.0):
+        """Operator from the reference's spatial (2N-1)^2 circulant (G_prep layout)."""
+        M = int(g_prep.shape[0])
+        N = (M + 1) // 2
+        gp, gk = _arg(g_prep, np.complex64)
+        cp, ck = _arg(chi, np.float64)
+        check(_lib.lib().cugmres_set_operator_circulant(self._ctx, N, gp, cp, float(chi_scale)),
+              "set_operator_circulant")
+        self._grid()
+        return self
+
+    def matvec(self, x, precision="fp64", out=None):
+        """y = A x; precision 'fp64' (complex128) or 'fp32' (complex64)."""
+        prec = _PREC[precision]
+        dt = np.complex128 if prec == _lib.CG_PREC_FP64 else np.complex64
+        xp, xk = _arg(x, dt)
+        if out is None:
+            out = np.empty((self.N, self.N), dt) if not _is_torch(x) else x.new_empty(x.shape)
+        yp, yk = _arg(out, dt)
+        check(_lib.lib().cugmres_matvec(self._ctx, xp, yp, prec), "matvec")
+        return yk
+
+    def residual(self, b, x):
+        """(r, ||r|| / ||b||) with r = b - A x in FP64."""
+        bp, bk = _arg(b, np.complex128)
+        xp, xk = _arg(x, np.complex128)
+        r = np.empty((self.N, self.N), np.complex128)
+        rel = ctypes.c_double(0.0)
+        check(_lib.lib().cugmres_residual(self._ctx, bp, xp, r.ctypes.data_as(ctypes.c_void_p),
+                                          ctypes.byref(rel)), "residual")
+        return r, rel.value
+
+    def solve(self, b, x0=None, restart=100, max_iter=10000, tol=1e-10, precision="fp64", givens="unitary",
+              inner_tol=1e-5, fixed_iterations=False, timeout_s=0.0, raise_on_failure=False):
+        """Solve A x = b.  Returns (x, info) where info holds status, iterations,
+        cycles, rel_residual_true / _estimate, seconds and res_hist."""
+        o = _lib.CgOpts()
+        _lib.lib().cugmres_default_opts(ctypes.byref(o))
+        o.restart = int(restart)
+        o.max_iter = int(max_iter)
+        o.tol = float(tol)
+        o.precision = _PREC[precision]
+        o.givens = _GIV[givens]
+        o.inner_tol = float(inner_tol)
+        o.fixed_iterations = int(bool(fixed_iterations))
+        o.timeout_s = float(timeout_s)
+        bp, bk = _arg(b, np.complex128)
+        if x0 is None:
+            o.zero_x0 = 1
+            x = np.zeros((self.N, self.N), np.complex128) if not _is_torch(b) else b.new_zeros(b.shape)
+        else:
+            x = x0 if _is_torch(x0) else np.array(x0, dtype=np.complex128, order="C", copy=True)
+        xp, xk = _arg(x, np.complex128)
+        hist = np.zeros(int(max_iter) + 1, np.float64)
+        res = _lib.CgResult()
+        st = _lib.lib().cugmres_solve(self._ctx, bp, xp, ctypes.byref(o), hist.ctypes.data_as(ctypes.c_void_p),
+                                      len(hist), ctypes.byref(res))
+        if st in (_lib.CG_ERR_INVALID, _lib.CG_ERR_CUDA, _lib.CG_ERR_OOM, _lib.CG_ERR_NO_OPERATOR,
+                  _lib.CG_ERR_NOT_IMPLEMENTED) or (raise_on_failure and st != _lib.CG_OK):
+            raise CugmresError(st, "cugmres_solve")
+        info = dict(status=st, status_text=_lib.strerror(st), iterations=res.iterations, cycles=res.cycles,
+                    rel_residual_estimate=res.rel_residual_estimate, rel_residual_true=res.rel_residual_true,
+                    seconds=res.seconds, res_hist=hist[: res.iterations + 1].copy())
+        return xk, info
+
+
+def gmres(g_block, chi, b, chi_scale=1.0, device=0, **kw):
+    """One-shot solve: builds a Solver, sets the operator and solves."""
+    with Solver(device) as s:
+        s.set_operator(g_block, chi, chi_scale)
+        return s.solve(b, **kw)
+
+
+# ---------------------------------------------------------------- PyGMRES API
+def get_plane_wave(k, size):
+    """exp(-i k col) on a size x size grid (PyGMRES/GMRES.py:13-18, angle 0)."""
+    y, x = np.mgrid[:size, :size]
+    return np.exp(-1j * k * x)
+
+
+def get_green_matrix(k, size):
+    """g[j_row, i_col] = (i/4) H0(k sqrt((i - 1/2)^2 + j^2)) (PyGMRES/GMRES.py:23-27)."""
+    return green_block("pygmres", size, k)
+
+
+def get_toeplitz_mat(ij_block):
+    """Even (2N-1)^2 circulant of an N x N block (PyGMRES/GMRES.py:64-69)."""
+    b = np.asarray(ij_block)
+    t1 = np.hstack((b, b[:, :0:-1]))
+    t2 = np.hstack((b[:0:-1, :], b[:0:-1, :0:-1]))
+    return np.vstack((t1, t2))
+
+
+def get_eps_from_mask(e, mask):
+    """(e - 1) * mask as an (N^2, 1) column (PyGMRES/GMRES.py:60-61)."""
+    return (e - 1) * np.asarray(mask).reshape((-1, 1))
+
+
+_mv_cache = {}
+
+
+def matvec(x, eps, k, qweq=False, transpose=False, g=None, device=0):
+    """x - G (k^2 eps x) on the GPU, the reference's matvec(x, eps, k)
+    (PyGMRES/GMRES.py:47-57).  x: N^2 vector, eps: N^2 real column, k: wavenumber,
+    g: optional (2N-1)^2 circulant (as get_toeplitz_mat returns).  Returns an
+    (N^2, 1) complex128 column.  ``qweq`` returns (G_block, G) as the reference.
+    ``transpose`` (x - chi G x) is not provided by this build."""
+    x = np.asarray(x).reshape(-1)
+    n = x.size
+    N = int(round(np.sqrt(n)))
+    if N * N != n:
+        raise ValueError("x must hold N^2 entries")
+    if g is None:
+        block = get_green_matrix(k, N)
+    else:
+        block = np.asarray(g)[:N, :N]
+    if qweq:
+        return block, (get_toeplitz_mat(block) if g is None else g)
+    if transpose:
+        raise NotImplementedError("transpose=True (x - chi G x) is not part of this build")
+    chi = np.asarray(eps, dtype=np.float64).reshape(N, N)
+    key = (device, N)
+    s = _mv_cache.get(key)
+    if s is None:
+        s = Solver(device)
+        _mv_cache[key] = s
+    s.set_operator(block, chi, float(k) ** 2)
+    return s.matvec(x.reshape(N, N).astype(np.complex128)).reshape(-1, 1)
+
+
+def fast_gmres(g_prep, mask, solution, maxiter, tolerance, chi_value, rhs=None, precision="fp64"):
+    """The reference's Fast_GMRES_with_CUDA semantics (CUDA_GMRES/GMRES.cuh:22-446)
+    through cugmres_fast_gmres.  Returns (solution complex64 N x N,
+    actual_residual[maxiter+1] float32, GMRES_n, res_vs_tol)."""
+    g_prep = np.ascontiguousarray(g_prep, np.complex64)
+    N = (g_prep.shape[0] + 1) // 2
+    m = np.ascontiguousarray(np.asarray(mask).reshape(N, N), np.uint8)
+    sol = np.array(solution, dtype=np.complex64, order="C", copy=True).reshape(N, N)
+    res = np.zeros(int(maxiter) + 1, np.float32)
+    n = ctypes.c_uint(0)
+    flag = ctypes.c_int(0)
+    rp = None
+    if rhs is not None:
+        rhs = np.ascontiguousarray(rhs, np.complex64)
+        rp = rhs.ctypes.data_as(ctypes.c_void_p)
+    check(_lib.lib().cugmres_fast_gmres(
+        g_prep.ctypes.data_as(ctypes.c_void_p), m.ctypes.data_as(ctypes.c_void_p),
+        sol.ctypes.data_as(ctypes.c_void_p), res.ctypes.data_as(ctypes.c_void_p), ctypes.byref(n),
+        ctypes.c_float(tolerance), ctypes.byref(flag), ctypes.c_uint(int(maxiter)), ctypes.c_uint(N),
+        ctypes.c_float(chi_value), rp, _PREC[precision]), "cugmres_fast_gmres")
+    return sol, res, n.value, bool(flag.value)

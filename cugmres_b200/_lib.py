@@ -1,0 +1,122 @@
+"""ctypes bindings of include/cugmres.h (libcugmres.so, built in-tree).
+
+The library is loaded from cugmres_b200/lib/libcugmres.so.  There is no CPU
+fallback: if the library is missing or cannot be loaded, every call raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libcugmres.so")
+
+CG_OK = 0
+CG_ERR_INVALID = 1
+CG_ERR_CUDA = 2
+CG_ERR_NOT_CONVERGED = 3
+CG_ERR_BREAKDOWN = 4
+CG_ERR_NONFINITE = 5
+CG_ERR_TIMEOUT = 6
+CG_ERR_NOT_IMPLEMENTED = 7
+CG_ERR_NO_OPERATOR = 8
+CG_ERR_OOM = 9
+
+CG_PREC_FP64 = 0
+CG_PREC_MIXED = 1
+CG_GIVENS_UNITARY = 0
+CG_GIVENS_REFERENCE = 1
+CG_GREEN_HELMHOLTZ = 0
+CG_GREEN_REFERENCE = 1
+CG_GREEN_PYGMRES = 2
+
+# Every symbol include/cugmres.h declares.
+EXPORTS = (
+    "cugmres_strerror", "cugmres_version", "cugmres_default_opts", "cugmres_create", "cugmres_destroy",
+    "cugmres_set_stream", "cugmres_synchronize", "cugmres_green_block", "cugmres_set_operator",
+    "cugmres_set_operator_circulant", "cugmres_grid_size", "cugmres_matvec", "cugmres_residual",
+    "cugmres_solve", "cugmres_fast_gmres",
+)
+
+
+class CgOpts(ctypes.Structure):
+    _fields_ = [
+        ("restart", ctypes.c_int),
+        ("max_iter", ctypes.c_int),
+        ("tol", ctypes.c_double),
+        ("precision", ctypes.c_int),
+        ("givens", ctypes.c_int),
+        ("inner_tol", ctypes.c_double),
+        ("zero_x0", ctypes.c_int),
+        ("fixed_iterations", ctypes.c_int),
+        ("timeout_s", ctypes.c_double),
+        ("reserved", ctypes.c_int * 8),
+    ]
+
+
+class CgResult(ctypes.Structure):
+    _fields_ = [
+        ("status", ctypes.c_int),
+        ("iterations", ctypes.c_int),
+        ("cycles", ctypes.c_int),
+        ("rel_residual_estimate", ctypes.c_double),
+        ("rel_residual_true", ctypes.c_double),
+        ("seconds", ctypes.c_double),
+    ]
+
+
+class CugmresError(RuntimeError):
+    def __init__(self, status, what=""):
+        self.status = status
+        msg = strerror(status)
+        super().__init__(f"{what}: {msg} (status {status})" if what else f"{msg} (status {status})")
+
+
+_lib = None
+
+
+def lib():
+    """Loads libcugmres.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m cugmres_b200.build`")
+        L = ctypes.CDLL(LIB_PATH)
+        _declare(L)
+        _lib = L
+    return _lib
+
+
+def _declare(L):
+    P, I, D, F, U = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.c_float, ctypes.c_uint
+    L.cugmres_strerror.argtypes = [I]
+    L.cugmres_strerror.restype = ctypes.c_char_p
+    L.cugmres_version.restype = I
+    L.cugmres_default_opts.argtypes = [ctypes.POINTER(CgOpts)]
+    L.cugmres_default_opts.restype = None
+    L.cugmres_create.argtypes = [ctypes.POINTER(P), I]
+    L.cugmres_destroy.argtypes = [P]
+    L.cugmres_set_stream.argtypes = [P, P]
+    L.cugmres_synchronize.argtypes = [P]
+    L.cugmres_green_block.argtypes = [I, I, D, D, P]
+    L.cugmres_set_operator.argtypes = [P, I, P, P, D]
+    L.cugmres_set_operator_circulant.argtypes = [P, I, P, P, D]
+    L.cugmres_grid_size.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(I)]
+    L.cugmres_matvec.argtypes = [P, P, P, I]
+    L.cugmres_residual.argtypes = [P, P, P, P, ctypes.POINTER(D)]
+    L.cugmres_solve.argtypes = [P, P, P, ctypes.POINTER(CgOpts), P, I, ctypes.POINTER(CgResult)]
+    L.cugmres_fast_gmres.argtypes = [P, P, P, P, ctypes.POINTER(U), F, ctypes.POINTER(I), U, U, F, P, I]
+    for name in EXPORTS:
+        if name not in ("cugmres_strerror", "cugmres_default_opts"):
+            getattr(L, name).restype = I
+
+
+def strerror(status):
+    try:
+        return lib().cugmres_strerror(int(status)).decode()
+    except Exception:
+        return "unknown"
+
+
+def check(status, what=""):
+    if status != CG_OK:
+        raise CugmresError(status, what)
+    return status

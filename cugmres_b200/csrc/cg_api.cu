@@ -1,0 +1,707 @@
+// C-ABI of cugmres_b200: context, operator setup, matvec and the GMRES driver.
+//
+// The driver replaces Fast_GMRES_with_CUDA (CUDA_GMRES/GMRES.cuh:22-446).
+// Differences by design:
+//   * all solver state lives on the device (DevState); the host enqueues a
+//     whole restart cycle and synchronises once per cycle to read the status,
+//     instead of a cudaDeviceSynchronize after every kernel and two host
+//     round trips per Arnoldi step (GMRES.cuh:369-371);
+//   * restart, a relative tolerance and early exit are supported; the
+//     reference's semantics (one cycle of exactly maxiter steps, absolute
+//     tolerance gating the first step) are the fixed_iterations mode;
+//   * errors are returned as status codes instead of exit() (GMRES_kernels.cuh:21-94);
+//   * workspace is owned by the context and reused across solves instead of a
+//     cudaMalloc/cudaFree per call (GMRES.cuh:74-76,443-444).
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/cugmres.h"
+#include "cg_common.cuh"
+#include "cg_internal.h"
+
+using namespace cg;
+
+struct cg_ctx {
+    int device = 0;
+    int sms = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // operator
+    bool have_op = false;
+    int N = 0, L = 0;
+    double2 *gq64 = nullptr;
+    float2 *gq32 = nullptr;
+    double *c64 = nullptr;
+    float *c32 = nullptr;
+    double2 *tw64 = nullptr;
+    float2 *tw32 = nullptr;
+    void *T = nullptr;  // N x L complex128 intermediate (also used as complex64)
+    // Krylov workspace
+    int mcap = 0;
+    int itcap = 0;
+    size_t vcap_bytes = 0;
+    void *V = nullptr;
+    DevState *st = nullptr;
+    DevState *st_host = nullptr;  // pinned mirror for status reads
+    KrylovPtrs kp{};
+    double2 *bbuf = nullptr;  // staging of host b
+    double2 *xbuf = nullptr;  // staging of host x
+    double2 *rbuf = nullptr;  // FP64 vector scratch (residual, matvec staging)
+    int nparts_cap = 0;
+    cudaEvent_t ev = nullptr;
+};
+
+namespace {
+
+int cuerr(cudaError_t e) { return e == cudaSuccess ? CG_OK : (e == cudaErrorMemoryAllocation ? CG_ERR_OOM : CG_ERR_CUDA); }
+
+#define CG_TRY(expr)                  \
+    do {                              \
+        int _s = (expr);              \
+        if (_s != CG_OK) return _s;   \
+    } while (0)
+#define CG_CU(expr) CG_TRY(cuerr(expr))
+#define CG_LAUNCH(expr)                                  \
+    do {                                                 \
+        int _e = (expr);                                 \
+        if (_e != 0) return CG_ERR_CUDA;                 \
+    } while (0)
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    cudaError_t e = cudaPointerGetAttributes(&a, p);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+void dfree(void *&p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+template <typename T> void dfree_t(T *&p) {
+    void *q = (void *)p;
+    dfree(q);
+    p = nullptr;
+}
+
+int next_embedding(int N) {
+    int L = 16;
+    while (L < 2 * N - 1) L *= 2;
+    return L;
+}
+
+double now_s() {
+    timespec t;
+    clock_gettime(CLOCK_MONOTONIC, &t);
+    return (double)t.tv_sec + 1e-9 * (double)t.tv_nsec;
+}
+
+// ------------------------------------------------------------ setup kernels
+__global__ void k_embed(const double2 *__restrict__ g, double2 *__restrict__ full, int N, int L) {
+    const long long tot = (long long)L * L;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e / L), j = (int)(e % L);
+        const int di = i <= L - i ? i : L - i;
+        const int dj = j <= L - j ? j : L - j;
+        full[e] = (di < N && dj < N) ? g[(size_t)di * N + dj] : make_double2(0.0, 0.0);
+    }
+}
+
+__global__ void k_quarter(const double2 *__restrict__ full, double2 *__restrict__ q64, float2 *__restrict__ q32, int L,
+                          double scale) {
+    const int Lq = L / 2 + 1;
+    const long long tot = (long long)Lq * Lq;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        const int r = (int)(e / Lq), c = (int)(e % Lq);
+        const double2 v = full[(size_t)r * L + c];
+        q64[e] = make_double2(v.x * scale, v.y * scale);
+        q32[e] = make_float2((float)(v.x * scale), (float)(v.y * scale));
+    }
+}
+
+__global__ void k_scale_real(const double *__restrict__ a, double s, double *__restrict__ o64, float *__restrict__ o32,
+                             long long n) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+        const double v = a[e] * s;
+        o64[e] = v;
+        o32[e] = (float)v;
+    }
+}
+
+__global__ void k_copy_c64_to_c128(const float2 *__restrict__ a, double2 *__restrict__ b, int rows, int cols, int lda) {
+    const long long tot = (long long)rows * cols;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(e / cols), j = (int)(e % cols);
+        const float2 v = a[(size_t)i * lda + j];
+        b[e] = make_double2(v.x, v.y);
+    }
+}
+
+int grid_for(long long n, int cap) {
+    long long g = (n + 255) / 256;
+    if (g > cap) g = cap;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+void free_operator(cg_ctx *c) {
+    dfree_t(c->gq64);
+    dfree_t(c->gq32);
+    dfree_t(c->c64);
+    dfree_t(c->c32);
+    dfree_t(c->tw64);
+    dfree_t(c->tw32);
+    dfree(c->T);
+    dfree_t(c->bbuf);
+    dfree_t(c->xbuf);
+    dfree_t(c->rbuf);
+    c->have_op = false;
+}
+
+void free_krylov(cg_ctx *c) {
+    dfree(c->V);
+    dfree_t(c->kp.scale);
+    dfree_t(c->kp.h1);
+    dfree_t(c->kp.h2);
+    dfree_t(c->kp.Rm);
+    dfree_t(c->kp.cs);
+    dfree_t(c->kp.sn);
+    dfree_t(c->kp.g);
+    dfree_t(c->kp.y);
+    dfree_t(c->kp.hist);
+    dfree_t(c->kp.part);
+    dfree_t(c->kp.npart);
+    c->mcap = 0;
+    c->itcap = 0;
+    c->vcap_bytes = 0;
+    c->nparts_cap = 0;
+}
+
+int dot_blocks(const cg_ctx *c) { return 2 * c->sms; }
+int axpy_blocks(const cg_ctx *c, long long n) { return grid_for(n, 4 * c->sms); }
+
+// Ensures basis and small-array capacity for restart m and budget maxit.
+int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
+    const long long n = (long long)c->N * c->N;
+    const size_t vbytes = (size_t)(m + 2) * (size_t)n * elem_bytes;
+    const int nparts = std::max(std::max(axpy_blocks(c, n), dot_blocks(c)), std::max(c->N, 4 * c->sms));
+    if (m > c->mcap || maxit > c->itcap || vbytes > c->vcap_bytes || nparts > c->nparts_cap) {
+        const int mc = std::max(m, c->mcap), ic = std::max(maxit, c->itcap);
+        const size_t vb = std::max(vbytes, c->vcap_bytes);
+        const int np = std::max(nparts, c->nparts_cap);
+        free_krylov(c);
+        CG_CU(cudaMalloc(&c->V, vb));
+        CG_CU(cudaMalloc((void **)&c->kp.scale, sizeof(double) * (mc + 2)));
+        CG_CU(cudaMalloc((void **)&c->kp.h1, sizeof(double2) * (mc + 1)));
+        CG_CU(cudaMalloc((void **)&c->kp.h2, sizeof(double2) * (mc + 1)));
+        CG_CU(cudaMalloc((void **)&c->kp.Rm, sizeof(double2) * (size_t)(mc + 1) * mc));
+        CG_CU(cudaMalloc((void **)&c->kp.cs, sizeof(double2) * mc));
+        CG_CU(cudaMalloc((void **)&c->kp.sn, sizeof(double) * mc));
+        CG_CU(cudaMalloc((void **)&c->kp.g, sizeof(double2) * (mc + 1)));
+        CG_CU(cudaMalloc((void **)&c->kp.y, sizeof(double2) * mc));
+        CG_CU(cudaMalloc((void **)&c->kp.hist, sizeof(double) * (ic + 1)));
+        CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * 2 * (size_t)dot_blocks(c) * (mc + 1)));
+        CG_CU(cudaMalloc((void **)&c->kp.npart, sizeof(double) * np));
+        c->mcap = mc;
+        c->itcap = ic;
+        c->vcap_bytes = vb;
+        c->nparts_cap = np;
+    }
+    c->kp.st = c->st;
+    c->kp.mcap = c->mcap;
+    return CG_OK;
+}
+
+MatvecArgs margs(const cg_ctx *c, int prec) {
+    MatvecArgs a;
+    a.N = c->N;
+    a.L = c->L;
+    a.gq = prec == 0 ? (const void *)c->gq64 : (const void *)c->gq32;
+    a.cdiag = prec == 0 ? (const void *)c->c64 : (const void *)c->c32;
+    a.tw = prec == 0 ? (const void *)c->tw64 : (const void *)c->tw32;
+    a.T = c->T;
+    return a;
+}
+
+VecSel fixed_vec(const void *p) {
+    VecSel v;
+    v.base = const_cast<void *>(p);
+    v.stride = 0;
+    v.koff = 0;
+    return v;
+}
+
+int row_blocks(const cg_ctx *c) {
+    const int rpc = rows_per_block(0, c->L);
+    return (c->N + rpc - 1) / rpc;
+}
+
+// y = A x (mode 0) or y = b - A x (mode 1) on explicit vectors, no gating.
+int apply_explicit(cg_ctx *c, int prec, int mode, int out_prec, const void *x, const void *b, void *y, double *npart) {
+    MatvecArgs a = margs(c, prec);
+    CG_LAUNCH(launch_rows_forward(prec, a, fixed_vec(x), nullptr, nullptr, GATE_NONE, c->stream));
+    CG_LAUNCH(launch_cols_convolve(prec, a, nullptr, GATE_NONE, c->stream));
+    CG_LAUNCH(launch_rows_inverse(prec, mode, out_prec, a, fixed_vec(x), nullptr, b, fixed_vec(y), npart, nullptr,
+                                  GATE_NONE, c->stream));
+    return CG_OK;
+}
+
+bool all_finite(const double *p, size_t n) {
+    for (size_t i = 0; i < n; i++)
+        if (!isfinite(p[i])) return false;
+    return true;
+}
+
+}  // namespace
+
+// ================================================================== C-ABI
+extern "C" {
+
+const char *cugmres_strerror(int s) {
+    switch (s) {
+        case CG_OK: return "ok";
+        case CG_ERR_INVALID: return "invalid argument";
+        case CG_ERR_CUDA: return "CUDA runtime error";
+        case CG_ERR_NOT_CONVERGED: return "not converged within the iteration budget";
+        case CG_ERR_BREAKDOWN: return "Arnoldi breakdown without convergence";
+        case CG_ERR_NONFINITE: return "non-finite value in input or iteration";
+        case CG_ERR_TIMEOUT: return "timeout";
+        case CG_ERR_NOT_IMPLEMENTED: return "not implemented for these sizes/options";
+        case CG_ERR_NO_OPERATOR: return "operator not set";
+        case CG_ERR_OOM: return "device out of memory";
+        default: return "unknown status";
+    }
+}
+
+int cugmres_version(void) { return 100; }
+
+void cugmres_default_opts(cg_opts *o) {
+    if (!o) return;
+    memset(o, 0, sizeof(*o));
+    o->restart = 100;
+    o->max_iter = 10000;
+    o->tol = 1e-10;
+    o->precision = CG_PREC_FP64;
+    o->givens = CG_GIVENS_UNITARY;
+    o->inner_tol = 1e-5;
+    o->zero_x0 = 0;
+    o->fixed_iterations = 0;
+    o->timeout_s = 0.0;
+}
+
+int cugmres_create(cg_ctx **out, int device) {
+    if (!out) return CG_ERR_INVALID;
+    *out = nullptr;
+    int ndev = 0;
+    CG_CU(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return CG_ERR_INVALID;
+    CG_CU(cudaSetDevice(device));
+    cg_ctx *c = new cg_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return CG_ERR_CUDA;
+    }
+    c->own_stream = true;
+    if (cudaMalloc((void **)&c->st, sizeof(DevState)) != cudaSuccess ||
+        cudaMallocHost((void **)&c->st_host, sizeof(DevState)) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev, cudaEventDisableTiming) != cudaSuccess) {
+        cugmres_destroy(c);
+        return CG_ERR_CUDA;
+    }
+    cudaMemset(c->st, 0, sizeof(DevState));
+    *out = c;
+    return CG_OK;
+}
+
+int cugmres_destroy(cg_ctx *c) {
+    if (!c) return CG_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    free_operator(c);
+    free_krylov(c);
+    dfree_t(c->st);
+    if (c->st_host) cudaFreeHost(c->st_host);
+    if (c->ev) cudaEventDestroy(c->ev);
+    if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return CG_OK;
+}
+
+int cugmres_set_stream(cg_ctx *c, void *stream) {
+    if (!c) return CG_ERR_INVALID;
+    cudaSetDevice(c->device);
+    if (c->own_stream && c->stream) {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamDestroy(c->stream);
+    }
+    c->stream = (cudaStream_t)stream;
+    c->own_stream = false;
+    return CG_OK;
+}
+
+int cugmres_synchronize(cg_ctx *c) {
+    if (!c) return CG_ERR_INVALID;
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+int cugmres_grid_size(const cg_ctx *c, int *N, int *L) {
+    if (!c || !c->have_op) return CG_ERR_NO_OPERATOR;
+    if (N) *N = c->N;
+    if (L) *L = c->L;
+    return CG_OK;
+}
+
+static int set_operator_dev(cg_ctx *c, int N, const double2 *g_dev, const double *chi_dev, double chi_scale) {
+    const int L = c->L;
+    const long long n = (long long)N * N;
+    // spectrum: even embedding, full FP64 2D transform, quarter with 1/L^2 folded in
+    double2 *full = nullptr;
+    CG_CU(cudaMalloc((void **)&full, sizeof(double2) * (size_t)L * L));
+    k_embed<<<grid_for((long long)L * L, 8 * c->sms), 256, 0, c->stream>>>(g_dev, full, N, L);
+    int e = launch_fft2d_full_fp64(L, full, c->tw64, c->stream);
+    if (e == 0) {
+        k_quarter<<<grid_for((long long)(L / 2 + 1) * (L / 2 + 1), 8 * c->sms), 256, 0, c->stream>>>(
+            full, c->gq64, c->gq32, L, 1.0 / ((double)L * (double)L));
+        k_scale_real<<<grid_for(n, 8 * c->sms), 256, 0, c->stream>>>(chi_dev, chi_scale, c->c64, c->c32, n);
+    }
+    cudaError_t ce = cudaStreamSynchronize(c->stream);
+    cudaFree(full);
+    if (e != 0) return CG_ERR_CUDA;
+    return cuerr(ce);
+}
+
+int cugmres_set_operator(cg_ctx *c, int N, const cg_c128 *g_block, const double *chi, double chi_scale) {
+    if (!c || !g_block || !chi || N < 1 || !isfinite(chi_scale)) return CG_ERR_INVALID;
+    const int L = next_embedding(N);
+    if (!fft_supported(L)) return CG_ERR_NOT_IMPLEMENTED;
+    CG_CU(cudaSetDevice(c->device));
+    const long long n = (long long)N * N;
+    const bool g_dev = is_device_ptr(g_block), chi_dev = is_device_ptr(chi);
+    if (!g_dev && !all_finite((const double *)g_block, 2 * (size_t)n)) return CG_ERR_NONFINITE;
+    if (!chi_dev && !all_finite(chi, (size_t)n)) return CG_ERR_NONFINITE;
+    free_operator(c);
+    free_krylov(c);
+    c->N = N;
+    c->L = L;
+    const int Lq = L / 2 + 1;
+    CG_CU(cudaMalloc((void **)&c->gq64, sizeof(double2) * (size_t)Lq * Lq));
+    CG_CU(cudaMalloc((void **)&c->gq32, sizeof(float2) * (size_t)Lq * Lq));
+    CG_CU(cudaMalloc((void **)&c->c64, sizeof(double) * n));
+    CG_CU(cudaMalloc((void **)&c->c32, sizeof(float) * n));
+    CG_CU(cudaMalloc((void **)&c->tw64, sizeof(double2) * 2 * L));
+    CG_CU(cudaMalloc((void **)&c->tw32, sizeof(float2) * 2 * L));
+    CG_CU(cudaMalloc(&c->T, sizeof(double2) * (size_t)N * L));
+    CG_CU(cudaMalloc((void **)&c->bbuf, sizeof(double2) * n));
+    CG_CU(cudaMalloc((void **)&c->xbuf, sizeof(double2) * n));
+    CG_CU(cudaMalloc((void **)&c->rbuf, sizeof(double2) * n));
+    // twiddles exp(-2 pi i m / L) and their conjugates, in double
+    std::vector<double2> tw(2 * L);
+    std::vector<float2> twf(2 * L);
+    const double pi = 3.14159265358979323846;
+    for (int m = 0; m < L; m++) {
+        const double a = 2.0 * pi * (double)m / (double)L;
+        const double cr = cos(a), si = sin(a);
+        tw[m] = make_double2(cr, -si);
+        tw[L + m] = make_double2(cr, si);
+        twf[m] = make_float2((float)cr, (float)-si);
+        twf[L + m] = make_float2((float)cr, (float)si);
+    }
+    CG_CU(cudaMemcpyAsync(c->tw64, tw.data(), sizeof(double2) * 2 * L, cudaMemcpyHostToDevice, c->stream));
+    CG_CU(cudaMemcpyAsync(c->tw32, twf.data(), sizeof(float2) * 2 * L, cudaMemcpyHostToDevice, c->stream));
+    double2 *g_tmp = nullptr;
+    double *chi_tmp = nullptr;
+    const double2 *gp = (const double2 *)g_block;
+    const double *cp = chi;
+    if (!g_dev) {
+        CG_CU(cudaMalloc((void **)&g_tmp, sizeof(double2) * n));
+        CG_CU(cudaMemcpyAsync(g_tmp, g_block, sizeof(double2) * n, cudaMemcpyHostToDevice, c->stream));
+        gp = g_tmp;
+    }
+    if (!chi_dev) {
+        CG_CU(cudaMalloc((void **)&chi_tmp, sizeof(double) * n));
+        CG_CU(cudaMemcpyAsync(chi_tmp, chi, sizeof(double) * n, cudaMemcpyHostToDevice, c->stream));
+        cp = chi_tmp;
+    }
+    int s = set_operator_dev(c, N, gp, cp, chi_scale);
+    if (g_tmp) cudaFree(g_tmp);
+    if (chi_tmp) cudaFree(chi_tmp);
+    if (s != CG_OK) return s;
+    c->have_op = true;
+    return CG_OK;
+}
+
+int cugmres_set_operator_circulant(cg_ctx *c, int N, const cg_c64 *g_prep, const double *chi, double chi_scale) {
+    if (!c || !g_prep || N < 1) return CG_ERR_INVALID;
+    const int M = 2 * N - 1;
+    std::vector<cg_c128> g((size_t)N * N);
+    if (is_device_ptr(g_prep)) {
+        std::vector<cg_c64> tmp((size_t)M * M);
+        CG_CU(cudaMemcpy(tmp.data(), g_prep, sizeof(cg_c64) * tmp.size(), cudaMemcpyDeviceToHost));
+        for (int i = 0; i < N; i++)
+            for (int j = 0; j < N; j++) g[(size_t)i * N + j] = {tmp[(size_t)i * M + j].re, tmp[(size_t)i * M + j].im};
+    } else {
+        for (int i = 0; i < N; i++)
+            for (int j = 0; j < N; j++)
+                g[(size_t)i * N + j] = {g_prep[(size_t)i * M + j].re, g_prep[(size_t)i * M + j].im};
+    }
+    return cugmres_set_operator(c, N, g.data(), chi, chi_scale);
+}
+
+int cugmres_matvec(cg_ctx *c, const void *x, void *y, int precision) {
+    if (!c || !x || !y) return CG_ERR_INVALID;
+    if (!c->have_op) return CG_ERR_NO_OPERATOR;
+    if (precision != CG_PREC_FP64 && precision != CG_PREC_MIXED) return CG_ERR_INVALID;
+    CG_CU(cudaSetDevice(c->device));
+    const int prec = precision == CG_PREC_FP64 ? 0 : 1;
+    const size_t es = prec == 0 ? sizeof(double2) : sizeof(float2);
+    const size_t bytes = es * (size_t)c->N * c->N;
+    const bool xd = is_device_ptr(x), yd = is_device_ptr(y);
+    const void *xp = x;
+    void *yp = y;
+    if (!xd) {
+        CG_CU(cudaMemcpyAsync(c->xbuf, x, bytes, cudaMemcpyHostToDevice, c->stream));
+        xp = c->xbuf;
+    }
+    if (!yd) yp = c->rbuf;
+    CG_TRY(apply_explicit(c, prec, 0, prec, xp, nullptr, yp, nullptr));
+    if (!yd) CG_CU(cudaMemcpyAsync(y, yp, bytes, cudaMemcpyDeviceToHost, c->stream));
+    return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+int cugmres_residual(cg_ctx *c, const cg_c128 *b, const cg_c128 *x, cg_c128 *r, double *rel) {
+    if (!c || !b || !x) return CG_ERR_INVALID;
+    if (!c->have_op) return CG_ERR_NO_OPERATOR;
+    CG_CU(cudaSetDevice(c->device));
+    const long long n = (long long)c->N * c->N;
+    const size_t bytes = sizeof(double2) * n;
+    CG_TRY(ensure_krylov(c, 1, 1, sizeof(double2)));
+    const void *bp = b, *xp = x;
+    if (!is_device_ptr(b)) {
+        CG_CU(cudaMemcpyAsync(c->bbuf, b, bytes, cudaMemcpyHostToDevice, c->stream));
+        bp = c->bbuf;
+    }
+    if (!is_device_ptr(x)) {
+        CG_CU(cudaMemcpyAsync(c->xbuf, x, bytes, cudaMemcpyHostToDevice, c->stream));
+        xp = c->xbuf;
+    }
+    void *rp = (r && is_device_ptr(r)) ? (void *)r : (void *)c->rbuf;
+    CG_TRY(apply_explicit(c, 0, 1, 0, xp, bp, rp, c->kp.npart));
+    const int nb = row_blocks(c);
+    std::vector<double> parts(nb);
+    CG_CU(cudaMemcpyAsync(parts.data(), c->kp.npart, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));
+    if (r && rp == c->rbuf) CG_CU(cudaMemcpyAsync(r, rp, bytes, cudaMemcpyDeviceToHost, c->stream));
+    CG_TRY(launch_norm2(0, bp, n, c->kp.npart, &c->st->counter[2], &c->st->scalar, axpy_blocks(c, n), c->stream) ? CG_ERR_CUDA : CG_OK);
+    double nb2 = 0.0;
+    CG_CU(cudaMemcpyAsync(&nb2, &c->st->scalar, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CG_CU(cudaStreamSynchronize(c->stream));
+    double rr = 0.0;
+    for (int i = 0; i < nb; i++) rr += parts[i];
+    if (rel) *rel = sqrt(rr) / nb2;
+    return CG_OK;
+}
+
+int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_in, double *res_hist, int res_hist_len,
+                  cg_result *result) {
+    const double t0 = now_s();
+    if (!c || !b || !x) return CG_ERR_INVALID;
+    if (!c->have_op) return CG_ERR_NO_OPERATOR;
+    cg_opts o;
+    if (opts_in) o = *opts_in;
+    else cugmres_default_opts(&o);
+    if (o.restart < 1 || o.max_iter < 0 || !(o.tol >= 0.0) || (o.precision != CG_PREC_FP64 && o.precision != CG_PREC_MIXED) ||
+        (o.givens != CG_GIVENS_UNITARY && o.givens != CG_GIVENS_REFERENCE))
+        return CG_ERR_INVALID;
+    // coefficient arrays of k_axpy / k_backsolve live in 48 KB of shared memory
+    if (o.restart > 3000 || (o.fixed_iterations && o.max_iter > 3000)) return CG_ERR_NOT_IMPLEMENTED;
+    CG_CU(cudaSetDevice(c->device));
+    const int prec = o.precision == CG_PREC_FP64 ? 0 : 1;
+    const int m = o.fixed_iterations ? std::max(1, o.max_iter) : o.restart;
+    const long long n = (long long)c->N * c->N;
+    const size_t bytes = sizeof(double2) * n;
+    CG_TRY(ensure_krylov(c, m, std::max(1, o.max_iter), prec == 0 ? sizeof(double2) : sizeof(float2)));
+    cudaStream_t s = c->stream;
+
+    // inputs
+    const bool bd = is_device_ptr(b), xd = is_device_ptr(x);
+    if (!bd && !all_finite((const double *)b, 2 * (size_t)n)) return CG_ERR_NONFINITE;
+    if (!xd && !o.zero_x0 && !all_finite((const double *)x, 2 * (size_t)n)) return CG_ERR_NONFINITE;
+    const double2 *bp = (const double2 *)b;
+    double2 *xp = (double2 *)x;
+    if (!bd) {
+        CG_CU(cudaMemcpyAsync(c->bbuf, b, bytes, cudaMemcpyHostToDevice, s));
+        bp = c->bbuf;
+    }
+    if (!xd) {
+        xp = c->xbuf;
+        if (!o.zero_x0) CG_CU(cudaMemcpyAsync(xp, x, bytes, cudaMemcpyHostToDevice, s));
+    }
+    if (o.zero_x0) CG_CU(cudaMemsetAsync(xp, 0, bytes, s));
+
+    // device state
+    DevState h;
+    memset(&h, 0, sizeof(h));
+    h.m = m;
+    h.maxit = o.max_iter;
+    h.rotation = o.givens == CG_GIVENS_REFERENCE ? 1 : 0;
+    h.fixed = o.fixed_iterations ? 1 : 0;
+    h.tol = o.tol;
+    h.inner_tol = prec == 1 ? o.inner_tol : 0.0;
+    *c->st_host = h;
+    CG_CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(DevState), cudaMemcpyHostToDevice, s));
+    CG_LAUNCH(launch_norm2(0, bp, n, c->kp.npart, &c->st->counter[2], &c->st->nb, axpy_blocks(c, n), s));
+
+    KrylovPtrs kp = c->kp;
+    MatvecArgs a64 = margs(c, 0);
+    MatvecArgs ap = margs(c, prec);
+    VecSel vk;  // V_k (input of the Arnoldi matvec)
+    vk.base = c->V;
+    vk.stride = n;
+    vk.koff = 0;
+    VecSel vk1 = vk;  // V_{k+1}
+    vk1.koff = 1;
+    VecSel xs = fixed_vec(xp);
+    const int nrb = row_blocks(c);
+    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n);
+    int status = CG_OK;
+
+    for (;;) {
+        // true residual r = b - A x (FP64) into V_0, then cycle decisions on device
+        CG_LAUNCH(launch_rows_forward(0, a64, xs, nullptr, nullptr, GATE_NONE, s));
+        CG_LAUNCH(launch_cols_convolve(0, a64, nullptr, GATE_NONE, s));
+        CG_LAUNCH(launch_rows_inverse(0, 1, prec, a64, xs, nullptr, bp, fixed_vec(c->V), kp.npart, nullptr, GATE_NONE, s));
+        CG_LAUNCH(launch_cycle_begin(kp, nrb, s));
+        CG_CU(cudaMemcpyAsync(c->st_host, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+        CG_CU(cudaEventRecord(c->ev, s));
+        CG_CU(cudaEventSynchronize(c->ev));
+        const DevState hs = *c->st_host;
+        if (hs.status != 0) break;
+        if (o.timeout_s > 0.0 && now_s() - t0 > o.timeout_s) {
+            status = CG_ERR_TIMEOUT;
+            break;
+        }
+        const int steps = std::min(m, o.max_iter - hs.it);
+        for (int i = 0; i < steps; i++) {
+            CG_LAUNCH(launch_rows_forward(prec, ap, vk, kp.scale, c->st, GATE_STOP, s));
+            CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, s));
+            CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, kp.scale, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
+            CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h1, 0, ndot, GATE_STOP, s));
+            CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h1, -1.0, NJ_K_PLUS_1, vk1, 0, 1, nax, GATE_STOP, s));
+            CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h2, 0, ndot, GATE_STOP, s));
+            CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h2, -1.0, NJ_K_PLUS_1, vk1, 1, 1, nax, GATE_STOP, s));
+            CG_LAUNCH(launch_givens(kp, s));
+        }
+        CG_LAUNCH(launch_backsolve(kp, s));
+        CG_LAUNCH(launch_axpy(prec, 0, c->V, n, kp, kp.y, 1.0, NJ_K, xs, 0, 1, nax, GATE_NONE, s));
+    }
+
+    const DevState hs = *c->st_host;
+    if (status == CG_OK) {
+        switch (hs.status) {
+            case 1: status = CG_OK; break;
+            case 2: status = o.fixed_iterations ? CG_OK : CG_ERR_NOT_CONVERGED; break;
+            case 3: status = CG_ERR_BREAKDOWN; break;
+            case 4: status = CG_ERR_NONFINITE; break;
+            default: status = CG_ERR_CUDA; break;
+        }
+    }
+    if (res_hist && res_hist_len > 0) {
+        const int nh = std::min(res_hist_len, hs.it + 1);
+        CG_CU(cudaMemcpyAsync(res_hist, kp.hist, sizeof(double) * nh, cudaMemcpyDeviceToHost, s));
+    }
+    if (!xd) CG_CU(cudaMemcpyAsync(x, xp, bytes, cudaMemcpyDeviceToHost, s));
+    CG_CU(cudaStreamSynchronize(s));
+    if (result) {
+        result->status = status;
+        result->iterations = hs.it;
+        result->cycles = hs.cycles;
+        result->rel_residual_estimate = hs.est;
+        result->rel_residual_true = hs.true_res;
+        result->seconds = now_s() - t0;
+    }
+    return status;
+}
+
+int cugmres_fast_gmres(const cg_c64 *g_prep, const unsigned char *mask, cg_c64 *solution, float *actual_residual,
+                       unsigned int *gmres_n, float tolerance, int *res_vs_tol, unsigned int maxiter, unsigned int N,
+                       float chi_value, const cg_c64 *rhs, int precision) {
+    if (!g_prep || !mask || !solution || N < 1 || maxiter < 1) return CG_ERR_INVALID;
+    const size_t n = (size_t)N * N;
+    int dev = 0;
+    CG_CU(cudaGetDevice(&dev));
+    // host copies of the inputs (pointers may be device memory, as in the reference)
+    std::vector<unsigned char> hm(n);
+    std::vector<cg_c64> hx(n), hb(n);
+    if (is_device_ptr(mask)) CG_CU(cudaMemcpy(hm.data(), mask, n, cudaMemcpyDeviceToHost));
+    else memcpy(hm.data(), mask, n);
+    const bool sol_dev = is_device_ptr(solution);
+    if (sol_dev) CG_CU(cudaMemcpy(hx.data(), solution, sizeof(cg_c64) * n, cudaMemcpyDeviceToHost));
+    else memcpy(hx.data(), solution, sizeof(cg_c64) * n);
+    if (rhs) {
+        if (is_device_ptr(rhs)) CG_CU(cudaMemcpy(hb.data(), rhs, sizeof(cg_c64) * n, cudaMemcpyDeviceToHost));
+        else memcpy(hb.data(), rhs, sizeof(cg_c64) * n);
+    } else {
+        // the reference's incident field exp(-i k row), CUDA_GMRES/GMRES_kernels.cuh:557-572
+        const float k = (2 * 3.14f) / ((float)N / 6.f);
+        for (unsigned int i = 0; i < N; i++) {
+            const float arg = (float)(-(double)k * (double)i);
+            for (unsigned int j = 0; j < N; j++) hb[(size_t)i * N + j] = {cosf(arg), sinf(arg)};
+        }
+    }
+    std::vector<double> chi(n);
+    for (size_t e = 0; e < n; e++) chi[e] = hm[e] ? (double)chi_value : 0.0;
+    std::vector<cg_c128> b128(n), x128(n);
+    for (size_t e = 0; e < n; e++) {
+        b128[e] = {hb[e].re, hb[e].im};
+        x128[e] = {hx[e].re, hx[e].im};
+    }
+    cg_ctx *c = nullptr;
+    CG_TRY(cugmres_create(&c, dev));
+    int s = cugmres_set_operator_circulant(c, (int)N, g_prep, chi.data(), 1.0);
+    std::vector<double> hist(maxiter + 1, 0.0);
+    cg_result r;
+    memset(&r, 0, sizeof(r));
+    if (s == CG_OK) {
+        cg_opts o;
+        cugmres_default_opts(&o);
+        o.restart = (int)maxiter;
+        o.max_iter = (int)maxiter;
+        o.tol = tolerance;
+        o.fixed_iterations = 1;
+        o.givens = CG_GIVENS_REFERENCE;
+        o.precision = precision;
+        o.inner_tol = 0.0;
+        s = cugmres_solve(c, b128.data(), x128.data(), &o, hist.data(), (int)maxiter + 1, &r);
+    }
+    if (s == CG_OK) {
+        double nb = 0.0;
+        for (size_t e = 0; e < n; e++) nb += b128[e].re * b128[e].re + b128[e].im * b128[e].im;
+        nb = sqrt(nb);
+        std::vector<float> res(maxiter + 1, 0.f);
+        for (int i = 0; i <= r.iterations && i <= (int)maxiter; i++) res[i] = (float)(hist[i] * nb);
+        for (size_t e = 0; e < n; e++) hx[e] = {(float)x128[e].re, (float)x128[e].im};
+        if (sol_dev) s = cuerr(cudaMemcpy(solution, hx.data(), sizeof(cg_c64) * n, cudaMemcpyHostToDevice));
+        else memcpy(solution, hx.data(), sizeof(cg_c64) * n);
+        if (actual_residual) {
+            if (is_device_ptr(actual_residual))
+                s = cuerr(cudaMemcpy(actual_residual, res.data(), sizeof(float) * (maxiter + 1), cudaMemcpyHostToDevice));
+            else memcpy(actual_residual, res.data(), sizeof(float) * (maxiter + 1));
+        }
+        if (gmres_n) *gmres_n = (unsigned int)r.iterations;
+        if (res_vs_tol) *res_vs_tol = (r.iterations > 0 ? res[r.iterations] : res[0]) > tolerance;
+    }
+    cugmres_destroy(c);
+    return s;
+}
+
+}  // extern "C"

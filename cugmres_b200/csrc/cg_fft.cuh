@@ -1,0 +1,258 @@
+// Stockham radix-16 FFT building blocks for the circulant-embedding matvec.
+//
+// The reference applies its BTTB operator with two cuFFT calls on an odd
+// (2N-1)^2 grid plus three elementwise kernels (CUDA_GMRES/Fast_matvec.cuh:1-28).
+// Here the embedding is a power-of-two L x L grid (L >= 2N-1, normally L = 2N)
+// and the 1D transforms are the project's own: a Stockham auto-sort FFT
+// (formulation of Govindaraju, Lloyd, Dotsenko, Smith and Manferdelli,
+// "High performance discrete Fourier transforms on graphics processors", SC08)
+// where each thread owns E = 16 points:
+//
+//   stage s with radix R and span Ns reads  a[j + r L/R]          (r < R)
+//   multiplies by the twiddle  w_L^{(j mod Ns) r L/(Ns R)},
+//   does an R-point DFT and writes b[(j/Ns) Ns R + (j mod Ns) + q Ns] (q < R).
+//
+// Thread t of a transform owns butterflies j = t + b*TPR (TPR = L/E threads).
+// The first stage (span 1, no twiddles) reads and the last stage (span L/R)
+// writes the "canonical" register set reg[p] = element t + p*TPR, so a
+// transform can start from coalesced global loads and end in coalesced global
+// stores or in the next transform without touching shared memory.  Middle
+// stages exchange through shared memory padded by one element every 16, which
+// keeps the 16-byte accesses of a quarter warp on distinct banks.
+#pragma once
+
+#include "cg_common.cuh"
+
+namespace cg {
+
+// ------------------------------------------------------------ small DFTs
+// In-place natural-order DFTs on register arrays.  INV selects the sign of
+// the exponent: forward exp(-2 pi i k/R), inverse exp(+2 pi i k/R), unscaled.
+
+// multiply by w_4^1 = -i (forward) or +i (inverse)
+template <bool INV, typename C> __device__ __forceinline__ C mul_w4(C a) {
+    return INV ? mk<C>(-a.y, a.x) : mk<C>(a.y, -a.x);
+}
+// multiply by w_8^1 = (1 -/+ i)/sqrt(2)
+template <bool INV, typename C> __device__ __forceinline__ C mul_w8_1(C a) {
+    typedef typename real_of<C>::type R;
+    const R h = (R)0.70710678118654752440;
+    return INV ? mk<C>((a.x - a.y) * h, (a.x + a.y) * h) : mk<C>((a.x + a.y) * h, (a.y - a.x) * h);
+}
+// multiply by w_8^3 = (-1 -/+ i)/sqrt(2)
+template <bool INV, typename C> __device__ __forceinline__ C mul_w8_3(C a) {
+    typedef typename real_of<C>::type R;
+    const R h = (R)0.70710678118654752440;
+    return INV ? mk<C>(-(a.x + a.y) * h, (a.x - a.y) * h) : mk<C>((a.y - a.x) * h, -(a.x + a.y) * h);
+}
+// multiply by (cr + i*ci) with ci negated for the forward direction
+template <bool INV, typename C>
+__device__ __forceinline__ C mul_cs(C a, typename real_of<C>::type cr, typename real_of<C>::type si) {
+    typedef typename real_of<C>::type R;
+    const R ci = INV ? si : -si;
+    return mk<C>(a.x * cr - a.y * ci, a.x * ci + a.y * cr);
+}
+
+template <bool INV, typename C> __device__ __forceinline__ void dft2(C *v) {
+    C t = v[0];
+    v[0] = cadd(t, v[1]);
+    v[1] = csub(t, v[1]);
+}
+
+template <bool INV, typename C> __device__ __forceinline__ void dft4(C *v) {
+    C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]), t3 = mul_w4<INV>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+}
+
+// combine two half-length DFTs: X[k] = E[k] + w^k O[k], X[k+h] = E[k] - w^k O[k]
+template <bool INV, typename C> __device__ __forceinline__ void dft8(C *v) {
+    C e[4] = {v[0], v[2], v[4], v[6]};
+    C o[4] = {v[1], v[3], v[5], v[7]};
+    dft4<INV>(e);
+    dft4<INV>(o);
+    o[1] = mul_w8_1<INV>(o[1]);
+    o[2] = mul_w4<INV>(o[2]);
+    o[3] = mul_w8_3<INV>(o[3]);
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        v[k] = cadd(e[k], o[k]);
+        v[k + 4] = csub(e[k], o[k]);
+    }
+}
+
+// cos(k pi/8), sin(k pi/8) for k = 1, 3 (exact decimal expansions of the
+// mathematical constants, rounded by the compiler)
+#define CG_C1 0.92387953251128675613
+#define CG_S1 0.38268343236508977173
+
+template <bool INV, typename C> __device__ __forceinline__ C mul_w16(C a, int k) {
+    typedef typename real_of<C>::type R;
+    switch (k) {
+        case 1: return mul_cs<INV>(a, (R)CG_C1, (R)CG_S1);
+        case 2: return mul_w8_1<INV>(a);
+        case 3: return mul_cs<INV>(a, (R)CG_S1, (R)CG_C1);
+        case 4: return mul_w4<INV>(a);
+        case 5: return mul_cs<INV>(a, -(R)CG_S1, (R)CG_C1);
+        case 6: return mul_w8_3<INV>(a);
+        case 7: return mul_cs<INV>(a, -(R)CG_C1, (R)CG_S1);
+        default: return a;
+    }
+}
+
+template <bool INV, typename C> __device__ __forceinline__ void dft16(C *v) {
+    C e[8], o[8];
+#pragma unroll
+    for (int r = 0; r < 8; r++) {
+        e[r] = v[2 * r];
+        o[r] = v[2 * r + 1];
+    }
+    dft8<INV>(e);
+    dft8<INV>(o);
+#pragma unroll
+    for (int k = 0; k < 8; k++) {
+        C t = mul_w16<INV>(o[k], k);
+        v[k] = cadd(e[k], t);
+        v[k + 8] = csub(e[k], t);
+    }
+}
+
+template <int R, bool INV, typename C> __device__ __forceinline__ void dft(C *v) {
+    if constexpr (R == 2) dft2<INV>(v);
+    else if constexpr (R == 4) dft4<INV>(v);
+    else if constexpr (R == 8) dft8<INV>(v);
+    else if constexpr (R == 16) dft16<INV>(v);
+}
+
+// DFT of length R whose inputs R/2 .. R-1 are zero (the zero-padded half of
+// the embedding): X[2m] = DFT_{R/2}(v)[m], X[2m+1] = DFT_{R/2}(v[r] w_R^r)[m].
+template <int R, bool INV, typename C> __device__ __forceinline__ void dft_half_input(C *v) {
+    if constexpr (R == 2) {
+        v[1] = v[0];
+    } else {
+    C a[R / 2], b[R / 2];
+#pragma unroll
+    for (int r = 0; r < R / 2; r++) a[r] = v[r];
+    if constexpr (R == 16) {
+#pragma unroll
+        for (int r = 0; r < 8; r++) b[r] = mul_w16<INV>(v[r], r);
+    } else if constexpr (R == 8) {
+        b[0] = v[0];
+        b[1] = mul_w8_1<INV>(v[1]);
+        b[2] = mul_w4<INV>(v[2]);
+        b[3] = mul_w8_3<INV>(v[3]);
+    } else {  // R == 4
+        b[0] = v[0];
+        b[1] = mul_w4<INV>(v[1]);
+    }
+    dft<R / 2, INV>(a);
+    dft<R / 2, INV>(b);
+#pragma unroll
+    for (int m = 0; m < R / 2; m++) {
+        v[2 * m] = a[m];
+        v[2 * m + 1] = b[m];
+    }
+    }
+}
+
+// ------------------------------------------------------------ plans
+// Length L = E^a * rem (rem in {1,2,4,8}) with E = 16: stages radix 16 ...,
+// then one stage of radix rem.  Lengths below 16 use a single stage of radix L.
+template <int L> struct Plan {
+    static constexpr int E = (L >= 16) ? 16 : L;
+    static constexpr int TPR = L / E;
+    __host__ __device__ static constexpr int ilog(int v) { return v <= 1 ? 0 : 1 + ilog(v / 2); }
+    static constexpr int LOG = ilog(L);
+    static constexpr int LOGE = ilog(E);
+    static constexpr int NFULL = LOG / LOGE;
+    static constexpr int REM = 1 << (LOG - NFULL * LOGE);
+    static constexpr int NST = NFULL + (REM > 1 ? 1 : 0);
+    __host__ __device__ static constexpr int radix(int s) { return s < NFULL ? E : REM; }
+    __host__ __device__ static constexpr int span(int s) { return s == 0 ? 1 : span(s - 1) * radix(s - 1); }
+    // padded shared-memory index (one pad element every 16)
+    static __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
+    static constexpr int SMEM_ELEMS = L + L / 16;
+};
+
+// Twiddle lookup: the caller passes the forward table exp(-2 pi i m / L) or,
+// for inverse transforms, the conjugated table; m < L.
+template <bool INV, typename C> __device__ __forceinline__ C twiddle(const C *__restrict__ tw, int m) {
+    return __ldg(tw + m);
+}
+
+// One Stockham stage S of a length-L transform (compile-time radix and span).
+// tmp holds the previous stage's butterfly outputs (tmp[b*Rp + q]) on entry
+// and this stage's outputs on exit; the last stage stores canonical reg.
+template <int L, bool INV, bool HALF_IN, int S> struct Stage {
+    typedef Plan<L> P;
+    static constexpr int E = P::E;
+    static constexpr int TPR = P::TPR;
+    static constexpr int R = P::radix(S);
+    static constexpr int Ns = P::span(S);
+    static constexpr int NB = E / R;  // butterflies per thread in this stage
+    template <typename C>
+    static __device__ __forceinline__ void run(C (&reg)[E], C (&tmp)[E], C *sm, const C *__restrict__ tw, int t) {
+        if constexpr (S > 0) {
+            // write the previous stage's outputs, then read this stage's inputs
+            constexpr int Rp = P::radix(S - 1);
+            constexpr int Nsp = P::span(S - 1);
+            constexpr int NBp = E / Rp;
+            __syncthreads();
+#pragma unroll
+            for (int b = 0; b < NBp; b++) {
+                const int j = t + b * TPR;
+                const int base = (j / Nsp) * Nsp * Rp + (j % Nsp);
+#pragma unroll
+                for (int q = 0; q < Rp; q++) sm[P::pad(base + q * Nsp)] = tmp[b * Rp + q];
+            }
+            __syncthreads();
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const int j = t + b * TPR;
+                const int k = j % Ns;
+                constexpr int step = L / (Ns * R);
+#pragma unroll
+                for (int r = 0; r < R; r++) {
+                    C v = sm[P::pad(j + r * (L / R))];
+                    if (r > 0) v = cmul(v, twiddle<INV>(tw, k * r * step));
+                    tmp[b * R + r] = v;
+                }
+            }
+        } else {
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+#pragma unroll
+                for (int r = 0; r < R; r++) tmp[b * R + r] = reg[b + r * NB];
+        }
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            if constexpr (S == 0 && HALF_IN) dft_half_input<R, INV>(tmp + b * R);
+            else dft<R, INV>(tmp + b * R);
+        }
+        if constexpr (S == P::NST - 1) {
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+#pragma unroll
+                for (int q = 0; q < R; q++) reg[b + q * NB] = tmp[b * R + q];
+        } else {
+            Stage<L, INV, HALF_IN, S + 1>::run(reg, tmp, sm, tw, t);
+        }
+    }
+};
+
+// Runs one length-L transform owned by TPR threads (this thread is t).
+// reg[p] holds element t + p*TPR on entry and on exit.  sm is this
+// transform's padded shared-memory region (Plan<L>::SMEM_ELEMS elements).
+// HALF_IN: inputs L/2 .. L-1 are zero (first stage uses dft_half_input).
+// Every thread of the block must call this the same number of times
+// (it contains __syncthreads()).
+template <int L, bool INV, bool HALF_IN, typename C>
+__device__ __forceinline__ void fft_run(C (&reg)[Plan<L>::E], C *sm, const C *__restrict__ tw, int t) {
+    C tmp[Plan<L>::E];
+    Stage<L, INV, HALF_IN, 0>::run(reg, tmp, sm, tw, t);
+}
+
+}  // namespace cg

@@ -1,0 +1,101 @@
+// Internal declarations shared by the cugmres translation units (not part of
+// the C-ABI; the public interface is include/cugmres.h).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace cg {
+
+// Solver state kept in device memory so that no host synchronisation is
+// needed per Arnoldi step (the reference copies Jtotal(i+1,0) to the host and
+// the residual back every iteration, CUDA_GMRES/GMRES.cuh:369-371).
+struct DevState {
+    int k;         // Arnoldi column being built in this cycle (basis holds k+1 vectors)
+    int it;        // iterations completed over all cycles
+    int stop;      // 1: the current cycle takes no further Arnoldi step
+    int status;    // 0 running, 1 converged, 2 iteration budget spent, 3 breakdown, 4 non-finite
+    int m;         // restart length of the current cycle
+    int maxit;     // total iteration budget
+    int rotation;  // 0 unitary Givens, 1 the reference's formula
+    int fixed;     // 1: never stop on the residual estimate (reference semantics)
+    int cycles;    // cycles started
+    int brk;       // breakdown seen in this cycle
+    int pad0, pad1;
+    double tol;       // relative tolerance on ||b - A x|| / ||b||
+    double inner_tol; // cycle stops when |g_{k+1}| <= inner_tol * beta0 (mixed precision)
+    double nb;        // ||b||
+    double beta0;     // ||r|| at the start of the current cycle
+    double est;       // last relative residual estimate |g_{k+1}| / ||b||
+    double true_res;  // last true relative residual ||b - A x|| / ||b||
+    double wnorm2;    // ||w||^2 of the vector just orthogonalised
+    double scalar;    // scratch scalar result of a norm reduction
+    unsigned int counter[8];  // tickets of the last-block reductions
+};
+
+// Device workspace of one Krylov cycle (restart m, budget maxit).
+struct KrylovPtrs {
+    DevState *st;
+    double *scale;   // [m+2] lazy normalisation of the stored basis vectors
+    double2 *h1;     // [m+1] first Gram-Schmidt coefficients
+    double2 *h2;     // [m+1] reorthogonalisation coefficients
+    double2 *Rm;     // [(m+1) * m] triangular factor, column k at Rm + k*(m+1)
+    double2 *cs;     // [m] rotation cosines (complex)
+    double *sn;      // [m] rotation sines (real)
+    double2 *g;      // [m+1] rotated right-hand side
+    double2 *y;      // [m] least-squares solution
+    double *hist;    // [maxit+1] relative residual history
+    double *part;    // [nblk_dot * (m+1) * 2] dot partials
+    double *npart;   // [nblk_max] norm partials
+    int mcap;        // allocated restart capacity (leading dimension of Rm / part)
+};
+
+// Matvec launch parameters for one precision (C = double2 or float2, R its real type).
+struct MatvecArgs {
+    int N, L;
+    const void *gq;     // quarter spectrum (C)
+    const void *cdiag;  // N x N real diagonal k0^2 chi (R)
+    const void *tw;     // L twiddles (C)
+    void *T;            // N x L intermediate (C)
+};
+
+// Reference to a basis vector selected by the device-side Arnoldi index:
+// ptr = base + (st ? st->k + koff : 0) * stride.
+struct VecSel {
+    void *base;
+    long long stride;
+    int koff;
+};
+
+// kernel launchers (cg_matvec.cu)
+int launch_rows_forward(int prec, const MatvecArgs &a, VecSel x, const double *xscale_base, const DevState *st,
+                        int gate, cudaStream_t s);
+int launch_cols_convolve(int prec, const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s);
+// mode 0: y = s*x - conv;  mode 1: y = b - x + conv (y may be float2 while the matvec is double2: out_prec)
+int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xscale_base,
+                        const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s);
+int rows_per_block(int prec, int L);
+int fft_supported(int L);
+
+// full (unpruned) forward 2D transform of an L x L FP64 array, used to build the spectrum
+int launch_fft2d_full_fp64(int L, double2 *a, const double2 *tw, cudaStream_t s);
+
+// kernel launchers (cg_krylov.cu)
+int launch_dots(int prec_v, const void *V, long long n, const KrylovPtrs &kp, VecSel w, double2 *out, int ctr,
+                int nblk, int gate, cudaStream_t s);
+int launch_axpy(int prec_v, int prec_w, const void *V, long long n, const KrylovPtrs &kp, const double2 *src,
+                double sign, int nj_mode, VecSel w, int want_norm, int ctr, int nblk, int gate, cudaStream_t s);
+int launch_givens(const KrylovPtrs &kp, cudaStream_t s);
+int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s);
+int launch_cycle_begin(const KrylovPtrs &kp, int nparts, cudaStream_t s);
+int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
+                 cudaStream_t s);
+int launch_convert(int from_prec, int to_prec, const void *src, void *dst, long long n, cudaStream_t s);
+
+// gate codes for the per-iteration kernels
+enum { GATE_NONE = 0, GATE_STOP = 1 };
+// nj_mode for launch_axpy: number of basis vectors used
+enum { NJ_K_PLUS_1 = 0, NJ_K = 1 };
+
+}  // namespace cg

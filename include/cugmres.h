@@ -1,0 +1,148 @@
+/* cugmres_b200 -- C-ABI of the B200 GMRES solver for A = I - G diag(c),
+ * G a symmetric block-Toeplitz-Toeplitz-block (BTTB) Green's-function matrix
+ * on an N x N grid and c a real diagonal (c = k0^2 chi for the Helmholtz
+ * Lippmann-Schwinger / GFIEM system).
+ *
+ * Every function returns a status code (CG_OK = 0) and never exits the
+ * process.  Arrays are row-major N x N grids of interleaved complex numbers
+ * (re, im); pointers may be host or device memory (detected per call).
+ * A context owns one CUDA stream and its device workspace; calls on one
+ * context must not overlap, different contexts are independent.
+ *
+ * Reference interfaces each entry point replaces (paths inside the reference
+ * project "Benchmarks of CUDA-based GMRES Solver for Toeplitz and Hankel
+ * Matrices and Applications to Topology Optimization of Photonic Devices/"):
+ *   CUDA_GMRES/GMRES.cuh:22-35           Fast_GMRES_with_CUDA   -> cugmres_solve, cugmres_fast_gmres
+ *   CUDA_GMRES/Fast_matvec.cuh:1-28      G_x_fft_matvec (+ crop) -> cugmres_matvec
+ *   CUDA_GMRES/launch_GMRES.cuh:93-142   cuFFT plan + FFT of G   -> cugmres_create, cugmres_set_operator
+ *   MKL_GMRES_test_09122019/source/loop_functions.h:128-168
+ *                                        Green_matrix_create_MKL -> cugmres_green_block
+ *   PyGMRES/GMRES.py:47-57               matvec(x, eps, k)       -> cugmres_matvec (via cugmres_b200.matvec)
+ */
+#ifndef CUGMRES_H
+#define CUGMRES_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { double re, im; } cg_c128;
+typedef struct { float re, im; } cg_c64;
+typedef struct cg_ctx cg_ctx;
+
+/* status codes */
+enum {
+    CG_OK = 0,
+    CG_ERR_INVALID = 1,         /* bad argument (null pointer, size, option)            */
+    CG_ERR_CUDA = 2,            /* a CUDA runtime call failed                           */
+    CG_ERR_NOT_CONVERGED = 3,   /* iteration budget spent before reaching tol           */
+    CG_ERR_BREAKDOWN = 4,       /* Arnoldi breakdown without convergence                */
+    CG_ERR_NONFINITE = 5,       /* NaN or Inf met in the input or during the iteration  */
+    CG_ERR_TIMEOUT = 6,         /* opts.timeout_s elapsed                               */
+    CG_ERR_NOT_IMPLEMENTED = 7, /* size or mode this build does not support             */
+    CG_ERR_NO_OPERATOR = 8,     /* cugmres_set_operator has not been called             */
+    CG_ERR_OOM = 9              /* device allocation failed                             */
+};
+
+/* precision of the Krylov cycle */
+enum {
+    CG_PREC_FP64 = 0,  /* complex128 everywhere                                         */
+    CG_PREC_MIXED = 1  /* complex64 Arnoldi cycles inside an FP64 residual/update loop  */
+};
+
+/* Givens rotation formula */
+enum {
+    CG_GIVENS_UNITARY = 0,   /* [[conj(c), s], [-s, c]]: true GMRES minimal residual          */
+    CG_GIVENS_REFERENCE = 1  /* [[c, s], [-s, c]] with c = h_ii/rho as the reference writes it
+                                (MKL_GMRES_test_09122019/source/loop_functions.h:630-689)      */
+};
+
+/* Green's-function constructions for cugmres_green_block */
+enum {
+    CG_GREEN_HELMHOLTZ = 0, /* G(d) = (i/4) H0(k0 h |d|) h^2, self term (i pi a/(2k0)) H1(k0 a) - 1/k0^2, pi a^2 = h^2 */
+    CG_GREEN_REFERENCE = 1, /* g(i,j) = (i/4) H0(k sqrt((i-1/2)^2 + j^2)) with k = 2*3.14f/(N/6.f), rounded to float
+                               (loop_functions.h:128-168)                                            */
+    CG_GREEN_PYGMRES = 2    /* g(i,j) = (i/4) H0(k0 sqrt(i^2 + (j-1/2)^2)) in double, the NumPy reference's
+                               get_green_matrix(k0, N) (PyGMRES/GMRES.py:20-27); h is ignored        */
+};
+
+typedef struct {
+    int restart;        /* Krylov dimension per cycle m (>= 1)                                 */
+    int max_iter;       /* total Arnoldi steps allowed                                         */
+    double tol;         /* stop when ||b - A x|| / ||b|| <= tol                                */
+    int precision;      /* CG_PREC_*                                                           */
+    int givens;         /* CG_GIVENS_*                                                         */
+    double inner_tol;   /* mixed: a complex64 cycle ends when its residual dropped by this      */
+    int zero_x0;        /* 1: ignore x on entry and start from 0                               */
+    int fixed_iterations; /* 1: reference semantics -- one cycle of exactly max_iter steps,
+                             tol is an absolute threshold on ||b - A x0|| only                 */
+    double timeout_s;   /* <= 0: none; otherwise the solve returns CG_ERR_TIMEOUT after this    */
+    int reserved[8];
+} cg_opts;
+
+typedef struct {
+    int status;                   /* CG_OK, CG_ERR_NOT_CONVERGED, CG_ERR_BREAKDOWN, ...   */
+    int iterations;               /* Arnoldi steps taken                                  */
+    int cycles;                   /* restart cycles started                               */
+    double rel_residual_estimate; /* last |g_{k+1}| / ||b||                               */
+    double rel_residual_true;     /* ||b - A x|| / ||b|| of the returned x (FP64 matvec)  */
+    double seconds;               /* wall time of the solve                               */
+} cg_result;
+
+const char *cugmres_strerror(int status);
+int cugmres_version(void);
+void cugmres_default_opts(cg_opts *opts);
+
+/* Creates a context on `device` with its own non-blocking stream. */
+int cugmres_create(cg_ctx **ctx, int device);
+int cugmres_destroy(cg_ctx *ctx);
+/* Optional: run on a caller-provided cudaStream_t instead of the context's own. */
+int cugmres_set_stream(cg_ctx *ctx, void *stream);
+int cugmres_synchronize(cg_ctx *ctx);
+
+/* Host-side Green's-function block g[d1*N + d2], 0 <= d1, d2 < N, for the
+ * symmetric BTTB matrix G(i1-i2, j1-j2) = g(|i1-i2|, |j1-j2|).  No GPU needed. */
+int cugmres_green_block(int kind, int N, double k0, double h, cg_c128 *out);
+
+/* Sets the operator A = I - G diag(chi_scale * chi).  g_block: N x N as
+ * produced by cugmres_green_block (host or device), chi: N x N real.
+ * Builds the L x L circulant spectrum (L = smallest power of two >= 2N-1) on
+ * the GPU in FP64 and keeps FP64 and FP32 copies of its even quarter. */
+int cugmres_set_operator(cg_ctx *ctx, int N, const cg_c128 *g_block, const double *chi, double chi_scale);
+/* Same from the reference's spatial (2N-1) x (2N-1) circulant G_prep
+ * (CUDA_GMRES/Release/input/G_prep_N.txt layout, row-major, complex64);
+ * its first N x N block is the g_block. */
+int cugmres_set_operator_circulant(cg_ctx *ctx, int N, const cg_c64 *g_prep, const double *chi, double chi_scale);
+int cugmres_grid_size(const cg_ctx *ctx, int *N, int *L);
+
+/* y = A x.  precision CG_PREC_FP64: x, y are cg_c128 arrays; CG_PREC_MIXED:
+ * cg_c64 arrays computed with the FP32 spectrum. */
+int cugmres_matvec(cg_ctx *ctx, const void *x, void *y, int precision);
+/* r = b - A x in FP64; *rel = ||r|| / ||b|| (either output may be NULL). */
+int cugmres_residual(cg_ctx *ctx, const cg_c128 *b, const cg_c128 *x, cg_c128 *r, double *rel);
+
+/* Solves A x = b.  x holds x0 on entry (unless opts->zero_x0) and the
+ * solution on return.  res_hist (may be NULL) receives up to res_hist_len
+ * relative residuals: [0] = ||b - A x0|| / ||b||, [i] = estimate after step i. */
+int cugmres_solve(cg_ctx *ctx, const cg_c128 *b, cg_c128 *x, const cg_opts *opts, double *res_hist,
+                  int res_hist_len, cg_result *result);
+
+/* Drop-in for the reference's Fast_GMRES_with_CUDA (CUDA_GMRES/GMRES.cuh:22-35):
+ * same iteration semantics (exactly maxiter Arnoldi steps, no restart,
+ * absolute `tolerance` gating the first step, the reference's Givens
+ * formula, residual history of maxiter+1 absolute estimates), complex64 in and
+ * out.  Instead of the pre-transformed spectrum, cuFFT plan and BLAS handles
+ * it takes the spatial circulant G_prep ((2N-1)^2, the array the reference
+ * transforms at CUDA_GMRES/launch_GMRES.cuh:138-142) and the contrast
+ * `chi_value` (the reference's CHI macro, CUDA_GMRES/GMRES_kernels.cuh:19) applied where
+ * mask != 0.  rhs may be NULL for the reference's plane wave exp(-i k row).
+ * The arithmetic is FP64 (precision = CG_PREC_FP64) or the mixed path. */
+int cugmres_fast_gmres(const cg_c64 *g_prep, const unsigned char *mask, cg_c64 *solution, float *actual_residual,
+                       unsigned int *gmres_n, float tolerance, int *res_vs_tol, unsigned int maxiter, unsigned int N,
+                       float chi_value, const cg_c64 *rhs, int precision);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUGMRES_H */

@@ -1,0 +1,136 @@
+"""GPU GMRES (CGS2 + single-warp Givens, device-side control) against the CPU
+oracle's restatement of the reference method, through the C-ABI."""
+import numpy as np
+import pytest
+
+from conftest import golden
+import cugmres_b200 as cg
+from cugmres_b200 import problems as P
+
+pytestmark = pytest.mark.gpu
+
+
+def test_reference_semantics_vs_oracle(solver, oracle):
+    """Fixed maxiter, reference Givens formula, x0 = b: the FP64 solution matches
+    the complex128 restatement of FFT_GMRES_with_MKL to 1e-10."""
+    N, maxit = 64, 20
+    pr = P.reference_cylinder(N)
+    solver.set_operator(pr["g_block"], pr["chi"], 1.0)
+    x, info = solver.solve(pr["b"], x0=pr["x0"], restart=maxit, max_iter=maxit, tol=1e-8,
+                           givens="reference", fixed_iterations=True)
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    xo, res, n, flag, _ = oracle.gmres_reference(gh, pr["chi"], pr["b"], pr["x0"], maxit, 1e-8)
+    assert info["iterations"] == n == maxit
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-10
+    nb = np.linalg.norm(pr["b"])
+    assert np.allclose(info["res_hist"] * nb, res, rtol=1e-8)
+
+
+def test_mkl_solution_256_on_gpu(solver, oracle):
+    N = 256
+    d = golden("ref_mkl_solution_256_m44.npz")
+    ref = d["solution"].astype(np.complex128)
+    pr = P.reference_cylinder(N)
+    solver.set_operator(pr["g_block"], pr["chi"], 1.0)
+    x, info = solver.solve(pr["b"], x0=pr["x0"], restart=44, max_iter=44, tol=1e-8, givens="reference",
+                           fixed_iterations=True)
+    assert info["iterations"] == 44
+    assert np.linalg.norm(x - ref) / np.linalg.norm(ref) < 3e-5
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    xo, *_ = oracle.gmres_reference(gh, pr["chi"], pr["b"], pr["x0"], 44, 1e-8)
+    assert np.linalg.norm(x - xo) / np.linalg.norm(xo) < 1e-10
+
+
+def test_fast_gmres_drop_in(cuda_device, oracle):
+    N, maxit = 64, 25
+    gp = golden("ref_G_prep_64.npz")["g_prep"]
+    pr = P.reference_cylinder(N)
+    sol, res, n, flag = cg.fast_gmres(gp, pr["mask"], pr["x0"].astype(np.complex64), maxit, 1e-3, pr["chi_value"])
+    assert n == maxit and res.shape == (maxit + 1,)
+    gh = oracle.spectrum(gp[:N, :N].astype(np.complex128), 2 * N)
+    xo, reso, no, flago, _ = oracle.gmres_reference(gh, pr["chi"], pr["b"], pr["x0"], maxit, 1e-3)
+    assert np.linalg.norm(sol - xo) / np.linalg.norm(xo) < 1e-6  # complex64 output
+    assert np.allclose(res, reso, rtol=1e-5)
+    assert flag == (res[-1] > 1e-3)
+
+
+@pytest.mark.parametrize("restart", [10, 30])
+def test_restarted_unitary_vs_oracle(solver, oracle, restart):
+    """Same number of steps, same restart: GPU CGS2 and oracle MGS iterates agree."""
+    N = 48
+    pr = P.helmholtz(N, 2.25, seed=21)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x, info = solver.solve(pr["b"], restart=restart, max_iter=60, tol=0.0)
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    o = oracle.gmres(gh, pr["chi"] * pr["chi_scale"], pr["b"], restart=restart, maxiter=60, tol=0.0)
+    assert info["iterations"] == o["iterations"] == 60
+    assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-10
+    assert np.allclose(info["res_hist"][1:], o["res_hist"][1:], rtol=1e-7)
+
+
+def test_config1_64_converges_like_oracle(solver, oracle):
+    """64x64, eps_r = 2.25, unrestarted, tol 1e-10, max 500: iterations within +-1 of
+    the oracle, FP64 true residual <= 1e-10, error vs a 1e-13 FP64 solve."""
+    N = 64
+    pr = P.helmholtz(N, 2.25, seed=0)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x, info = solver.solve(pr["b"], restart=500, max_iter=500, tol=1e-10)
+    assert info["status"] == 0
+    assert info["rel_residual_true"] <= 1e-10
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    c = pr["chi"] * pr["chi_scale"]
+    o = oracle.gmres(gh, c, pr["b"], restart=500, maxiter=500, tol=1e-10)
+    assert abs(info["iterations"] - o["iterations"]) <= 1
+    assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
+    tight = oracle.gmres(gh, c, pr["b"], restart=500, maxiter=500, tol=1e-13)
+    assert np.linalg.norm(x - tight["x"]) / np.linalg.norm(tight["x"]) < 1e-8
+
+
+def test_mixed_precision_refinement(solver, oracle):
+    N = 128
+    pr = P.helmholtz(N, 2.25, seed=2)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x, info = solver.solve(pr["b"], restart=50, max_iter=3000, tol=1e-10, precision="mixed", inner_tol=1e-5)
+    assert info["status"] == 0 and info["rel_residual_true"] <= 1e-10
+    x64, info64 = solver.solve(pr["b"], restart=50, max_iter=3000, tol=1e-13)
+    assert np.linalg.norm(x - x64) / np.linalg.norm(x64) < 1e-8
+    _, rel = solver.residual(pr["b"], x)
+    assert rel <= 1e-10
+
+
+def test_identity_operator_happy_breakdown(solver):
+    N = 32
+    pr = P.helmholtz(N, 1.0, seed=0)  # eps_r = 1 -> chi = 0 -> A = I
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x, info = solver.solve(pr["b"], restart=10, max_iter=10, tol=1e-12)
+    assert info["status"] == 0 and info["iterations"] == 1
+    assert np.abs(x - pr["b"]).max() < 1e-14
+
+
+def test_status_codes(solver):
+    N = 32
+    pr = P.helmholtz(N, 4.0, seed=0)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x, info = solver.solve(pr["b"], restart=5, max_iter=5, tol=1e-14)
+    assert info["status"] == cg._lib.CG_ERR_NOT_CONVERGED and info["iterations"] == 5
+    bad = pr["b"].copy()
+    bad[3, 4] = np.nan
+    x, info = solver.solve(bad, restart=5, max_iter=5)
+    assert info["status"] == cg._lib.CG_ERR_NONFINITE
+    with pytest.raises(cg.CugmresError):
+        solver.solve(pr["b"], restart=0)
+    x, info = solver.solve(pr["b"], restart=50, max_iter=100000, tol=1e-30, timeout_s=0.2)
+    assert info["status"] == cg._lib.CG_ERR_TIMEOUT
+
+
+def test_device_resident_solve(solver):
+    import torch
+    N = 64
+    pr = P.helmholtz(N, 2.25, seed=7)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    bt = torch.from_numpy(pr["b"]).cuda()
+    xt, info = solver.solve(bt, restart=100, max_iter=500, tol=1e-10)
+    assert xt.is_cuda and info["status"] == 0
+    x, info2 = solver.solve(pr["b"], restart=100, max_iter=500, tol=1e-10)
+    assert info["iterations"] == info2["iterations"]
+    assert np.abs(xt.cpu().numpy() - x).max() == 0.0
