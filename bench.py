@@ -1,0 +1,273 @@
+"""Benchmark: time-to-1e-10 FP64 relative residual per Helmholtz GFIEM solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--N 1024] [--eps 4] [--restart 100] [--tol 1e-10] [--precision fp64|mixed]
+
+One step = one complete GMRES solve of A x = b (x0 = 0) to ||b - A x|| / ||b|| <= tol
+on a synthetic seeded system (the configuration's shape, sizes and value
+distribution; no dataset is involved).  The value is device time per solve,
+measured with CUDA events on the solver's stream, max over ranks; for N > 1
+every rank solves its own replica and value = max rank time / solves of all
+ranks (replicas only: a single solve does not shard).
+
+Extra keys: roofline of the dominant phase (algorithmic bytes / live CUDA-event
+time vs the measured HBM copy bandwidth in MEASURED_PEAKS.json), e2e (the same
+solve through the public API from pinned host buffers, H2D/D2H inside the
+timed region), the CPU oracle timed on a bounded sample (rank 0, N = 1), clocks
+sampled with nvidia-smi during the timed region.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "time-to-1e-10 residual per 1024² solve: learned+mixed vs plain FP64; matvec GB/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--N", type=int, default=1024)
+    ap.add_argument("--eps", type=float, default=4.0)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--restart", type=int, default=100)
+    ap.add_argument("--tol", type=float, default=1e-10)
+    ap.add_argument("--max-iter", type=int, default=20000)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--inner-tol", type=float, default=1e-5)
+    ap.add_argument("--cpu-sample-steps", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampler running during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def make_problem(args):
+    from cugmres_b200 import problems as P
+    return P.helmholtz(args.N, args.eps, seed=args.seed)
+
+
+def workload(args):
+    return {"workload": f"helmholtz-gfiem {args.N}x{args.N} eps_r={args.eps:g} seed={args.seed} "
+                        f"restart={args.restart} tol={args.tol:g} x0=0 precision={args.precision}",
+            "N": args.N, "unknowns": args.N * args.N, "eps_r": args.eps, "lambda_over_h": 20,
+            "restart": args.restart, "tol": args.tol, "precision": args.precision,
+            "l2": "inputs larger than L2 (basis of restart+1 vectors of N^2 complex)"}
+
+
+def cpu_baseline(args, pr, iters_needed):
+    """Oracle (plain-C restatement of the reference's CPU GMRES) on a bounded
+    sample: `cpu-sample-steps` Arnoldi steps of the same system with every host
+    thread, scaled to one solve by the GPU's iteration count."""
+    from oracle import oracle as O
+    O.build()
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    L = 16
+    while L < 2 * args.N - 1:
+        L *= 2
+    gh = O.spectrum(pr["g_block"], L)
+    c = pr["chi"] * pr["chi_scale"]
+    s = max(1, args.cpu_sample_steps)
+    t0 = time.perf_counter()
+    out = O.gmres(gh, c, pr["b"], restart=args.restart, maxiter=s, tol=0.0)
+    dt = time.perf_counter() - t0
+    per_step = dt / max(1, out["iterations"])
+    return {"value": per_step * iters_needed, "unit": "s", "cores": threads, "kind": "port",
+            "sample": f"{out['iterations']} Arnoldi steps (incl. one FP64 residual) of the same "
+                      f"{args.N}x{args.N} system in {dt:.2f} s, scaled by {iters_needed} steps/solve"}
+
+
+def run_reference(args, rank, world):
+    """The reference's CPU GMRES (oracle port: MKL absent) on the host cores."""
+    if rank != 0:
+        return
+    pr = make_problem(args)
+    iters = int(os.environ.get("CUGMRES_BENCH_ITERS", "0")) or args.max_iter
+    times = []
+    for i in range(args.warmup + args.steps):
+        b = cpu_baseline(args, pr, iters)
+        if i >= args.warmup:
+            times.append(b["value"])
+    v = float(np.mean(times))
+    line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": workload(args), "cpu_baseline": {"kind": b["kind"], "cores": b["cores"],
+                                                       "sample": b["sample"], "value": v, "unit": "s"},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    import torch.distributed as dist
+    import cugmres_b200 as cg
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    pr = make_problem(args)
+    stream = torch.cuda.current_stream()
+    s = cg.Solver(local)
+    s.set_stream(stream.cuda_stream)
+    s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    b_dev = torch.from_numpy(pr["b"]).cuda()
+    kw = dict(restart=args.restart, max_iter=args.max_iter, tol=args.tol, precision=args.precision,
+              inner_tol=args.inner_tol)
+
+    for _ in range(args.warmup):
+        x, info = s.solve(b_dev, **kw)
+    torch.cuda.synchronize()
+
+    clocks = Clocks(local)
+    clocks.start()
+    s.profile(True)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    infos = []
+    for _ in range(args.steps):
+        x, info = s.solve(b_dev, **kw)
+        infos.append(info)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ms_total = e0.elapsed_time(e1)
+    prof = s.profile_read()
+    s.profile(False)
+    clk = clocks.stop()
+
+    # end to end through the public API from pinned host memory
+    b_host = torch.from_numpy(pr["b"]).pin_memory()
+    torch.cuda.synchronize()
+    e2 = torch.cuda.Event(enable_timing=True)
+    e3 = torch.cuda.Event(enable_timing=True)
+    e2.record(stream)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        xh, info_h = s.solve(b_host.numpy(), **kw)
+    e3.record(stream)
+    torch.cuda.synchronize()
+    e2e_wall = (time.perf_counter() - t0) / args.steps
+
+    t = torch.tensor([ms_total], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t.item()) / args.steps
+    value = ms_per_step / 1e3 / world  # seconds per solve over all ranks' solves
+
+    last = infos[-1]
+    hbm, peak_kind = peaks()
+    phases = {k: v for k, v in prof.items() if v["ms"] > 0}
+    dom = max(phases.items(), key=lambda kv: kv[1]["ms"])
+    tot_ms = sum(v["ms"] for v in phases.values())
+    roof = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1]["gbs"], 1), "peak": hbm, "unit": "GB/s",
+            "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind, "traffic": None,
+            "phases": {k: {"share": round(v["ms"] / tot_ms, 4), "gbs": round(v["gbs"], 1),
+                           "ms": round(v["ms"], 3)} for k, v in phases.items()}}
+    mv = prof.get("matvec", {})
+    line = {"metric": METRIC, "value": value, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128" if args.precision == "fp64" else "c64/c128",
+            "data": "synthetic", "config": workload(args),
+            "iterations": last["iterations"], "cycles": last["cycles"],
+            "rel_residual_true": last["rel_residual_true"], "status": last["status_text"],
+            "matvec_gbs": round(mv.get("gbs", 0.0), 1),
+            "roofline": roof,
+            "e2e": {"value": e2e_wall, "unit": "s", "h2d_bytes_per_step": int(pr["b"].nbytes),
+                    "d2h_bytes_per_step": int(pr["b"].nbytes)},
+            "gpu_launches": None, "clocks": clk}
+    # our kernels per solve: 8 per Arnoldi step + 5 per cycle (+1 norm)
+    line["gpu_launches"] = int(args.steps * (8 * last["iterations"] + 5 * last["cycles"] + 1))
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, pr, last["iterations"])
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -92,6 +92,20 @@ class Solver:
     def synchronize(self):
         check(_lib.lib().cugmres_synchronize(self._ctx), "synchronize")
 
+    def profile(self, enable=True):
+        """Enable (and reset) per-phase device timing of solve()."""
+        check(_lib.lib().cugmres_profile(self._ctx, int(bool(enable))), "profile")
+
+    def profile_read(self):
+        """{phase: dict(ms, bytes, launches, gbs)} accumulated since profile(True)."""
+        arr = (_lib.CgPhaseStats * len(_lib.PHASES))()
+        check(_lib.lib().cugmres_profile_read(self._ctx, arr), "profile_read")
+        out = {}
+        for name, st in zip(_lib.PHASES, arr):
+            out[name] = dict(ms=st.ms, bytes=st.bytes, launches=st.launches,
+                             gbs=(st.bytes / (st.ms * 1e-3) / 1e9) if st.ms > 0 else 0.0)
+        return out
+
     def set_operator(self, g_block, chi, chi_scale=1.0):
         """A = I - G diag(chi_scale * chi); g_block[d1, d2] is G at offset (d1, d2)."""
         N = int(g_block.shape[0])

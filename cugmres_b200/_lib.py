@@ -33,8 +33,10 @@ EXPORTS = (
     "cugmres_strerror", "cugmres_version", "cugmres_default_opts", "cugmres_create", "cugmres_destroy",
     "cugmres_set_stream", "cugmres_synchronize", "cugmres_green_block", "cugmres_set_operator",
     "cugmres_set_operator_circulant", "cugmres_grid_size", "cugmres_matvec", "cugmres_residual",
-    "cugmres_solve", "cugmres_fast_gmres",
+    "cugmres_solve", "cugmres_fast_gmres", "cugmres_profile", "cugmres_profile_read",
 )
+
+PHASES = ("matvec", "dots", "axpy", "small", "update", "residual")
 
 
 class CgOpts(ctypes.Structure):
@@ -61,6 +63,10 @@ class CgResult(ctypes.Structure):
         ("rel_residual_true", ctypes.c_double),
         ("seconds", ctypes.c_double),
     ]
+
+
+class CgPhaseStats(ctypes.Structure):
+    _fields_ = [("ms", ctypes.c_double), ("bytes", ctypes.c_double), ("launches", ctypes.c_longlong)]
 
 
 class CugmresError(RuntimeError):
@@ -104,6 +110,8 @@ def _declare(L):
     L.cugmres_residual.argtypes = [P, P, P, P, ctypes.POINTER(D)]
     L.cugmres_solve.argtypes = [P, P, P, ctypes.POINTER(CgOpts), P, I, ctypes.POINTER(CgResult)]
     L.cugmres_fast_gmres.argtypes = [P, P, P, P, ctypes.POINTER(U), F, ctypes.POINTER(I), U, U, F, P, I]
+    L.cugmres_profile.argtypes = [P, I]
+    L.cugmres_profile_read.argtypes = [P, ctypes.POINTER(CgPhaseStats)]
     for name in EXPORTS:
         if name not in ("cugmres_strerror", "cugmres_default_opts"):
             getattr(L, name).restype = I

@@ -54,6 +54,10 @@ struct cg_ctx {
     double2 *rbuf = nullptr;  // FP64 vector scratch (residual, matvec staging)
     int nparts_cap = 0;
     cudaEvent_t ev = nullptr;
+    // per-phase timing
+    bool prof = false;
+    std::vector<cudaEvent_t> evpool;
+    cg_phase_stats stats[CG_NPHASES] = {};
 };
 
 namespace {
@@ -255,6 +259,70 @@ int apply_explicit(cg_ctx *c, int prec, int mode, int out_prec, const void *x, c
     return CG_OK;
 }
 
+// Events recorded since the last collection: the interval between event i and
+// event i+1 belongs to phase tag[i] of Arnoldi step iter[i] (-1: not a step).
+struct CycleProf {
+    std::vector<int> tag;
+    std::vector<int> iter;
+    int used = 0;
+};
+
+int prof_event(cg_ctx *c, int idx, cudaEvent_t *out) {
+    while ((int)c->evpool.size() <= idx) {
+        cudaEvent_t e;
+        CG_CU(cudaEventCreate(&e));
+        c->evpool.push_back(e);
+    }
+    *out = c->evpool[idx];
+    return CG_OK;
+}
+
+// Records the event closing `phase` (the first call only opens).
+int prof_mark(cg_ctx *c, CycleProf &cp, int phase, int iter, cudaStream_t s) {
+    if (!c->prof) return CG_OK;
+    cudaEvent_t e;
+    CG_TRY(prof_event(c, cp.used, &e));
+    CG_CU(cudaEventRecord(e, s));
+    if (cp.used > 0) {
+        cp.tag.push_back(phase);
+        cp.iter.push_back(iter);
+    }
+    cp.used++;
+    return CG_OK;
+}
+
+// Called once the stream has passed every recorded event.  steps_done: Arnoldi
+// steps that did work in the cycle these events cover (later steps were gated
+// off on device and move no bytes); e: element bytes of the cycle precision.
+int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done) {
+    if (c->prof && cp.used >= 2) {
+        for (int i = 0; i + 1 < cp.used; i++) {
+            float ms = 0.f;
+            CG_CU(cudaEventElapsedTime(&ms, c->evpool[i], c->evpool[i + 1]));
+            const int t = cp.tag[i], k = cp.iter[i];
+            const bool live = k < steps_done;
+            double bytes = 0.0;
+            switch (t) {
+                case CG_PHASE_MATVEC: bytes = live ? 16.0 * n * e : 0.0; break;
+                case CG_PHASE_DOTS: bytes = live ? (k + 2.0) * n * e : 0.0; break;
+                case CG_PHASE_AXPY: bytes = live ? (k + 3.0) * n * e : 0.0; break;
+                case CG_PHASE_UPDATE: bytes = steps_done * n * e + 2.0 * n * 16.0; break;
+                case CG_PHASE_RESIDUAL: bytes = 16.0 * n * 16.0; break;
+                default: bytes = 0.0;
+            }
+            if (t >= 0 && t < CG_NPHASES) {
+                c->stats[t].ms += ms;
+                c->stats[t].bytes += bytes;
+                c->stats[t].launches += (t == CG_PHASE_SMALL || live || t == CG_PHASE_UPDATE || t == CG_PHASE_RESIDUAL) ? 1 : 0;
+            }
+        }
+    }
+    cp.used = 0;
+    cp.tag.clear();
+    cp.iter.clear();
+    return CG_OK;
+}
+
 bool all_finite(const double *p, size_t n) {
     for (size_t i = 0; i < n; i++)
         if (!isfinite(p[i])) return false;
@@ -333,6 +401,7 @@ int cugmres_destroy(cg_ctx *c) {
     dfree_t(c->st);
     if (c->st_host) cudaFreeHost(c->st_host);
     if (c->ev) cudaEventDestroy(c->ev);
+    for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CG_OK;
@@ -353,6 +422,19 @@ int cugmres_set_stream(cg_ctx *c, void *stream) {
 int cugmres_synchronize(cg_ctx *c) {
     if (!c) return CG_ERR_INVALID;
     return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+int cugmres_profile(cg_ctx *c, int enable) {
+    if (!c) return CG_ERR_INVALID;
+    c->prof = enable != 0;
+    for (int i = 0; i < CG_NPHASES; i++) c->stats[i] = cg_phase_stats{0.0, 0.0, 0};
+    return CG_OK;
+}
+
+int cugmres_profile_read(cg_ctx *c, cg_phase_stats *out) {
+    if (!c || !out) return CG_ERR_INVALID;
+    for (int i = 0; i < CG_NPHASES; i++) out[i] = c->stats[i];
+    return CG_OK;
 }
 
 int cugmres_grid_size(const cg_ctx *c, int *N, int *L) {
@@ -575,34 +657,51 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     const int ndot = dot_blocks(c), nax = axpy_blocks(c, n);
     int status = CG_OK;
 
+    CycleProf cp;
+    int it_prev = 0;
+    const double nd = (double)n, esz = prec == 0 ? 16.0 : 8.0;
     for (;;) {
+        if (cp.used == 0) CG_TRY(prof_mark(c, cp, -1, -1, s));
         // true residual r = b - A x (FP64) into V_0, then cycle decisions on device
         CG_LAUNCH(launch_rows_forward(0, a64, xs, nullptr, nullptr, GATE_NONE, s));
         CG_LAUNCH(launch_cols_convolve(0, a64, nullptr, GATE_NONE, s));
         CG_LAUNCH(launch_rows_inverse(0, 1, prec, a64, xs, nullptr, bp, fixed_vec(c->V), kp.npart, nullptr, GATE_NONE, s));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_RESIDUAL, -1, s));
         CG_LAUNCH(launch_cycle_begin(kp, nrb, s));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, s));
         CG_CU(cudaMemcpyAsync(c->st_host, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
         CG_CU(cudaEventRecord(c->ev, s));
         CG_CU(cudaEventSynchronize(c->ev));
         const DevState hs = *c->st_host;
+        CG_TRY(prof_collect(c, cp, nd, esz, hs.it - it_prev));
+        it_prev = hs.it;
         if (hs.status != 0) break;
         if (o.timeout_s > 0.0 && now_s() - t0 > o.timeout_s) {
             status = CG_ERR_TIMEOUT;
             break;
         }
+        CG_TRY(prof_mark(c, cp, -1, -1, s));
         const int steps = std::min(m, o.max_iter - hs.it);
         for (int i = 0; i < steps; i++) {
             CG_LAUNCH(launch_rows_forward(prec, ap, vk, kp.scale, c->st, GATE_STOP, s));
             CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, s));
             CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, kp.scale, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, s));
             CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h1, 0, ndot, GATE_STOP, s));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
             CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h1, -1.0, NJ_K_PLUS_1, vk1, 0, 1, nax, GATE_STOP, s));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
             CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h2, 0, ndot, GATE_STOP, s));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
             CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h2, -1.0, NJ_K_PLUS_1, vk1, 1, 1, nax, GATE_STOP, s));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
             CG_LAUNCH(launch_givens(kp, s));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, s));
         }
         CG_LAUNCH(launch_backsolve(kp, s));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, s));
         CG_LAUNCH(launch_axpy(prec, 0, c->V, n, kp, kp.y, 1.0, NJ_K, xs, 0, 1, nax, GATE_NONE, s));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, s));
     }
 
     const DevState hs = *c->st_host;

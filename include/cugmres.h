@@ -127,6 +127,28 @@ int cugmres_residual(cg_ctx *ctx, const cg_c128 *b, const cg_c128 *x, cg_c128 *r
 int cugmres_solve(cg_ctx *ctx, const cg_c128 *b, cg_c128 *x, const cg_opts *opts, double *res_hist,
                   int res_hist_len, cg_result *result);
 
+/* Per-phase device timing of cugmres_solve, the counterpart of the reference's
+ * clock_gettime step stamps (CUDA_GMRES/GMRES.cuh:39-445, labels in
+ * launch_GMRES.cuh:245-307): CUDA events recorded between kernel groups on the
+ * context's stream, plus the algorithmic HBM bytes each phase moves
+ * (e = element bytes of the phase's precision, n = N*N):
+ *   MATVEC    Arnoldi operator application, 16 n e per matvec
+ *   DOTS      V^H w for k+1 basis vectors, (k+2) n e per launch
+ *   AXPY      w -= V h, (k+3) n e per launch
+ *   SMALL     Givens / back-substitution / cycle bookkeeping (no bulk bytes)
+ *   UPDATE    x += V y, (k + 2 * 16/e) n e per cycle
+ *   RESIDUAL  FP64 r = b - A x per cycle, 16 n 16 (model of one FP64 matvec)
+ * Enabling resets the counters; they accumulate over solves while enabled. */
+enum { CG_PHASE_MATVEC = 0, CG_PHASE_DOTS, CG_PHASE_AXPY, CG_PHASE_SMALL, CG_PHASE_UPDATE, CG_PHASE_RESIDUAL,
+       CG_NPHASES };
+typedef struct {
+    double ms;          /* summed device time                 */
+    double bytes;       /* summed algorithmic bytes           */
+    long long launches; /* kernel groups timed                */
+} cg_phase_stats;
+int cugmres_profile(cg_ctx *ctx, int enable);
+int cugmres_profile_read(cg_ctx *ctx, cg_phase_stats *out /* CG_NPHASES entries */);
+
 /* Drop-in for the reference's Fast_GMRES_with_CUDA (CUDA_GMRES/GMRES.cuh:22-35):
  * same iteration semantics (exactly maxiter Arnoldi steps, no restart,
  * absolute `tolerance` gating the first step, the reference's Givens

@@ -151,7 +151,7 @@ def gmres_reference(ghat, chi, b, x0, maxiter, tol, precision="c128"):
 def gmres(ghat, chi, b, x0=None, restart=100, maxiter=1000, tol=1e-10, ortho="mgs",
           rotation="unitary", precision="c128"):
     """Restarted GMRES(m) with early exit on the relative residual estimate.
-    Returns dict(x, res_hist, iters, cycles, true_res, status)."""
+    Returns dict(x, res_hist, iterations, cycles, true_res, status)."""
     sfx, ct, rt = _types(precision)
     ghat = np.ascontiguousarray(ghat, dtype=ct)
     chi = np.ascontiguousarray(chi, dtype=rt)
@@ -164,7 +164,7 @@ def gmres(ghat, chi, b, x0=None, restart=100, maxiter=1000, tol=1e-10, ortho="mg
         int(maxiter), float(tol), {"mgs": 0, "cgs2": 1}[ortho],
         {"reference": 0, "unitary": 1}[rotation], _ptr(hist), ctypes.byref(it),
         ctypes.byref(cyc), ctypes.byref(tr))
-    return dict(x=x, res_hist=hist[: it.value + 1], iters=it.value, cycles=cyc.value,
+    return dict(x=x, res_hist=hist[: it.value + 1], iterations=it.value, cycles=cyc.value,
                 true_res=tr.value, status=st)
 
 
