@@ -30,6 +30,7 @@ __all__ = ["Solver", "CugmresError", "green_block", "helmholtz", "reference_cyli
 
 _PREC = {"fp64": _lib.CG_PREC_FP64, "mixed": _lib.CG_PREC_MIXED, "fp32": _lib.CG_PREC_MIXED}
 _GIV = {"unitary": _lib.CG_GIVENS_UNITARY, "reference": _lib.CG_GIVENS_REFERENCE}
+_ORTHO = {"dcgs2": _lib.CG_ORTHO_DCGS2, "cgs2": _lib.CG_ORTHO_CGS2}
 
 
 def _is_torch(a):
@@ -148,7 +149,7 @@ class Solver:
         return r, rel.value
 
     def solve(self, b, x0=None, restart=100, max_iter=10000, tol=1e-10, precision="fp64", givens="unitary",
-              inner_tol=1e-5, fixed_iterations=False, timeout_s=0.0, raise_on_failure=False):
+              inner_tol=1e-5, fixed_iterations=False, timeout_s=0.0, ortho="dcgs2", raise_on_failure=False):
         """Solve A x = b.  Returns (x, info) where info holds status, iterations,
         cycles, rel_residual_true / _estimate, seconds and res_hist."""
         o = _lib.CgOpts()
@@ -161,6 +162,7 @@ class Solver:
         o.inner_tol = float(inner_tol)
         o.fixed_iterations = int(bool(fixed_iterations))
         o.timeout_s = float(timeout_s)
+        o.ortho = _ORTHO[ortho]
         bp, bk = _arg(b, np.complex128)
         if x0 is None:
             o.zero_x0 = 1

@@ -23,6 +23,8 @@ CG_ERR_OOM = 9
 CG_PREC_FP64 = 0
 CG_PREC_MIXED = 1
 CG_GIVENS_UNITARY = 0
+CG_ORTHO_DCGS2 = 0
+CG_ORTHO_CGS2 = 1
 CG_GIVENS_REFERENCE = 1
 CG_GREEN_HELMHOLTZ = 0
 CG_GREEN_REFERENCE = 1
@@ -50,7 +52,8 @@ class CgOpts(ctypes.Structure):
         ("zero_x0", ctypes.c_int),
         ("fixed_iterations", ctypes.c_int),
         ("timeout_s", ctypes.c_double),
-        ("reserved", ctypes.c_int * 8),
+        ("ortho", ctypes.c_int),
+        ("reserved", ctypes.c_int * 7),
     ]
 
 

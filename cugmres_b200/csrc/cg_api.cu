@@ -184,6 +184,12 @@ void free_krylov(cg_ctx *c) {
     dfree_t(c->kp.hist);
     dfree_t(c->kp.part);
     dfree_t(c->kp.npart);
+    dfree_t(c->kp.Hm);
+    dfree_t(c->kp.D1);
+    dfree_t(c->kp.D2);
+    dfree_t(c->kp.tv);
+    dfree_t(c->kp.P);
+    dfree_t(c->kp.S);
     c->mcap = 0;
     c->itcap = 0;
     c->vcap_bytes = 0;
@@ -213,8 +219,16 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
         CG_CU(cudaMalloc((void **)&c->kp.g, sizeof(double2) * (mc + 1)));
         CG_CU(cudaMalloc((void **)&c->kp.y, sizeof(double2) * mc));
         CG_CU(cudaMalloc((void **)&c->kp.hist, sizeof(double) * (ic + 1)));
-        CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * 2 * (size_t)dot_blocks(c) * (mc + 1)));
+        const size_t part_cgs2 = 2 * (size_t)dot_blocks(c) * (mc + 1);
+        const size_t part_dcgs2 = 4 * (size_t)dots2_blocks(c->sms) * (size_t)std::max(mc + 1, 32);
+        CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(part_cgs2, part_dcgs2)));
         CG_CU(cudaMalloc((void **)&c->kp.npart, sizeof(double) * np));
+        CG_CU(cudaMalloc((void **)&c->kp.Hm, sizeof(double2) * (size_t)(mc + 1) * (mc + 1)));
+        CG_CU(cudaMalloc((void **)&c->kp.D1, sizeof(double2) * (mc + 2)));
+        CG_CU(cudaMalloc((void **)&c->kp.D2, sizeof(double2) * (mc + 2)));
+        CG_CU(cudaMalloc((void **)&c->kp.tv, sizeof(double2) * (mc + 2)));
+        CG_CU(cudaMalloc((void **)&c->kp.P, sizeof(double2) * (mc + 1)));
+        CG_CU(cudaMalloc((void **)&c->kp.S, sizeof(double2) * (mc + 1)));
         c->mcap = mc;
         c->itcap = ic;
         c->vcap_bytes = vb;
@@ -294,7 +308,7 @@ int prof_mark(cg_ctx *c, CycleProf &cp, int phase, int iter, cudaStream_t s) {
 // Called once the stream has passed every recorded event.  steps_done: Arnoldi
 // steps that did work in the cycle these events cover (later steps were gated
 // off on device and move no bytes); e: element bytes of the cycle precision.
-int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done) {
+int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed) {
     if (c->prof && cp.used >= 2) {
         for (int i = 0; i + 1 < cp.used; i++) {
             float ms = 0.f;
@@ -305,8 +319,8 @@ int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done) {
             switch (t) {
                 case CG_PHASE_MATVEC: bytes = live ? 16.0 * n * e : 0.0; break;
                 case CG_PHASE_DOTS: bytes = live ? (k + 2.0) * n * e : 0.0; break;
-                case CG_PHASE_AXPY: bytes = live ? (k + 3.0) * n * e : 0.0; break;
-                case CG_PHASE_UPDATE: bytes = steps_done * n * e + 2.0 * n * 16.0; break;
+                case CG_PHASE_AXPY: bytes = live ? (k + (delayed ? 4.0 : 3.0)) * n * e : 0.0; break;
+                case CG_PHASE_UPDATE: bytes = (steps_done - (delayed ? 1 : 0)) * n * e + 2.0 * n * 16.0; break;
                 case CG_PHASE_RESIDUAL: bytes = 16.0 * n * 16.0; break;
                 default: bytes = 0.0;
             }
@@ -364,6 +378,7 @@ void cugmres_default_opts(cg_opts *o) {
     o->zero_x0 = 0;
     o->fixed_iterations = 0;
     o->timeout_s = 0.0;
+    o->ortho = CG_ORTHO_DCGS2;
 }
 
 int cugmres_create(cg_ctx **out, int device) {
@@ -602,10 +617,11 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     if (opts_in) o = *opts_in;
     else cugmres_default_opts(&o);
     if (o.restart < 1 || o.max_iter < 0 || !(o.tol >= 0.0) || (o.precision != CG_PREC_FP64 && o.precision != CG_PREC_MIXED) ||
-        (o.givens != CG_GIVENS_UNITARY && o.givens != CG_GIVENS_REFERENCE))
+        (o.givens != CG_GIVENS_UNITARY && o.givens != CG_GIVENS_REFERENCE) ||
+        (o.ortho != CG_ORTHO_DCGS2 && o.ortho != CG_ORTHO_CGS2))
         return CG_ERR_INVALID;
-    // coefficient arrays of k_axpy / k_backsolve live in 48 KB of shared memory
-    if (o.restart > 3000 || (o.fixed_iterations && o.max_iter > 3000)) return CG_ERR_NOT_IMPLEMENTED;
+    // per-cycle coefficient arrays live in shared memory (<= 227 KB per block)
+    if (o.restart > 4500 || (o.fixed_iterations && o.max_iter > 4500)) return CG_ERR_NOT_IMPLEMENTED;
     CG_CU(cudaSetDevice(c->device));
     const int prec = o.precision == CG_PREC_FP64 ? 0 : 1;
     const int m = o.fixed_iterations ? std::max(1, o.max_iter) : o.restart;
@@ -639,6 +655,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     h.fixed = o.fixed_iterations ? 1 : 0;
     h.tol = o.tol;
     h.inner_tol = prec == 1 ? o.inner_tol : 0.0;
+    h.ortho = o.ortho == CG_ORTHO_CGS2 ? 1 : 0;
+    const bool delayed = h.ortho == 0;
     *c->st_host = h;
     CG_CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(DevState), cudaMemcpyHostToDevice, s));
     CG_LAUNCH(launch_norm2(0, bp, n, c->kp.npart, &c->st->counter[2], &c->st->nb, axpy_blocks(c, n), s));
@@ -654,7 +672,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     vk1.koff = 1;
     VecSel xs = fixed_vec(xp);
     const int nrb = row_blocks(c);
-    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n);
+    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(c->sms);
     int status = CG_OK;
 
     CycleProf cp;
@@ -673,7 +691,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_CU(cudaEventRecord(c->ev, s));
         CG_CU(cudaEventSynchronize(c->ev));
         const DevState hs = *c->st_host;
-        CG_TRY(prof_collect(c, cp, nd, esz, hs.it - it_prev));
+        CG_TRY(prof_collect(c, cp, nd, esz, hs.it - it_prev + (delayed ? 1 : 0), delayed));
         it_prev = hs.it;
         if (hs.status != 0) break;
         if (o.timeout_s > 0.0 && now_s() - t0 > o.timeout_s) {
@@ -681,8 +699,22 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             break;
         }
         CG_TRY(prof_mark(c, cp, -1, -1, s));
-        const int steps = std::min(m, o.max_iter - hs.it);
+        const int steps = std::min(m, o.max_iter - hs.it) + (delayed ? 1 : 0);
         for (int i = 0; i < steps; i++) {
+            if (delayed) {
+                // w = A u_k into V[k+1]; one dot pass; normalisation + Givens; one axpy pass
+                CG_LAUNCH(launch_rows_forward(prec, ap, vk, nullptr, c->st, GATE_STOP, s));
+                CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, s));
+                CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, nullptr, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, s));
+                CG_LAUNCH(launch_dots2(prec, c->V, n, kp, ndot2, s));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
+                CG_LAUNCH(launch_dcgs2_step(kp, s));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, s));
+                CG_LAUNCH(launch_axpy2(prec, c->V, n, kp, nax, s));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
+                continue;
+            }
             CG_LAUNCH(launch_rows_forward(prec, ap, vk, kp.scale, c->st, GATE_STOP, s));
             CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, s));
             CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, kp.scale, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
@@ -700,7 +732,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         }
         CG_LAUNCH(launch_backsolve(kp, s));
         CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, s));
-        CG_LAUNCH(launch_axpy(prec, 0, c->V, n, kp, kp.y, 1.0, NJ_K, xs, 0, 1, nax, GATE_NONE, s));
+        CG_LAUNCH(launch_axpy(prec, 0, c->V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, s));
         CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, s));
     }
 

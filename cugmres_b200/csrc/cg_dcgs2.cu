@@ -1,0 +1,441 @@
+// Arnoldi with classical Gram-Schmidt and delayed reorthogonalisation.
+//
+// CGS2 reads the basis four times per Arnoldi step (h1 = V^H w, w -= V h1,
+// h2 = V^H w, w -= V h2).  Here the second (re)orthogonalisation pass of
+// each vector is delayed by one step and merged with the first pass of the
+// next one (the "DCGS2" scheme of Swirydowicz, Langou, Ananthan, Yang and
+// Thomas, "Low synchronization Gram-Schmidt and GMRES algorithms", Numer.
+// Linear Algebra Appl. 28 (2021), and Bielich et al., Parallel Computing 112
+// (2022)), so each step reads the basis twice.  Notation of step k
+// (q_0..q_{k-1} orthonormal, u_k = A q_{k-1} projected once, not yet
+// reorthogonalised nor normalised; slot V[k] holds u_k):
+//
+//   w = A u_k                                   (matvec into slot V[k+1])
+//   one dot pass:  a = Q^H u_k, alpha = u_k^H u_k, c = Q^H w, d = u_k^H w
+//   nu = sqrt(alpha - |a|^2),  q_k = (u_k - Q a) / nu
+//   column k-1 of H:  H(0:k, k-1) = t_{k-1} + a,  H(k, k-1) = nu
+//   delta = (d - a^H c) / nu  (= q_k^H w)
+//   u_{k+1} = (w - Q c - q_k delta) / nu        (A q_k projected once)
+//   t_k = ([c; delta] - H(0:k, 0:k-1) a) / nu  (first-pass coefficients of A q_k)
+//   one axpy pass writes q_k into V[k] and u_{k+1} into V[k+1]; its blocks
+//   also evaluate the O(k^2) product H a for t_k (a warp per row of H).
+//
+// Step 0 uses u_0 = r (the residual the cycle starts from), so nu_0 = ||r||.
+// Column k-1 is final only at step k, so the Givens update of the least-
+// squares problem runs one step behind and a cycle of m columns makes m+1
+// operator applications.  The identities assume Q orthonormal; they were
+// checked against plain CGS2 (Q and H agree to 2e-15).
+#include "cg_common.cuh"
+#include "cg_internal.h"
+
+namespace cg {
+
+static constexpr int D2_THREADS = 256;
+static constexpr int D2_WARPS = D2_THREADS / 32;
+static constexpr int D2_J = 4;  // basis vectors per warp work item
+static constexpr int AX2_THREADS = 256;
+static constexpr int STEP_THREADS = 256;
+
+int dots2_blocks(int sms) { return 4 * sms; }
+
+static __device__ __forceinline__ int part_ld(const KrylovPtrs &kp) {
+    return kp.mcap + 1 > 32 ? kp.mcap + 1 : 32;
+}
+
+static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int t = atomicAdd(ticket, 1u);
+        is_last = (t == gridDim.x - 1);
+        if (is_last) *ticket = 0u;
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// --------------------------------------------------------------- dots2
+// For j = 0..k: D1[j] = <V_j, u_k>, D2[j] = <V_j, w> with u_k = V[k], w = V[k+1].
+// Work items: groups of D2_J basis vectors; when there are fewer groups than
+// warps, each group's element range is split into S slices.
+template <typename CV, bool COMP>
+__global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int nj = k + 1;
+    const CV *u = V + (long long)k * n;
+    const CV *w = V + (long long)(k + 1) * n;
+    long long chunk = (n + gridDim.x - 1) / gridDim.x;
+    chunk = (chunk + 31) & ~31LL;
+    const long long b0 = (long long)blockIdx.x * chunk < n ? (long long)blockIdx.x * chunk : n;
+    const long long b1 = b0 + chunk < n ? b0 + chunk : n;
+    const int ng = (nj + D2_J - 1) / D2_J;
+    const int S = ng >= D2_WARPS ? 1 : D2_WARPS / ng;
+    const int items = ng * S;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pld = part_ld(kp);
+    for (int it = warp; it < items; it += D2_WARPS) {
+        const int grp = it / S, sl = it % S;
+        const int j0 = grp * D2_J;
+        const int jn = nj - j0 < D2_J ? nj - j0 : D2_J;
+        long long sc = (b1 - b0 + S - 1) / S;
+        sc = (sc + 31) & ~31LL;
+        const long long e0 = b0 + sl * sc < b1 ? b0 + sl * sc : b1;
+        const long long e1 = e0 + sc < b1 ? e0 + sc : b1;
+        const CV *vj[D2_J];
+#pragma unroll
+        for (int q = 0; q < D2_J; q++) vj[q] = V + (long long)(j0 + (q < jn ? q : 0)) * n;
+        double out[D2_J][4];
+        if constexpr (COMP) {
+            // FP32 products accumulated with FMA over runs of 8 elements, each
+            // run folded into a compensated (TwoSum) FP32 accumulator
+            Acc2f acc[D2_J][4];
+#pragma unroll
+            for (int q = 0; q < D2_J; q++)
+#pragma unroll
+                for (int r = 0; r < 4; r++) acc[q][r].zero();
+            long long e = e0 + lane;
+            while (e < e1) {
+                float run[D2_J][4];
+#pragma unroll
+                for (int q = 0; q < D2_J; q++)
+#pragma unroll
+                    for (int r = 0; r < 4; r++) run[q][r] = 0.f;
+#pragma unroll 2
+                for (int t = 0; t < 8 && e < e1; t++, e += 32) {
+                    const CV uu = u[e], ww = w[e];
+#pragma unroll
+                    for (int q = 0; q < D2_J; q++) {
+                        if (q < jn) {
+                            const CV a = vj[q][e];
+                            run[q][0] = fmaf(a.x, uu.x, fmaf(a.y, uu.y, run[q][0]));
+                            run[q][1] = fmaf(a.x, uu.y, fmaf(-a.y, uu.x, run[q][1]));
+                            run[q][2] = fmaf(a.x, ww.x, fmaf(a.y, ww.y, run[q][2]));
+                            run[q][3] = fmaf(a.x, ww.y, fmaf(-a.y, ww.x, run[q][3]));
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < D2_J; q++)
+#pragma unroll
+                    for (int r = 0; r < 4; r++) acc[q][r].add(run[q][r]);
+            }
+#pragma unroll
+            for (int q = 0; q < D2_J; q++)
+#pragma unroll
+                for (int r = 0; r < 4; r++) {
+                    Acc2f t = warp_sum(acc[q][r]);
+                    out[q][r] = (double)t.hi + (double)t.lo;
+                }
+        } else {
+            typedef typename real_of<CV>::type R;
+            R acc[D2_J][4];
+#pragma unroll
+            for (int q = 0; q < D2_J; q++)
+#pragma unroll
+                for (int r = 0; r < 4; r++) acc[q][r] = 0;
+            long long e = e0 + lane;
+            for (; e + 32 < e1; e += 64) {
+                const CV u0 = u[e], w0 = w[e], u1 = u[e + 32], w1 = w[e + 32];
+#pragma unroll
+                for (int q = 0; q < D2_J; q++) {
+                    if (q < jn) {
+                        const CV a0 = vj[q][e], a1 = vj[q][e + 32];
+                        acc[q][0] += a0.x * u0.x + a0.y * u0.y + (a1.x * u1.x + a1.y * u1.y);
+                        acc[q][1] += a0.x * u0.y - a0.y * u0.x + (a1.x * u1.y - a1.y * u1.x);
+                        acc[q][2] += a0.x * w0.x + a0.y * w0.y + (a1.x * w1.x + a1.y * w1.y);
+                        acc[q][3] += a0.x * w0.y - a0.y * w0.x + (a1.x * w1.y - a1.y * w1.x);
+                    }
+                }
+            }
+            if (e < e1) {
+                const CV u0 = u[e], w0 = w[e];
+#pragma unroll
+                for (int q = 0; q < D2_J; q++) {
+                    if (q < jn) {
+                        const CV a0 = vj[q][e];
+                        acc[q][0] += a0.x * u0.x + a0.y * u0.y;
+                        acc[q][1] += a0.x * u0.y - a0.y * u0.x;
+                        acc[q][2] += a0.x * w0.x + a0.y * w0.y;
+                        acc[q][3] += a0.x * w0.y - a0.y * w0.x;
+                    }
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < D2_J; q++)
+#pragma unroll
+                for (int r = 0; r < 4; r++) out[q][r] = warp_sum((double)acc[q][r]);
+        }
+        if (lane == 0) {
+            for (int q = 0; q < jn; q++) {
+                double *p = kp.part + 4 * ((size_t)blockIdx.x * pld + (size_t)sl * nj + j0 + q);
+                p[0] = out[q][0];
+                p[1] = out[q][1];
+                p[2] = out[q][2];
+                p[3] = out[q][3];
+            }
+        }
+    }
+    if (last_block2(&st->counter[3])) {
+        // warp per coefficient, lanes stride the block partials, fixed-order butterfly
+        const int nparts = (int)gridDim.x * S;
+        for (int j = warp; j < nj; j += D2_WARPS) {
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            for (int pi = lane; pi < nparts; pi += 32) {
+                const int b = pi / S, sl = pi % S;
+                const double *p = kp.part + 4 * ((size_t)b * pld + (size_t)sl * nj + j);
+                s0 += __ldcg(p);
+                s1 += __ldcg(p + 1);
+                s2 += __ldcg(p + 2);
+                s3 += __ldcg(p + 3);
+            }
+            s0 = warp_sum(s0);
+            s1 = warp_sum(s1);
+            s2 = warp_sum(s2);
+            s3 = warp_sum(s3);
+            if (lane == 0) {
+                kp.D1[j] = make_double2(s0, s1);
+                kp.D2[j] = make_double2(s2, s3);
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------- the step
+static __device__ __forceinline__ double block_sum(double v, double *red) {
+    v = warp_sum(v);
+    __syncthreads();
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    double t = 0.0;
+    for (int i = 0; i < STEP_THREADS / 32; i++) t += red[i];
+    return t;
+}
+
+// One block: normalisation of q_k, column k-1 of H, Givens update, residual
+// estimate, stop decision and the coefficients of the axpy pass.
+__global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
+    DevState *st = kp.st;
+    if (st->stop) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    __shared__ double red[STEP_THREADS / 32];
+    __shared__ int flag;
+    const int k = st->k;
+    const int ld = kp.mcap + 1;
+    const int tid = threadIdx.x;
+    double2 *col = reinterpret_cast<double2 *>(smraw);  // k+1 entries
+    double2 *css = col + (kp.mcap + 2);                // k entries
+    double *sns = reinterpret_cast<double *>(css + (kp.mcap + 1));
+    double sa = 0.0, acr = 0.0, aci = 0.0;
+    for (int j = tid; j < k; j += STEP_THREADS) {
+        const double2 a = kp.D1[j], c = kp.D2[j];
+        sa += a.x * a.x + a.y * a.y;
+        acr += a.x * c.x + a.y * c.y;  // conj(a) c
+        aci += a.x * c.y - a.y * c.x;
+    }
+    sa = block_sum(sa, red);
+    acr = block_sum(acr, red);
+    aci = block_sum(aci, red);
+    const double alpha = kp.D1[k].x;
+    const double2 d = kp.D2[k];
+    const double nu2 = alpha - sa;
+    if (tid == 0) {
+        int f = 0;
+        if (!isfinite(nu2) || !isfinite(acr) || !isfinite(aci) || !isfinite(d.x) || !isfinite(d.y)) f = 2;
+        else if (!(nu2 > 1e-28 * alpha) || !(alpha > 0.0)) f = 1;
+        flag = f;
+    }
+    __syncthreads();
+    if (flag) {
+        if (tid == 0) {
+            if (flag == 2) st->status = 4;
+            else st->brk = 1;
+            st->stop = 1;
+        }
+        return;
+    }
+    const double nu = sqrt(nu2);
+    const double inu = 1.0 / nu;
+    const double2 delta = make_double2((d.x - acr) * inu, (d.y - aci) * inu);
+    if (k >= 1) {
+        // column k-1 of H = t + a (rows 0..k-1), nu (row k); H is stored row-major
+        for (int i = tid; i < k; i += STEP_THREADS) {
+            const double2 h = cadd(kp.tv[i], kp.D1[i]);
+            col[i] = h;
+            kp.Hm[(size_t)i * ld + (k - 1)] = h;
+        }
+        if (tid == 0) {
+            col[k] = make_double2(nu, 0.0);
+            kp.Hm[(size_t)k * ld + (k - 1)] = make_double2(nu, 0.0);
+        }
+        for (int j = tid; j < k - 1; j += STEP_THREADS) {
+            css[j] = kp.cs[j];
+            sns[j] = kp.sn[j];
+        }
+    }
+    __syncthreads();
+    // axpy coefficients P = a / nu, S = c / nu - delta a / nu^2; t_k is finished by k_axpy2
+    for (int i = tid; i < k; i += STEP_THREADS) {
+        const double2 a = kp.D1[i], c = kp.D2[i];
+        kp.P[i] = make_double2(a.x * inu, a.y * inu);
+        const double2 da = cmul(delta, a);
+        kp.S[i] = make_double2((c.x - da.x * inu) * inu, (c.y - da.y * inu) * inu);
+    }
+    if (tid == 0) {
+        st->cu = inu;
+        st->cw = inu;
+        st->du = make_double2(-delta.x * inu * inu, -delta.y * inu * inu);
+        st->delta = delta;
+        int stop = 0;
+        if (k == 0) {
+            kp.g[0] = make_double2(nu, 0.0);
+        } else {
+            // Givens: rotations 0..k-2 on col[0..k-1], new rotation from (col[k-1], nu)
+            const bool ref = st->rotation == 1;
+            double2 carry = col[0];
+            for (int j = 0; j < k - 1; j++) {
+                const double2 nx = col[j + 1];
+                const double2 c = css[j];
+                const double s = sns[j];
+                col[j] = cadd(cmul(ref ? c : cconj(c), carry), cscale(nx, s));
+                carry = csub(cmul(c, nx), cscale(carry, s));
+            }
+            const double rho = hypot(hypot(carry.x, carry.y), nu);
+            double2 c;
+            double s;
+            if (!(rho > 0.0) || !isfinite(rho)) {
+                c = make_double2(1.0, 0.0);
+                s = 0.0;
+            } else {
+                c = make_double2(carry.x / rho, carry.y / rho);
+                s = nu / rho;
+            }
+            const double2 cc = ref ? c : cconj(c);
+            col[k - 1] = cadd(cmul(cc, carry), make_double2(s * nu, 0.0));
+            kp.cs[k - 1] = c;
+            kp.sn[k - 1] = s;
+            const double2 gk = kp.g[k - 1];
+            kp.g[k] = cscale(gk, -s);
+            kp.g[k - 1] = cmul(cc, gk);
+            const int it = st->it + 1;
+            st->it = it;
+            const double gabs = hypot(gk.x, gk.y) * s;
+            st->est = gabs / st->nb;
+            kp.hist[it] = st->est;
+            st->ncol = k;
+            if (!st->fixed && (gabs <= st->tol * st->nb || gabs <= st->inner_tol * st->beta0)) stop = 1;
+            if (k >= st->m) stop = 1;
+            if (it >= st->maxit) stop = 1;
+        }
+        st->k = k + 1;
+        st->stop = stop;
+    }
+    __syncthreads();
+    if (k >= 1)
+        for (int i = tid; i < k; i += STEP_THREADS) kp.Rm[(size_t)(k - 1) * ld + i] = col[i];
+}
+
+// --------------------------------------------------------------- axpy2
+// q_k = cu u - sum_j P_j q_j into V[k];  u_{k+1} = cw w + du u - sum_j S_j q_j into V[k+1]
+// (k = st->k - 1: the step kernel has advanced the index).
+template <typename CV>
+__global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    typedef typename real_of<CV>::type R;
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k - 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    CV *Pc = reinterpret_cast<CV *>(smraw);
+    CV *Sc = Pc + (kp.mcap + 1);
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+        const double2 p = kp.P[j], q = kp.S[j];
+        Pc[j] = mk<CV>((R)p.x, (R)p.y);
+        Sc[j] = mk<CV>((R)q.x, (R)q.y);
+    }
+    const R cu = (R)st->cu, cw = (R)st->cw;
+    const CV du = mk<CV>((R)st->du.x, (R)st->du.y);
+    {
+        // t_k = ([c; delta] - H(0:k, 0:k-1) a) / nu, one warp per row of H
+        const int ld = kp.mcap + 1;
+        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+        const double inu = st->cu;
+        for (int i = blockIdx.x * (AX2_THREADS / 32) + warp; i <= k; i += gridDim.x * (AX2_THREADS / 32)) {
+            double er = 0.0, ei = 0.0;
+            for (int j = (i > 0 ? i - 1 : 0) + lane; j < k; j += 32) {
+                const double2 h = kp.Hm[(size_t)i * ld + j];
+                const double2 a = kp.D1[j];
+                er += h.x * a.x - h.y * a.y;
+                ei += h.x * a.y + h.y * a.x;
+            }
+            er = warp_sum(er);
+            ei = warp_sum(ei);
+            if (lane == 0) {
+                const double2 c = i < k ? kp.D2[i] : st->delta;
+                kp.tv[i] = make_double2((c.x - er) * inu, (c.y - ei) * inu);
+            }
+        }
+    }
+    __syncthreads();
+    CV *u = V + (long long)k * n;
+    CV *w = V + (long long)(k + 1) * n;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
+        const CV uu = u[e], ww = w[e];
+        CV sp = czero<CV>(), ss = czero<CV>();
+        int j = 0;
+        for (; j + 4 <= k; j += 4) {
+            const CV q0 = V[(long long)j * n + e], q1 = V[(long long)(j + 1) * n + e];
+            const CV q2 = V[(long long)(j + 2) * n + e], q3 = V[(long long)(j + 3) * n + e];
+            sp = cadd(sp, cadd(cadd(cmul(Pc[j], q0), cmul(Pc[j + 1], q1)), cadd(cmul(Pc[j + 2], q2), cmul(Pc[j + 3], q3))));
+            ss = cadd(ss, cadd(cadd(cmul(Sc[j], q0), cmul(Sc[j + 1], q1)), cadd(cmul(Sc[j + 2], q2), cmul(Sc[j + 3], q3))));
+        }
+        for (; j < k; j++) {
+            const CV q0 = V[(long long)j * n + e];
+            sp = cadd(sp, cmul(Pc[j], q0));
+            ss = cadd(ss, cmul(Sc[j], q0));
+        }
+        u[e] = csub(cscale(uu, cu), sp);
+        w[e] = csub(cadd(cscale(ww, cw), cmul(du, uu)), ss);
+    }
+}
+
+// ------------------------------------------------------------- launchers
+int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s) {
+    if (prec_v == 0) k_dots2<double2, false><<<nblk, D2_THREADS, 0, s>>>((const double2 *)V, n, kp);
+    else k_dots2<float2, true><<<nblk, D2_THREADS, 0, s>>>((const float2 *)V, n, kp);
+    return (int)cudaGetLastError();
+}
+
+int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s) {
+    const size_t smem = (size_t)(kp.mcap + 2) * sizeof(double2) + (size_t)(kp.mcap + 1) * sizeof(double2) +
+                        (size_t)(kp.mcap + 1) * sizeof(double);
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(k_dcgs2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return (int)e;
+    }
+    k_dcgs2_step<<<1, STEP_THREADS, smem, s>>>(kp);
+    return (int)cudaGetLastError();
+}
+
+int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s) {
+    const size_t smem = 2 * (size_t)(kp.mcap + 1) * (prec_v == 0 ? sizeof(double2) : sizeof(float2));
+    if (prec_v == 0) {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_axpy2<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return (int)e;
+        }
+        k_axpy2<double2><<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
+    } else {
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(k_axpy2<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return (int)e;
+        }
+        k_axpy2<float2><<<nblk, AX2_THREADS, smem, s>>>((float2 *)V, n, kp);
+    }
+    return (int)cudaGetLastError();
+}
+
+}  // namespace cg

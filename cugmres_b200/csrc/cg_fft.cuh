@@ -186,7 +186,7 @@ template <bool INV, typename C> __device__ __forceinline__ C twiddle(const C *__
 // One Stockham stage S of a length-L transform (compile-time radix and span).
 // tmp holds the previous stage's butterfly outputs (tmp[b*Rp + q]) on entry
 // and this stage's outputs on exit; the last stage stores canonical reg.
-template <int L, bool INV, bool HALF_IN, int S> struct Stage {
+template <int L, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
     typedef Plan<L> P;
     static constexpr int E = P::E;
     static constexpr int TPR = P::TPR;
@@ -206,7 +206,7 @@ template <int L, bool INV, bool HALF_IN, int S> struct Stage {
                 const int j = t + b * TPR;
                 const int base = (j / Nsp) * Nsp * Rp + (j % Nsp);
 #pragma unroll
-                for (int q = 0; q < Rp; q++) sm[P::pad(base + q * Nsp)] = tmp[b * Rp + q];
+                for (int q = 0; q < Rp; q++) sm[P::pad(base + q * Nsp) * SMS] = tmp[b * Rp + q];
             }
             __syncthreads();
 #pragma unroll
@@ -216,7 +216,7 @@ template <int L, bool INV, bool HALF_IN, int S> struct Stage {
                 constexpr int step = L / (Ns * R);
 #pragma unroll
                 for (int r = 0; r < R; r++) {
-                    C v = sm[P::pad(j + r * (L / R))];
+                    C v = sm[P::pad(j + r * (L / R)) * SMS];
                     if (r > 0) v = cmul(v, twiddle<INV>(tw, k * r * step));
                     tmp[b * R + r] = v;
                 }
@@ -238,21 +238,23 @@ template <int L, bool INV, bool HALF_IN, int S> struct Stage {
 #pragma unroll
                 for (int q = 0; q < R; q++) reg[b + q * NB] = tmp[b * R + q];
         } else {
-            Stage<L, INV, HALF_IN, S + 1>::run(reg, tmp, sm, tw, t);
+            Stage<L, INV, HALF_IN, S + 1, SMS>::run(reg, tmp, sm, tw, t);
         }
     }
 };
 
 // Runs one length-L transform owned by TPR threads (this thread is t).
 // reg[p] holds element t + p*TPR on entry and on exit.  sm is this
-// transform's padded shared-memory region (Plan<L>::SMEM_ELEMS elements).
+// transform's padded shared-memory region: element i lives at sm[pad(i) * SMS]
+// (SMS > 1 interleaves the regions of SMS transforms element by element, which
+// keeps the column kernels' accesses on distinct banks).
 // HALF_IN: inputs L/2 .. L-1 are zero (first stage uses dft_half_input).
 // Every thread of the block must call this the same number of times
 // (it contains __syncthreads()).
-template <int L, bool INV, bool HALF_IN, typename C>
+template <int L, bool INV, bool HALF_IN, int SMS = 1, typename C>
 __device__ __forceinline__ void fft_run(C (&reg)[Plan<L>::E], C *sm, const C *__restrict__ tw, int t) {
     C tmp[Plan<L>::E];
-    Stage<L, INV, HALF_IN, 0>::run(reg, tmp, sm, tw, t);
+    Stage<L, INV, HALF_IN, 0, SMS>::run(reg, tmp, sm, tw, t);
 }
 
 }  // namespace cg

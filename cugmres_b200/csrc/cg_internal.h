@@ -22,7 +22,8 @@ struct DevState {
     int fixed;     // 1: never stop on the residual estimate (reference semantics)
     int cycles;    // cycles started
     int brk;       // breakdown seen in this cycle
-    int pad0, pad1;
+    int ncol;      // Hessenberg columns finalised in this cycle
+    int ortho;     // 0 delayed CGS2, 1 CGS2
     double tol;       // relative tolerance on ||b - A x|| / ||b||
     double inner_tol; // cycle stops when |g_{k+1}| <= inner_tol * beta0 (mixed precision)
     double nb;        // ||b||
@@ -31,6 +32,9 @@ struct DevState {
     double true_res;  // last true relative residual ||b - A x|| / ||b||
     double wnorm2;    // ||w||^2 of the vector just orthogonalised
     double scalar;    // scratch scalar result of a norm reduction
+    double cu, cw;    // delayed CGS2 axpy scalars: q_k = cu u - sum P_j q_j,
+    double2 du;       //   u_{k+1} = cw w + du u - sum S_j q_j
+    double2 delta;    // q_k^H w of the current delayed CGS2 step
     unsigned int counter[8];  // tickets of the last-block reductions
 };
 
@@ -48,6 +52,12 @@ struct KrylovPtrs {
     double *hist;    // [maxit+1] relative residual history
     double *part;    // [nblk_dot * (m+1) * 2] dot partials
     double *npart;   // [nblk_max] norm partials
+    double2 *Hm;     // [(m+1) * (m+1)] unrotated Hessenberg, row-major: H(i,j) at Hm[i*(m+1) + j]
+    double2 *D1;     // [m+2] <q_j, u_k> (j < k) and <u_k, u_k> (j = k)
+    double2 *D2;     // [m+2] <q_j, w> (j < k) and <u_k, w> (j = k)
+    double2 *tv;     // [m+2] first-pass coefficients of A q_{k-1}
+    double2 *P;      // [m+1] axpy coefficients for q_k
+    double2 *S;      // [m+1] axpy coefficients for u_{k+1}
     int mcap;        // allocated restart capacity (leading dimension of Rm / part)
 };
 
@@ -87,6 +97,11 @@ int launch_dots(int prec_v, const void *V, long long n, const KrylovPtrs &kp, Ve
 int launch_axpy(int prec_v, int prec_w, const void *V, long long n, const KrylovPtrs &kp, const double2 *src,
                 double sign, int nj_mode, VecSel w, int want_norm, int ctr, int nblk, int gate, cudaStream_t s);
 int launch_givens(const KrylovPtrs &kp, cudaStream_t s);
+// delayed CGS2 step (cg_dcgs2.cu)
+int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
+int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s);
+int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
+int dots2_blocks(int sms);
 int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s);
 int launch_cycle_begin(const KrylovPtrs &kp, int nparts, cudaStream_t s);
 int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
@@ -96,6 +111,6 @@ int launch_convert(int from_prec, int to_prec, const void *src, void *dst, long 
 // gate codes for the per-iteration kernels
 enum { GATE_NONE = 0, GATE_STOP = 1 };
 // nj_mode for launch_axpy: number of basis vectors used
-enum { NJ_K_PLUS_1 = 0, NJ_K = 1 };
+enum { NJ_K_PLUS_1 = 0, NJ_K = 1, NJ_NCOL = 2 };
 
 }  // namespace cg

@@ -119,15 +119,20 @@ k_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp, VecSel w, double2 *
         }
     }
     if (last_block(&st->counter[ctr])) {
-        for (int j = threadIdx.x; j < nj; j += blockDim.x) {
+        // warp per coefficient, lanes stride the block partials, fixed-order butterfly
+        for (int j = warp; j < nj; j += DOT_THREADS / 32) {
             double re = 0.0, im = 0.0;
-            for (int b = 0; b < (int)gridDim.x; b++) {
+            for (int b = lane; b < (int)gridDim.x; b += 32) {
                 const double *p = kp.part + 2 * ((size_t)b * ld + j);
                 re += __ldcg(p);
                 im += __ldcg(p + 1);
             }
-            const double s = kp.scale[j];
-            out[j] = make_double2(re * s, im * s);
+            re = warp_sum(re);
+            im = warp_sum(im);
+            if (lane == 0) {
+                const double s = kp.scale[j];
+                out[j] = make_double2(re * s, im * s);
+            }
         }
     }
 }
@@ -142,7 +147,7 @@ k_axpy(const CV *__restrict__ V, long long n, KrylovPtrs kp, const double2 *__re
     typedef typename real_of<CW>::type R;
     DevState *st = kp.st;
     if (gate == GATE_STOP && st->stop) return;
-    const int nj = (nj_mode == NJ_K_PLUS_1) ? st->k + 1 : st->k;
+    const int nj = (nj_mode == NJ_K_PLUS_1) ? st->k + 1 : (nj_mode == NJ_K ? st->k : st->ncol);
     extern __shared__ __align__(16) unsigned char smraw[];
     CW *coef = reinterpret_cast<CW *>(smraw);
     __shared__ double wsum[AXPY_THREADS / 32];
@@ -253,6 +258,7 @@ __global__ void k_givens(KrylovPtrs kp) {
     kp.hist[it] = est;
     kp.scale[k + 1] = hk1 > 0.0 ? 1.0 / hk1 : 0.0;
     st->k = k + 1;
+    st->ncol = k + 1;
     int stop = 0;
     if (!finite) {
         st->status = 4;
@@ -273,7 +279,7 @@ __global__ void k_givens(KrylovPtrs kp) {
 // oriented so the lanes update the remaining right-hand side in parallel.
 __global__ void k_backsolve(KrylovPtrs kp) {
     DevState *st = kp.st;
-    const int kk = st->k;
+    const int kk = st->ncol;
     const int ld = kp.mcap + 1;
     const int lane = threadIdx.x;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -307,6 +313,7 @@ __global__ void k_cycle_begin(KrylovPtrs kp, int nparts) {
     acc = warp_sum(acc);
     const int m = st->m;
     for (int j = lane; j <= m; j += 32) kp.g[j] = make_double2(0.0, 0.0);
+    for (int j = lane; j <= m + 1; j += 32) kp.scale[j] = 1.0;
     __syncwarp();
     if (lane != 0) return;
     const double beta = sqrt(acc);
@@ -315,6 +322,7 @@ __global__ void k_cycle_begin(KrylovPtrs kp, int nparts) {
     st->beta0 = beta;
     if (st->cycles == 0) kp.hist[0] = rel;
     st->k = 0;
+    st->ncol = 0;
     int stop = 0;
     if (!isfinite(beta)) {
         st->status = 4;
@@ -335,7 +343,8 @@ __global__ void k_cycle_begin(KrylovPtrs kp, int nparts) {
     st->brk = 0;
     st->cycles += 1;
     if (!stop) {
-        kp.scale[0] = 1.0 / beta;
+        // CGS2 normalises V_0 lazily; the delayed scheme normalises it in its first step
+        if (st->ortho == 1) kp.scale[0] = 1.0 / beta;
         kp.g[0] = make_double2(beta, 0.0);
     }
     st->stop = stop;
@@ -386,9 +395,19 @@ int launch_dots(int prec_v, const void *V, long long n, const KrylovPtrs &kp, Ve
     return (int)cudaGetLastError();
 }
 
+template <typename K> static int smem_attr(K kern, size_t smem) {
+    if (smem <= 48 * 1024) return 0;
+    return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
 int launch_axpy(int prec_v, int prec_w, const void *V, long long n, const KrylovPtrs &kp, const double2 *src,
                 double sign, int nj_mode, VecSel w, int want_norm, int ctr, int nblk, int gate, cudaStream_t s) {
     const size_t smem = (size_t)(kp.mcap + 1) * (prec_w == 0 ? sizeof(double2) : sizeof(float2));
+    int e = 0;
+    if (prec_v == 0 && prec_w == 0) e = smem_attr(k_axpy<double2, double2>, smem);
+    else if (prec_v == 1 && prec_w == 1) e = smem_attr(k_axpy<float2, float2>, smem);
+    else if (prec_v == 1 && prec_w == 0) e = smem_attr(k_axpy<float2, double2>, smem);
+    if (e) return e;
     if (prec_v == 0 && prec_w == 0)
         k_axpy<double2, double2><<<nblk, AXPY_THREADS, smem, s>>>((const double2 *)V, n, kp, src, sign, nj_mode, w,
                                                                     want_norm, ctr, gate);
@@ -409,7 +428,10 @@ int launch_givens(const KrylovPtrs &kp, cudaStream_t s) {
 }
 
 int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s) {
-    k_backsolve<<<1, 32, (size_t)(kp.mcap + 1) * sizeof(double2), s>>>(kp);
+    const size_t smem = (size_t)(kp.mcap + 1) * sizeof(double2);
+    int e = smem_attr(k_backsolve, smem);
+    if (e) return e;
+    k_backsolve<<<1, 32, smem, s>>>(kp);
     return (int)cudaGetLastError();
 }
 

@@ -52,7 +52,8 @@ template <int L, int ESZ> struct ColCfg {
     static constexpr int CPB0 = (TPR >= TARGET) ? 1 : TARGET / TPR;
     static constexpr int CPB = CPB0 > L ? L : CPB0;
     static constexpr int THREADS = CPB * TPR;
-    static constexpr int REGION = Plan<L>::SMEM_ELEMS + 2;  // +2 keeps columns on distinct banks
+    // columns interleaved element by element: element i of column c at sm[pad(i) * CPB + c]
+    static constexpr int SMEM_ELEMS = Plan<L>::SMEM_ELEMS * CPB;
 };
 
 // ---------------------------------------------------------------- pass 1
@@ -106,7 +107,7 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
     if (gated(st, gate)) return;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int cl = threadIdx.x % CPB, t = threadIdx.x / CPB;
-    C *sm = reinterpret_cast<C *>(smraw) + cl * Q::REGION;
+    C *sm = reinterpret_cast<C *>(smraw) + cl;
     // neighbouring blocks take mirrored column tiles so they share quarter-spectrum columns in L2
     const int ntiles = L / CPB;
     const int b = blockIdx.x;
@@ -119,7 +120,7 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
         reg[p] = czero<C>();
         if (p < E / 2 && k < N) reg[p] = T[(size_t)k * L + col];
     }
-    fft_run<L, false, true>(reg, sm, tw, t);
+    fft_run<L, false, true, CPB>(reg, sm, tw, t);
     const int Lq = L / 2 + 1;
     const int qc = col <= L / 2 ? col : L - col;
 #pragma unroll
@@ -128,7 +129,7 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
         const int qr = k1 <= L / 2 ? k1 : L - k1;
         reg[p] = cmul(reg[p], __ldg(gq + (size_t)qr * Lq + qc));
     }
-    fft_run<L, true, false>(reg, sm, tw + L, t);
+    fft_run<L, true, false, CPB>(reg, sm, tw + L, t);
 #pragma unroll
     for (int p = 0; p < E / 2; p++) {
         const int k = t + p * TPR;
@@ -230,12 +231,12 @@ k_cols_fft_full(double2 *__restrict__ A, const double2 *__restrict__ tw) {
     constexpr int E = P::E, TPR = P::TPR, CPB = Q::CPB;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int cl = threadIdx.x % CPB, t = threadIdx.x / CPB;
-    double2 *sm = reinterpret_cast<double2 *>(smraw) + cl * Q::REGION;
+    double2 *sm = reinterpret_cast<double2 *>(smraw) + cl;
     const int col = blockIdx.x * CPB + cl;
     double2 reg[E];
 #pragma unroll
     for (int p = 0; p < E; p++) reg[p] = A[(size_t)(t + p * TPR) * L + col];
-    fft_run<L, false, false>(reg, sm, tw, t);
+    fft_run<L, false, false, CPB>(reg, sm, tw, t);
 #pragma unroll
     for (int p = 0; p < E; p++) A[(size_t)(t + p * TPR) * L + col] = reg[p];
 }
@@ -265,7 +266,7 @@ static int rows_forward_t(const MatvecArgs &a, VecSel x, const double *xs, const
 template <typename C, int L>
 static int cols_convolve_t(const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
     typedef ColCfg<L, sizeof(C)> Q;
-    const size_t smem = (size_t)Q::CPB * Q::REGION * sizeof(C);
+    const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
     auto kern = k_cols_convolve<C, L>;
     int e = set_smem(kern, smem);
     if (e) return e;
@@ -296,7 +297,7 @@ template <int L> static int fft2d_full_t(double2 *A, const double2 *tw, cudaStre
     e = (int)cudaGetLastError();
     if (e) return e;
     typedef ColCfg<L, 16> Q;
-    smem = (size_t)Q::CPB * Q::REGION * sizeof(double2);
+    smem = (size_t)Q::SMEM_ELEMS * sizeof(double2);
     auto kc = k_cols_fft_full<L>;
     e = set_smem(kc, smem);
     if (e) return e;

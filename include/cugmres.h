@@ -57,6 +57,12 @@ enum {
                                 (MKL_GMRES_test_09122019/source/loop_functions.h:630-689)      */
 };
 
+/* Arnoldi orthogonalisation */
+enum {
+    CG_ORTHO_DCGS2 = 0, /* classical Gram-Schmidt, reorthogonalisation delayed one step: 2 passes over the basis per step */
+    CG_ORTHO_CGS2 = 1   /* classical Gram-Schmidt with one immediate reorthogonalisation: 4 passes per step            */
+};
+
 /* Green's-function constructions for cugmres_green_block */
 enum {
     CG_GREEN_HELMHOLTZ = 0, /* G(d) = (i/4) H0(k0 h |d|) h^2, self term (i pi a/(2k0)) H1(k0 a) - 1/k0^2, pi a^2 = h^2 */
@@ -77,7 +83,8 @@ typedef struct {
     int fixed_iterations; /* 1: reference semantics -- one cycle of exactly max_iter steps,
                              tol is an absolute threshold on ||b - A x0|| only                 */
     double timeout_s;   /* <= 0: none; otherwise the solve returns CG_ERR_TIMEOUT after this    */
-    int reserved[8];
+    int ortho;          /* CG_ORTHO_*                                                          */
+    int reserved[7];
 } cg_opts;
 
 typedef struct {
