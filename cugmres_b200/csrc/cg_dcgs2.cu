@@ -229,36 +229,39 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
     double2 *col = reinterpret_cast<double2 *>(smraw);  // k+1 entries
     double2 *css = col + (kp.mcap + 2);                // k entries
     double *sns = reinterpret_cast<double *>(css + (kp.mcap + 1));
-    double sa = 0.0, acr = 0.0, aci = 0.0;
+    double sa = 0.0, acr = 0.0, aci = 0.0, hn = 0.0;
     for (int j = tid; j < k; j += STEP_THREADS) {
         const double2 a = kp.D1[j], c = kp.D2[j];
         sa += a.x * a.x + a.y * a.y;
         acr += a.x * c.x + a.y * c.y;  // conj(a) c
         aci += a.x * c.y - a.y * c.x;
+        const double2 h = cadd(kp.tv[j], a);  // column k-1 of H above the subdiagonal
+        hn += h.x * h.x + h.y * h.y;
     }
     sa = block_sum(sa, red);
     acr = block_sum(acr, red);
     aci = block_sum(aci, red);
+    hn = block_sum(hn, red);
     const double alpha = kp.D1[k].x;
     const double2 d = kp.D2[k];
-    const double nu2 = alpha - sa;
+    double nu2 = alpha - sa;
     if (tid == 0) {
-        int f = 0;
-        if (!isfinite(nu2) || !isfinite(acr) || !isfinite(aci) || !isfinite(d.x) || !isfinite(d.y)) f = 2;
-        else if (!(nu2 > 1e-28 * alpha) || !(alpha > 0.0)) f = 1;
-        flag = f;
+        flag = (!isfinite(nu2) || !isfinite(acr) || !isfinite(aci) || !isfinite(d.x) || !isfinite(d.y) ||
+                !isfinite(hn)) ? 2 : 0;
     }
     __syncthreads();
     if (flag) {
         if (tid == 0) {
-            if (flag == 2) st->status = 4;
-            else st->brk = 1;
+            st->status = 4;
             st->stop = 1;
         }
         return;
     }
+    if (!(nu2 > 0.0)) nu2 = 0.0;
+    // (happy) breakdown: the new direction vanishes against the column it closes
+    const bool brk = k >= 1 ? !(nu2 > 1e-28 * (hn + nu2)) : !(nu2 > 0.0);
     const double nu = sqrt(nu2);
-    const double inu = 1.0 / nu;
+    const double inu = nu > 0.0 ? 1.0 / nu : 0.0;
     const double2 delta = make_double2((d.x - acr) * inu, (d.y - aci) * inu);
     if (k >= 1) {
         // column k-1 of H = t + a (rows 0..k-1), nu (row k); H is stored row-major
@@ -285,6 +288,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
         kp.S[i] = make_double2((c.x - da.x * inu) * inu, (c.y - da.y * inu) * inu);
     }
     if (tid == 0) {
+        if (brk) st->brk = 1;
         st->cu = inu;
         st->cw = inu;
         st->du = make_double2(-delta.x * inu * inu, -delta.y * inu * inu);
@@ -330,6 +334,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
             if (k >= st->m) stop = 1;
             if (it >= st->maxit) stop = 1;
         }
+        if (brk) stop = 1;
         st->k = k + 1;
         st->stop = stop;
     }
