@@ -29,13 +29,14 @@ CG_GIVENS_REFERENCE = 1
 CG_GREEN_HELMHOLTZ = 0
 CG_GREEN_REFERENCE = 1
 CG_GREEN_PYGMRES = 2
+NOALLOC_MAX_N = 256
 
 # Every symbol include/cugmres.h declares.
 EXPORTS = (
     "cugmres_strerror", "cugmres_version", "cugmres_default_opts", "cugmres_create", "cugmres_destroy",
     "cugmres_set_stream", "cugmres_synchronize", "cugmres_green_block", "cugmres_set_operator",
     "cugmres_set_operator_circulant", "cugmres_grid_size", "cugmres_matvec", "cugmres_residual",
-    "cugmres_solve", "cugmres_fast_gmres", "cugmres_profile", "cugmres_profile_read",
+    "cugmres_solve", "cugmres_fast_gmres", "cugmres_profile", "cugmres_profile_read", "cugmres_matvec_noalloc",
 )
 
 PHASES = ("matvec", "dots", "axpy", "small", "update", "residual")
@@ -113,6 +114,7 @@ def _declare(L):
     L.cugmres_residual.argtypes = [P, P, P, P, ctypes.POINTER(D)]
     L.cugmres_solve.argtypes = [P, P, P, ctypes.POINTER(CgOpts), P, I, ctypes.POINTER(CgResult)]
     L.cugmres_fast_gmres.argtypes = [P, P, P, P, ctypes.POINTER(U), F, ctypes.POINTER(I), U, U, F, P, I]
+    L.cugmres_matvec_noalloc.argtypes = [I, P, P, D, P, P, P]
     L.cugmres_profile.argtypes = [P, I]
     L.cugmres_profile_read.argtypes = [P, ctypes.POINTER(CgPhaseStats)]
     for name in EXPORTS:

@@ -170,6 +170,27 @@ int cugmres_fast_gmres(const cg_c64 *g_prep, const unsigned char *mask, cg_c64 *
                        unsigned int *gmres_n, float tolerance, int *res_vs_tol, unsigned int maxiter, unsigned int N,
                        float chi_value, const cg_c64 *rhs, int precision);
 
+/* Allocation-free y = A x (FP64) for callers that cannot allocate device
+ * memory -- for example a plug-in inside a host application whose GPU memory
+ * is owned entirely by its own pool allocator, or a latency-critical loop that
+ * cannot afford the implicit device synchronisation of cudaMalloc/cudaFree.
+ * No counterpart in the reference (its matvec allocates through cuFFT plans and
+ * the solver cudaMallocs per call).  It builds the spectrum from g_block and
+ * applies A = I - G diag(chi_scale * chi) to x, using only a fixed scratch
+ * array compiled into the library (about 7.6 MB per GPU, held until exit).
+ *   - N <= CUGMRES_NOALLOC_MAX_N, otherwise CG_ERR_INVALID (use cugmres_matvec);
+ *   - g_block (N x N), chi (N x N), x and y must be device memory of the current
+ *     device, otherwise CG_ERR_INVALID;
+ *   - the first call on a device looks up the scratch array's address (once per
+ *     device); make it before any stream capture;
+ *   - calls share the scratch array: calls whose GPU work overlaps (other
+ *     streams or host threads) race, so serialise them on one stream;
+ *   - the work is enqueued on `stream` (a cudaStream_t, NULL = default stream);
+ *     y is ready once the stream reaches it. */
+#define CUGMRES_NOALLOC_MAX_N 256
+int cugmres_matvec_noalloc(int N, const cg_c128 *g_block, const double *chi, double chi_scale, const cg_c128 *x,
+                           cg_c128 *y, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
