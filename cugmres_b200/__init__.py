@@ -24,7 +24,7 @@ from . import _lib
 from ._lib import CugmresError, check
 from .problems import green_block, helmholtz, reference_cylinder
 
-__all__ = ["Solver", "CugmresError", "green_block", "helmholtz", "reference_cylinder", "matvec",
+__all__ = ["Solver", "CugmresError", "green_block", "helmholtz", "reference_cylinder", "matvec", "solve_batch",
            "get_plane_wave", "get_green_matrix", "get_toeplitz_mat", "get_eps_from_mask",
            "fast_gmres", "gmres"]
 
@@ -92,6 +92,12 @@ class Solver:
 
     def synchronize(self):
         check(_lib.lib().cugmres_synchronize(self._ctx), "synchronize")
+
+    def matvec_shapes(self, precision="fp64"):
+        """Autotuned launch shapes (row forward, column convolution, row inverse)."""
+        arr = (ctypes.c_int * 3)()
+        check(_lib.lib().cugmres_matvec_shapes(self._ctx, _PREC[precision], arr), "matvec_shapes")
+        return tuple(arr)
 
     def profile(self, enable=True):
         """Enable (and reset) per-phase device timing of solve()."""
@@ -181,6 +187,39 @@ class Solver:
                     rel_residual_estimate=res.rel_residual_estimate, rel_residual_true=res.rel_residual_true,
                     seconds=res.seconds, res_hist=hist[: res.iterations + 1].copy())
         return xk, info
+
+
+def solve_batch(systems, device=0, workers=8, restart=100, max_iter=10000, tol=1e-10, precision="fp64",
+                givens="unitary", inner_tol=1e-5, ortho="dcgs2"):
+    """Solve many independent systems concurrently (cugmres_solve_batch).
+
+    systems: iterable of dicts with g_block, chi, chi_scale, b and optionally x0.
+    Returns (xs, infos): solutions (complex128 N x N) and per-system dicts with
+    status, iterations, rel_residual_true and seconds (set-up + solve latency)."""
+    systems = list(systems)
+    keep, arr = [], (_lib.CgSystem * max(1, len(systems)))()
+    xs = []
+    for i, sysd in enumerate(systems):
+        N = int(sysd["g_block"].shape[0])
+        g = np.ascontiguousarray(sysd["g_block"], np.complex128)
+        c = np.ascontiguousarray(sysd["chi"], np.float64)
+        b = np.ascontiguousarray(sysd["b"], np.complex128)
+        x = np.zeros((N, N), np.complex128) if sysd.get("x0") is None else np.array(sysd["x0"], np.complex128)
+        keep += [g, c, b]
+        xs.append(x)
+        arr[i] = _lib.CgSystem(N, g.ctypes.data, c.ctypes.data, float(sysd.get("chi_scale", 1.0)), b.ctypes.data,
+                               x.ctypes.data)
+    o = _lib.CgOpts()
+    _lib.lib().cugmres_default_opts(ctypes.byref(o))
+    o.restart, o.max_iter, o.tol = int(restart), int(max_iter), float(tol)
+    o.precision, o.givens, o.inner_tol, o.ortho = _PREC[precision], _GIV[givens], float(inner_tol), _ORTHO[ortho]
+    res = (_lib.CgResult * max(1, len(systems)))()
+    check(_lib.lib().cugmres_solve_batch(int(device), len(systems), arr, ctypes.byref(o), int(workers), res),
+          "cugmres_solve_batch")
+    infos = [dict(status=r.status, status_text=_lib.strerror(r.status), iterations=r.iterations, cycles=r.cycles,
+                  rel_residual_true=r.rel_residual_true, rel_residual_estimate=r.rel_residual_estimate,
+                  seconds=r.seconds) for r in res[: len(systems)]]
+    return xs, infos
 
 
 def gmres(g_block, chi, b, chi_scale=1.0, device=0, **kw):

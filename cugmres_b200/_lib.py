@@ -37,6 +37,7 @@ EXPORTS = (
     "cugmres_set_stream", "cugmres_synchronize", "cugmres_green_block", "cugmres_set_operator",
     "cugmres_set_operator_circulant", "cugmres_grid_size", "cugmres_matvec", "cugmres_residual",
     "cugmres_solve", "cugmres_fast_gmres", "cugmres_profile", "cugmres_profile_read", "cugmres_matvec_noalloc",
+    "cugmres_matvec_shapes", "cugmres_solve_batch",
 )
 
 PHASES = ("matvec", "dots", "axpy", "small", "update", "residual")
@@ -66,6 +67,17 @@ class CgResult(ctypes.Structure):
         ("rel_residual_estimate", ctypes.c_double),
         ("rel_residual_true", ctypes.c_double),
         ("seconds", ctypes.c_double),
+    ]
+
+
+class CgSystem(ctypes.Structure):
+    _fields_ = [
+        ("N", ctypes.c_int),
+        ("g_block", ctypes.c_void_p),
+        ("chi", ctypes.c_void_p),
+        ("chi_scale", ctypes.c_double),
+        ("b", ctypes.c_void_p),
+        ("x", ctypes.c_void_p),
     ]
 
 
@@ -115,6 +127,9 @@ def _declare(L):
     L.cugmres_solve.argtypes = [P, P, P, ctypes.POINTER(CgOpts), P, I, ctypes.POINTER(CgResult)]
     L.cugmres_fast_gmres.argtypes = [P, P, P, P, ctypes.POINTER(U), F, ctypes.POINTER(I), U, U, F, P, I]
     L.cugmres_matvec_noalloc.argtypes = [I, P, P, D, P, P, P]
+    L.cugmres_matvec_shapes.argtypes = [P, I, ctypes.POINTER(I)]
+    L.cugmres_solve_batch.argtypes = [I, I, ctypes.POINTER(CgSystem), ctypes.POINTER(CgOpts), I,
+                                      ctypes.POINTER(CgResult)]
     L.cugmres_profile.argtypes = [P, I]
     L.cugmres_profile_read.argtypes = [P, ctypes.POINTER(CgPhaseStats)]
     for name in EXPORTS:

@@ -15,9 +15,15 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#include <sys/stat.h>
 #include <time.h>
 
 #include <algorithm>
+#include <array>
+#include <cstdio>
+#include <map>
+#include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/cugmres.h"
@@ -54,6 +60,9 @@ struct cg_ctx {
     double2 *rbuf = nullptr;  // FP64 vector scratch (residual, matvec staging)
     int nparts_cap = 0;
     cudaEvent_t ev = nullptr;
+    // launch shapes of the three matvec passes per precision (autotuned)
+    int var[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    char devname[256] = {0};
     // per-phase timing
     bool prof = false;
     std::vector<cudaEvent_t> evpool;
@@ -243,6 +252,9 @@ MatvecArgs margs(const cg_ctx *c, int prec) {
     MatvecArgs a;
     a.N = c->N;
     a.L = c->L;
+    a.vfwd = c->var[prec][0];
+    a.vcols = c->var[prec][1];
+    a.vinv = c->var[prec][2];
     a.gq = prec == 0 ? (const void *)c->gq64 : (const void *)c->gq32;
     a.cdiag = prec == 0 ? (const void *)c->c64 : (const void *)c->c32;
     a.tw = prec == 0 ? (const void *)c->tw64 : (const void *)c->tw32;
@@ -258,9 +270,134 @@ VecSel fixed_vec(const void *p) {
     return v;
 }
 
+// blocks of the FP64 residual pass (each writes one ||r||^2 partial)
 int row_blocks(const cg_ctx *c) {
-    const int rpc = rows_per_block(0, c->L);
+    const int rpc = rows_per_block(c->var[0][2], c->L);
     return (c->N + rpc - 1) / rpc;
+}
+
+// ------------------------------------------------------------- autotuner
+// Times each launch shape of each matvec pass on the context's operator with
+// CUDA events and keeps the fastest.  Choices are cached per process and in a
+// text file (one line "device|L|precision fwd cols inv") under
+// $CUGMRES_TUNE_CACHE, else $XDG_CACHE_HOME/cugmres_b200/autotune.txt, else
+// ~/.cache/cugmres_b200/autotune.txt.  CUGMRES_AUTOTUNE=0 disables tuning;
+// CUGMRES_MATVEC_SHAPE=v forces shape v.
+std::mutex g_tune_mu;
+std::map<std::string, std::array<int, 3>> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_path() {
+    const char *e = getenv("CUGMRES_TUNE_CACHE");
+    if (e && *e) return std::string(e);
+    std::string base;
+    const char *x = getenv("XDG_CACHE_HOME");
+    if (x && *x) base = x;
+    else {
+        const char *h = getenv("HOME");
+        base = std::string(h && *h ? h : "/tmp") + "/.cache";
+    }
+    return base + "/cugmres_b200/autotune.txt";
+}
+
+void tune_load() {
+    if (g_tune_loaded) return;
+    g_tune_loaded = true;
+    FILE *f = fopen(tune_path().c_str(), "r");
+    if (!f) return;
+    char key[512];
+    int a, b, cc;
+    while (fscanf(f, "%511s %d %d %d", key, &a, &b, &cc) == 4) g_tune[key] = {a, b, cc};
+    fclose(f);
+}
+
+void tune_save(const std::string &key, const std::array<int, 3> &v) {
+    const std::string path = tune_path();
+    const size_t slash = path.rfind('/');
+    if (slash != std::string::npos) {
+        std::string dir = path.substr(0, slash);
+        std::string cmd_dir;
+        for (size_t i = 1; i <= dir.size(); i++)
+            if (i == dir.size() || dir[i] == '/') {
+                cmd_dir = dir.substr(0, i);
+                mkdir(cmd_dir.c_str(), 0755);
+            }
+    }
+    FILE *f = fopen(path.c_str(), "a");
+    if (!f) return;
+    fprintf(f, "%s %d %d %d\n", key.c_str(), v[0], v[1], v[2]);
+    fclose(f);
+}
+
+int autotune(cg_ctx *c, int prec) {
+    c->var[prec][0] = c->var[prec][1] = c->var[prec][2] = 0;
+    const int nv = matvec_variants(c->L);
+    if (nv <= 1) return CG_OK;
+    const char *env = getenv("CUGMRES_AUTOTUNE");
+    if (env && env[0] == '0') return CG_OK;
+    // CUGMRES_MATVEC_SHAPE=v forces shape v on all three passes (diagnostics, tests)
+    const char *force = getenv("CUGMRES_MATVEC_SHAPE");
+    if (force && *force) {
+        const int v = atoi(force);
+        if (v < 0 || v >= nv) return CG_ERR_INVALID;
+        for (int p = 0; p < 3; p++) c->var[prec][p] = v;
+        return CG_OK;
+    }
+    std::string key = std::string(c->devname) + "|" + std::to_string(c->L) + "|" + std::to_string(prec);
+    for (char &ch : key)
+        if (ch == ' ') ch = '_';
+    {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        tune_load();
+        auto it = g_tune.find(key);
+        if (it != g_tune.end() && it->second[0] < nv && it->second[1] < nv && it->second[2] < nv) {
+            for (int p = 0; p < 3; p++) c->var[prec][p] = it->second[p];
+            return CG_OK;
+        }
+    }
+    const long long n = (long long)c->N * c->N;
+    cudaStream_t s = c->stream;
+    CG_CU(cudaMemsetAsync(c->xbuf, 0, sizeof(double2) * n, s));
+    CG_CU(cudaMemsetAsync(c->T, 0, sizeof(double2) * (size_t)c->N * c->L, s));
+    cudaEvent_t e0, e1;
+    CG_CU(cudaEventCreate(&e0));
+    CG_CU(cudaEventCreate(&e1));
+    std::array<int, 3> best = {0, 0, 0};
+    int status = CG_OK;
+    for (int pass = 0; pass < 3 && status == CG_OK; pass++) {
+        float best_ms = 1e30f;
+        for (int v = 0; v < nv && status == CG_OK; v++) {
+            MatvecArgs a = margs(c, prec);
+            a.vfwd = a.vcols = a.vinv = v;
+            auto launch = [&]() -> int {
+                if (pass == 0) return launch_rows_forward(prec, a, fixed_vec(c->xbuf), nullptr, nullptr, GATE_NONE, s);
+                if (pass == 1) return launch_cols_convolve(prec, a, nullptr, GATE_NONE, s);
+                return launch_rows_inverse(prec, 0, prec, a, fixed_vec(c->xbuf), nullptr, nullptr, fixed_vec(c->rbuf),
+                                           nullptr, nullptr, GATE_NONE, s);
+            };
+            for (int w = 0; w < 2 && status == CG_OK; w++)
+                if (launch() != 0) status = CG_ERR_CUDA;
+            cudaEventRecord(e0, s);
+            for (int r = 0; r < 5 && status == CG_OK; r++)
+                if (launch() != 0) status = CG_ERR_CUDA;
+            cudaEventRecord(e1, s);
+            if (cudaEventSynchronize(e1) != cudaSuccess) status = CG_ERR_CUDA;
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best[pass] = v;
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (status != CG_OK) return status;
+    for (int p = 0; p < 3; p++) c->var[prec][p] = best[p];
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = best;
+    tune_save(key, best);
+    return CG_OK;
 }
 
 // y = A x (mode 0) or y = b - A x (mode 1) on explicit vectors, no gating.
@@ -391,6 +528,12 @@ int cugmres_create(cg_ctx **out, int device) {
     cg_ctx *c = new cg_ctx();
     c->device = device;
     cudaDeviceGetAttribute(&c->sms, cudaDevAttrMultiProcessorCount, device);
+    {
+        cudaDeviceProp prop;
+        if (cudaGetDeviceProperties(&prop, device) == cudaSuccess) {
+            strncpy(c->devname, prop.name, sizeof(c->devname) - 1);
+        }
+    }
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete c;
         return CG_ERR_CUDA;
@@ -452,6 +595,14 @@ int cugmres_profile_read(cg_ctx *c, cg_phase_stats *out) {
     return CG_OK;
 }
 
+int cugmres_matvec_shapes(const cg_ctx *c, int precision, int *shapes) {
+    if (!c || !shapes || (precision != CG_PREC_FP64 && precision != CG_PREC_MIXED)) return CG_ERR_INVALID;
+    if (!c->have_op) return CG_ERR_NO_OPERATOR;
+    const int p = precision == CG_PREC_FP64 ? 0 : 1;
+    for (int i = 0; i < 3; i++) shapes[i] = c->var[p][i];
+    return CG_OK;
+}
+
 int cugmres_grid_size(const cg_ctx *c, int *N, int *L) {
     if (!c || !c->have_op) return CG_ERR_NO_OPERATOR;
     if (N) *N = c->N;
@@ -487,21 +638,26 @@ int cugmres_set_operator(cg_ctx *c, int N, const cg_c128 *g_block, const double 
     const bool g_dev = is_device_ptr(g_block), chi_dev = is_device_ptr(chi);
     if (!g_dev && !all_finite((const double *)g_block, 2 * (size_t)n)) return CG_ERR_NONFINITE;
     if (!chi_dev && !all_finite(chi, (size_t)n)) return CG_ERR_NONFINITE;
-    free_operator(c);
-    free_krylov(c);
-    c->N = N;
-    c->L = L;
-    const int Lq = L / 2 + 1;
-    CG_CU(cudaMalloc((void **)&c->gq64, sizeof(double2) * (size_t)Lq * Lq));
-    CG_CU(cudaMalloc((void **)&c->gq32, sizeof(float2) * (size_t)Lq * Lq));
-    CG_CU(cudaMalloc((void **)&c->c64, sizeof(double) * n));
-    CG_CU(cudaMalloc((void **)&c->c32, sizeof(float) * n));
-    CG_CU(cudaMalloc((void **)&c->tw64, sizeof(double2) * 2 * L));
-    CG_CU(cudaMalloc((void **)&c->tw32, sizeof(float2) * 2 * L));
-    CG_CU(cudaMalloc(&c->T, sizeof(double2) * (size_t)N * L));
-    CG_CU(cudaMalloc((void **)&c->bbuf, sizeof(double2) * n));
-    CG_CU(cudaMalloc((void **)&c->xbuf, sizeof(double2) * n));
-    CG_CU(cudaMalloc((void **)&c->rbuf, sizeof(double2) * n));
+    // a context keeps its buffers when the grid size does not change (batched sweeps)
+    const bool same = c->gq64 != nullptr && c->N == N && c->L == L;
+    c->have_op = false;
+    if (!same) {
+        free_operator(c);
+        free_krylov(c);
+        c->N = N;
+        c->L = L;
+        const int Lq = L / 2 + 1;
+        CG_CU(cudaMalloc((void **)&c->gq64, sizeof(double2) * (size_t)Lq * Lq));
+        CG_CU(cudaMalloc((void **)&c->gq32, sizeof(float2) * (size_t)Lq * Lq));
+        CG_CU(cudaMalloc((void **)&c->c64, sizeof(double) * n));
+        CG_CU(cudaMalloc((void **)&c->c32, sizeof(float) * n));
+        CG_CU(cudaMalloc((void **)&c->tw64, sizeof(double2) * 2 * L));
+        CG_CU(cudaMalloc((void **)&c->tw32, sizeof(float2) * 2 * L));
+        CG_CU(cudaMalloc(&c->T, sizeof(double2) * (size_t)N * L));
+        CG_CU(cudaMalloc((void **)&c->bbuf, sizeof(double2) * n));
+        CG_CU(cudaMalloc((void **)&c->xbuf, sizeof(double2) * n));
+        CG_CU(cudaMalloc((void **)&c->rbuf, sizeof(double2) * n));
+    }
     // twiddles exp(-2 pi i m / L) and their conjugates, in double
     std::vector<double2> tw(2 * L);
     std::vector<float2> twf(2 * L);
@@ -534,6 +690,8 @@ int cugmres_set_operator(cg_ctx *c, int N, const cg_c128 *g_block, const double 
     if (g_tmp) cudaFree(g_tmp);
     if (chi_tmp) cudaFree(chi_tmp);
     if (s != CG_OK) return s;
+    CG_TRY(autotune(c, 0));
+    CG_TRY(autotune(c, 1));
     c->have_op = true;
     return CG_OK;
 }

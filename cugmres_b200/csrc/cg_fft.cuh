@@ -1,4 +1,4 @@
-// Stockham radix-16 FFT building blocks for the circulant-embedding matvec.
+// Stockham radix-16 / radix-8 FFT building blocks for the circulant-embedding matvec.
 //
 // The reference applies its BTTB operator with two cuFFT calls on an odd
 // (2N-1)^2 grid plus three elementwise kernels (CUDA_GMRES/Fast_matvec.cuh:1-28).
@@ -6,7 +6,7 @@
 // and the 1D transforms are the project's own: a Stockham auto-sort FFT
 // (formulation of Govindaraju, Lloyd, Dotsenko, Smith and Manferdelli,
 // "High performance discrete Fourier transforms on graphics processors", SC08)
-// where each thread owns E = 16 points:
+// where each thread owns E = 16 (or 8) points:
 //
 //   stage s with radix R and span Ns reads  a[j + r L/R]          (r < R)
 //   multiplies by the twiddle  w_L^{(j mod Ns) r L/(Ns R)},
@@ -159,10 +159,10 @@ template <int R, bool INV, typename C> __device__ __forceinline__ void dft_half_
 }
 
 // ------------------------------------------------------------ plans
-// Length L = E^a * rem (rem in {1,2,4,8}) with E = 16: stages radix 16 ...,
-// then one stage of radix rem.  Lengths below 16 use a single stage of radix L.
-template <int L> struct Plan {
-    static constexpr int E = (L >= 16) ? 16 : L;
+// Length L = E^a * rem with E points per thread (16 or 8): stages of radix E,
+// then one stage of radix rem < E.  Lengths below E use one stage of radix L.
+template <int L, int E0 = 16> struct Plan {
+    static constexpr int E = (L >= E0) ? E0 : L;
     static constexpr int TPR = L / E;
     __host__ __device__ static constexpr int ilog(int v) { return v <= 1 ? 0 : 1 + ilog(v / 2); }
     static constexpr int LOG = ilog(L);
@@ -186,8 +186,8 @@ template <bool INV, typename C> __device__ __forceinline__ C twiddle(const C *__
 // One Stockham stage S of a length-L transform (compile-time radix and span).
 // tmp holds the previous stage's butterfly outputs (tmp[b*Rp + q]) on entry
 // and this stage's outputs on exit; the last stage stores canonical reg.
-template <int L, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
-    typedef Plan<L> P;
+template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
+    typedef Plan<L, E0> P;
     static constexpr int E = P::E;
     static constexpr int TPR = P::TPR;
     static constexpr int R = P::radix(S);
@@ -238,7 +238,7 @@ template <int L, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
 #pragma unroll
                 for (int q = 0; q < R; q++) reg[b + q * NB] = tmp[b * R + q];
         } else {
-            Stage<L, INV, HALF_IN, S + 1, SMS>::run(reg, tmp, sm, tw, t);
+            Stage<L, E0, INV, HALF_IN, S + 1, SMS>::run(reg, tmp, sm, tw, t);
         }
     }
 };
@@ -251,10 +251,10 @@ template <int L, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
 // HALF_IN: inputs L/2 .. L-1 are zero (first stage uses dft_half_input).
 // Every thread of the block must call this the same number of times
 // (it contains __syncthreads()).
-template <int L, bool INV, bool HALF_IN, int SMS = 1, typename C>
-__device__ __forceinline__ void fft_run(C (&reg)[Plan<L>::E], C *sm, const C *__restrict__ tw, int t) {
-    C tmp[Plan<L>::E];
-    Stage<L, INV, HALF_IN, 0, SMS>::run(reg, tmp, sm, tw, t);
+template <int L, int E0, bool INV, bool HALF_IN, int SMS = 1, typename C>
+__device__ __forceinline__ void fft_run(C (&reg)[Plan<L, E0>::E], C *sm, const C *__restrict__ tw, int t) {
+    C tmp[Plan<L, E0>::E];
+    Stage<L, E0, INV, HALF_IN, 0, SMS>::run(reg, tmp, sm, tw, t);
 }
 
 }  // namespace cg

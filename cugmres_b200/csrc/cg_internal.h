@@ -64,6 +64,7 @@ struct KrylovPtrs {
 // Matvec launch parameters for one precision (C = double2 or float2, R its real type).
 struct MatvecArgs {
     int N, L;
+    int vfwd, vcols, vinv;  // launch shape of each pass (0..matvec_variants(L)-1), chosen by the autotuner
     const void *gq;     // quarter spectrum (C)
     const void *cdiag;  // N x N real diagonal k0^2 chi (R)
     const void *tw;     // L twiddles (C)
@@ -85,8 +86,9 @@ int launch_cols_convolve(int prec, const MatvecArgs &a, const DevState *st, int 
 // mode 0: y = s*x - conv;  mode 1: y = b - x + conv (y may be float2 while the matvec is double2: out_prec)
 int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xscale_base,
                         const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s);
-int rows_per_block(int prec, int L);
+int rows_per_block(int variant, int L);
 int fft_supported(int L);
+int matvec_variants(int L);
 
 // full (unpruned) forward 2D transform of an L x L FP64 array, used to build the spectrum
 int launch_fft2d_full_fp64(int L, double2 *a, const double2 *tw, cudaStream_t s);

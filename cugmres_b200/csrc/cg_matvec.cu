@@ -12,23 +12,24 @@
 //   pass 2  k_cols_convolve  per column: forward column FFT (upper half of the
 //                            input is zero), multiply by the spectrum, inverse
 //                            column FFT, store only rows 0..N-1 back into T.
-// Twiddle tables hold 2L entries: exp(-2 pi i m/L) then its conjugate, so the
-// inverse transform reads different addresses from the forward one (otherwise
-// the compiler keeps the forward twiddles live across the column convolution).
 //   pass 3  k_rows_inverse   inverse row FFT, crop to the first N columns and
 //                            finish: y = s x - conv  (matvec)  or
 //                            r = b - x + conv (residual), with ||y||^2 partials.
 // The spectrum is even in both axes for the reference's kernel and for the
 // GFIEM kernel (G depends on |d1|, |d2|), so only its quarter
 // (L/2+1) x (L/2+1) is stored and read; the 1/L^2 normalisation is folded into it.
+// Twiddle tables hold 2L entries: exp(-2 pi i m/L) then its conjugate, so the
+// inverse transform reads different addresses from the forward one (otherwise
+// the compiler keeps the forward twiddles live across the column convolution).
+//
+// Launch shapes (points per thread, threads per block, resident blocks per SM
+// requested from the compiler) are template parameters; the MvShape variants
+// 0..3 are instantiated for L >= 256 and the autotuner in cg_api.cu picks one
+// per (precision, L); smaller L always use variant 0.
 #include "cg_fft.cuh"
 #include "cg_internal.h"
 
 namespace cg {
-
-template <typename C> struct PrecOf;
-template <> struct PrecOf<double2> { static const int value = 0; };
-template <> struct PrecOf<float2> { static const int value = 1; };
 
 static __device__ __forceinline__ bool gated(const DevState *st, int gate) {
     return gate == GATE_STOP && st != nullptr && st->stop != 0;
@@ -38,37 +39,50 @@ static __device__ __forceinline__ long long sel_index(const DevState *st, int ko
     return st ? (long long)(st->k + koff) : 0;
 }
 
-template <int L> struct RowCfg {
-    static constexpr int TPR = Plan<L>::TPR;
-    static constexpr int RPC = (TPR >= 256) ? 1 : 256 / TPR;
+// E: points per thread; ROWT: target threads per row block; COLT64 / COLT32:
+// target threads per column block in FP64 / FP32; MINB: resident blocks per SM
+// requested from the compiler (bounds the registers per thread).
+template <int E_, int ROWT_, int COLT64_, int COLT32_, int MINB_> struct MvShape {
+    static constexpr int E = E_, ROWT = ROWT_, COLT64 = COLT64_, COLT32 = COLT32_, MINB = MINB_;
+};
+typedef MvShape<16, 256, 256, 512, 1> MvV0;  // 16 points, wide blocks
+typedef MvShape<16, 256, 256, 512, 2> MvV1;  // 16 points, two blocks per SM (<= 128 registers)
+typedef MvShape<8, 256, 512, 512, 1> MvV2;   // 8 points, twice the threads per column
+typedef MvShape<8, 256, 256, 256, 2> MvV3;   // 8 points, two blocks per SM
+constexpr int MV_VARIANTS = 4;
+
+template <int L, typename SH> struct RowCfg {
+    typedef Plan<L, SH::E> P;
+    static constexpr int TPR = P::TPR;
+    static constexpr int RPC = (TPR >= SH::ROWT) ? 1 : SH::ROWT / TPR;
     static constexpr int THREADS = RPC * TPR;
+    static constexpr int SMEM_ELEMS = RPC * P::SMEM_ELEMS;
 };
 
-// Column blocks: 256 threads for FP64 (16 complex doubles per thread need
-// more than the 128 registers a 512-thread block allows), 512 for FP32.
-template <int L, int ESZ> struct ColCfg {
-    static constexpr int TPR = Plan<L>::TPR;
-    static constexpr int TARGET = ESZ >= 16 ? 256 : 512;
+template <int L, typename SH, int ESZ> struct ColCfg {
+    typedef Plan<L, SH::E> P;
+    static constexpr int TPR = P::TPR;
+    static constexpr int TARGET = ESZ >= 16 ? SH::COLT64 : SH::COLT32;
     static constexpr int CPB0 = (TPR >= TARGET) ? 1 : TARGET / TPR;
     static constexpr int CPB = CPB0 > L ? L : CPB0;
     static constexpr int THREADS = CPB * TPR;
     // columns interleaved element by element: element i of column c at sm[pad(i) * CPB + c]
-    static constexpr int SMEM_ELEMS = Plan<L>::SMEM_ELEMS * CPB;
+    static constexpr int SMEM_ELEMS = P::SMEM_ELEMS * CPB;
 };
 
 // ---------------------------------------------------------------- pass 1
-template <typename C, int L>
-__global__ void __launch_bounds__(RowCfg<L>::THREADS)
+template <typename C, int L, typename SH>
+__global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
 k_rows_forward(VecSel xs, const double *__restrict__ xscale, const typename real_of<C>::type *__restrict__ cdiag,
                C *__restrict__ T, const C *__restrict__ tw, int N, const DevState *st, int gate) {
     typedef typename real_of<C>::type R;
-    typedef Plan<L> P;
+    typedef Plan<L, SH::E> P;
     constexpr int E = P::E, TPR = P::TPR;
     if (gated(st, gate)) return;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int lr = threadIdx.x / TPR, t = threadIdx.x % TPR;
     C *sm = reinterpret_cast<C *>(smraw) + lr * P::SMEM_ELEMS;
-    const int row = blockIdx.x * RowCfg<L>::RPC + lr;
+    const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
     const long long ks = sel_index(st, xs.koff);
     const C *x = reinterpret_cast<const C *>(xs.base) + ks * xs.stride;
     const R s = xscale ? (R)xscale[ks] : (R)1;
@@ -85,7 +99,7 @@ k_rows_forward(VecSel xs, const double *__restrict__ xscale, const typename real
             reg[p] = cscale(v, c);
         }
     }
-    fft_run<L, false, true>(reg, sm, tw, t);
+    fft_run<L, SH::E, false, true>(reg, sm, tw, t);
     if (live) {
         C *out = T + (size_t)row * L;
 #pragma unroll
@@ -94,15 +108,12 @@ k_rows_forward(VecSel xs, const double *__restrict__ xscale, const typename real
 }
 
 // ---------------------------------------------------------------- pass 2
-template <typename C, int L>
-#ifndef CG_COL_MINB
-#define CG_COL_MINB 1
-#endif
-__global__ void __launch_bounds__(ColCfg<L, sizeof(C)>::THREADS, CG_COL_MINB)
+template <typename C, int L, typename SH>
+__global__ void __launch_bounds__(ColCfg<L, SH, sizeof(C)>::THREADS, SH::MINB)
 k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict__ tw, int N, const DevState *st,
                 int gate) {
-    typedef Plan<L> P;
-    typedef ColCfg<L, sizeof(C)> Q;
+    typedef Plan<L, SH::E> P;
+    typedef ColCfg<L, SH, sizeof(C)> Q;
     constexpr int E = P::E, TPR = P::TPR, CPB = Q::CPB;
     if (gated(st, gate)) return;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -120,7 +131,7 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
         reg[p] = czero<C>();
         if (p < E / 2 && k < N) reg[p] = T[(size_t)k * L + col];
     }
-    fft_run<L, false, true, CPB>(reg, sm, tw, t);
+    fft_run<L, SH::E, false, true, CPB>(reg, sm, tw, t);
     const int Lq = L / 2 + 1;
     const int qc = col <= L / 2 ? col : L - col;
 #pragma unroll
@@ -129,7 +140,7 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
         const int qr = k1 <= L / 2 ? k1 : L - k1;
         reg[p] = cmul(reg[p], __ldg(gq + (size_t)qr * Lq + qc));
     }
-    fft_run<L, true, false, CPB>(reg, sm, tw + L, t);
+    fft_run<L, SH::E, true, false, CPB>(reg, sm, tw + L, t);
 #pragma unroll
     for (int p = 0; p < E / 2; p++) {
         const int k = t + p * TPR;
@@ -138,20 +149,21 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
 }
 
 // ---------------------------------------------------------------- pass 3
-template <typename C, typename CO, int L, int MODE>
-__global__ void __launch_bounds__(RowCfg<L>::THREADS)
+template <typename C, typename CO, int L, int MODE, typename SH>
+__global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
 k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xscale, const C *__restrict__ bvec,
                VecSel ys, double *__restrict__ npart, const C *__restrict__ tw, int N, const DevState *st, int gate) {
     typedef typename real_of<C>::type R;
     typedef typename real_of<CO>::type RO;
-    typedef Plan<L> P;
+    typedef Plan<L, SH::E> P;
     constexpr int E = P::E, TPR = P::TPR;
+    constexpr int NWARP = (RowCfg<L, SH>::THREADS + 31) / 32;
     if (gated(st, gate)) return;
     extern __shared__ __align__(16) unsigned char smraw[];
-    __shared__ double wsum[RowCfg<L>::THREADS / 32];
+    __shared__ double wsum[NWARP];
     const int lr = threadIdx.x / TPR, t = threadIdx.x % TPR;
     C *sm = reinterpret_cast<C *>(smraw) + lr * P::SMEM_ELEMS;
-    const int row = blockIdx.x * RowCfg<L>::RPC + lr;
+    const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
     const bool live = row < N;
     C reg[E];
     if (live) {
@@ -162,7 +174,7 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
 #pragma unroll
         for (int p = 0; p < E; p++) reg[p] = czero<C>();
     }
-    fft_run<L, true, false>(reg, sm, tw + L, t);
+    fft_run<L, SH::E, true, false>(reg, sm, tw + L, t);
     const long long kx = sel_index(st, xs.koff);
     const long long ky = sel_index(st, ys.koff);
     const C *x = reinterpret_cast<const C *>(xs.base) + kx * xs.stride;
@@ -196,7 +208,7 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
         __syncthreads();
         if (threadIdx.x == 0) {
             double tot = 0.0;
-            for (int w = 0; w < RowCfg<L>::THREADS / 32; w++) tot += wsum[w];
+            for (int w = 0; w < NWARP; w++) tot += wsum[w];
             npart[blockIdx.x] = tot;
         }
     }
@@ -204,19 +216,19 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
 
 // ------------------------------------------------- full transforms (setup)
 template <int L>
-__global__ void __launch_bounds__(RowCfg<L>::THREADS)
+__global__ void __launch_bounds__(RowCfg<L, MvV0>::THREADS)
 k_rows_fft_full(double2 *__restrict__ A, const double2 *__restrict__ tw) {
-    typedef Plan<L> P;
+    typedef Plan<L, 16> P;
     constexpr int E = P::E, TPR = P::TPR;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int lr = threadIdx.x / TPR, t = threadIdx.x % TPR;
     double2 *sm = reinterpret_cast<double2 *>(smraw) + lr * P::SMEM_ELEMS;
-    const int row = blockIdx.x * RowCfg<L>::RPC + lr;
+    const int row = blockIdx.x * RowCfg<L, MvV0>::RPC + lr;
     const bool live = row < L;
     double2 reg[E];
 #pragma unroll
     for (int p = 0; p < E; p++) reg[p] = live ? A[(size_t)row * L + t + p * TPR] : czero<double2>();
-    fft_run<L, false, false>(reg, sm, tw, t);
+    fft_run<L, 16, false, false>(reg, sm, tw, t);
     if (live) {
 #pragma unroll
         for (int p = 0; p < E; p++) A[(size_t)row * L + t + p * TPR] = reg[p];
@@ -224,10 +236,10 @@ k_rows_fft_full(double2 *__restrict__ A, const double2 *__restrict__ tw) {
 }
 
 template <int L>
-__global__ void __launch_bounds__(ColCfg<L, 16>::THREADS)
+__global__ void __launch_bounds__(ColCfg<L, MvV0, 16>::THREADS)
 k_cols_fft_full(double2 *__restrict__ A, const double2 *__restrict__ tw) {
-    typedef Plan<L> P;
-    typedef ColCfg<L, 16> Q;
+    typedef Plan<L, 16> P;
+    typedef ColCfg<L, MvV0, 16> Q;
     constexpr int E = P::E, TPR = P::TPR, CPB = Q::CPB;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int cl = threadIdx.x % CPB, t = threadIdx.x / CPB;
@@ -236,7 +248,7 @@ k_cols_fft_full(double2 *__restrict__ A, const double2 *__restrict__ tw) {
     double2 reg[E];
 #pragma unroll
     for (int p = 0; p < E; p++) reg[p] = A[(size_t)(t + p * TPR) * L + col];
-    fft_run<L, false, false, CPB>(reg, sm, tw, t);
+    fft_run<L, 16, false, false, CPB>(reg, sm, tw, t);
 #pragma unroll
     for (int p = 0; p < E; p++) A[(size_t)(t + p * TPR) * L + col] = reg[p];
 }
@@ -250,133 +262,170 @@ template <typename K> static int set_smem(K kern, size_t bytes) {
     return 0;
 }
 
-template <typename C, int L>
-static int rows_forward_t(const MatvecArgs &a, VecSel x, const double *xs, const DevState *st, int gate,
-                          cudaStream_t s) {
-    typedef typename real_of<C>::type R;
-    const size_t smem = (size_t)RowCfg<L>::RPC * Plan<L>::SMEM_ELEMS * sizeof(C);
-    auto kern = k_rows_forward<C, L>;
-    int e = set_smem(kern, smem);
-    if (e) return e;
-    const int grid = (a.N + RowCfg<L>::RPC - 1) / RowCfg<L>::RPC;
-    kern<<<grid, RowCfg<L>::THREADS, smem, s>>>(x, xs, (const R *)a.cdiag, (C *)a.T, (const C *)a.tw, a.N, st, gate);
-    return (int)cudaGetLastError();
+// The three passes for one launch shape SH and one embedding size L.
+template <typename SH, int L> struct Passes {
+    static int fwd(int prec, const MatvecArgs &a, VecSel x, const double *xs, const DevState *st, int gate,
+                   cudaStream_t s) {
+        typedef RowCfg<L, SH> Q;
+        const int grid = (a.N + Q::RPC - 1) / Q::RPC;
+        if (prec == 0) {
+            const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(double2);
+            auto kern = k_rows_forward<double2, L, SH>;
+            int e = set_smem(kern, smem);
+            if (e) return e;
+            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, (const double *)a.cdiag, (double2 *)a.T,
+                                                (const double2 *)a.tw, a.N, st, gate);
+        } else {
+            const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(float2);
+            auto kern = k_rows_forward<float2, L, SH>;
+            int e = set_smem(kern, smem);
+            if (e) return e;
+            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, (const float *)a.cdiag, (float2 *)a.T, (const float2 *)a.tw,
+                                                a.N, st, gate);
+        }
+        return (int)cudaGetLastError();
+    }
+
+    template <typename C> static int cols_t(const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
+        typedef ColCfg<L, SH, sizeof(C)> Q;
+        const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
+        auto kern = k_cols_convolve<C, L, SH>;
+        int e = set_smem(kern, smem);
+        if (e) return e;
+        kern<<<L / Q::CPB, Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate);
+        return (int)cudaGetLastError();
+    }
+    static int cols(int prec, const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
+        return prec == 0 ? cols_t<double2>(a, st, gate, s) : cols_t<float2>(a, st, gate, s);
+    }
+
+    template <typename C, typename CO, int MODE>
+    static int inv_t(const MatvecArgs &a, VecSel x, const double *xs, const void *b, VecSel y, double *npart,
+                     const DevState *st, int gate, cudaStream_t s) {
+        typedef RowCfg<L, SH> Q;
+        const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
+        auto kern = k_rows_inverse<C, CO, L, MODE, SH>;
+        int e = set_smem(kern, smem);
+        if (e) return e;
+        const int grid = (a.N + Q::RPC - 1) / Q::RPC;
+        kern<<<grid, Q::THREADS, smem, s>>>((const C *)a.T, x, xs, (const C *)b, y, npart, (const C *)a.tw, a.N,
+                                              st, gate);
+        return (int)cudaGetLastError();
+    }
+    static int inv(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xs, const void *b,
+                   VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s) {
+        if (prec == 0) {
+            if (mode == 0) return inv_t<double2, double2, 0>(a, x, xs, b, y, npart, st, gate, s);
+            return out_prec == 0 ? inv_t<double2, double2, 1>(a, x, xs, b, y, npart, st, gate, s)
+                                 : inv_t<double2, float2, 1>(a, x, xs, b, y, npart, st, gate, s);
+        }
+        if (mode == 0) return inv_t<float2, float2, 0>(a, x, xs, b, y, npart, st, gate, s);
+        return inv_t<float2, float2, 1>(a, x, xs, b, y, npart, st, gate, s);
+    }
+    static int rpc() { return RowCfg<L, SH>::RPC; }
+};
+
+// Calls F<Passes<SH, L>>::run(args...) for the shape selected by `variant`
+// (L >= 256) or variant 0 (smaller L).
+template <template <typename> class F, typename... A> static int dispatch(int variant, int L, A... args) {
+    switch (L) {
+        case 16: return F<Passes<MvV0, 16>>::run(args...);
+        case 32: return F<Passes<MvV0, 32>>::run(args...);
+        case 64: return F<Passes<MvV0, 64>>::run(args...);
+        case 128: return F<Passes<MvV0, 128>>::run(args...);
+        default: break;
+    }
+#define CG_V_CASES(SH)                                            \
+    switch (L) {                                                  \
+        case 256: return F<Passes<SH, 256>>::run(args...);        \
+        case 512: return F<Passes<SH, 512>>::run(args...);        \
+        case 1024: return F<Passes<SH, 1024>>::run(args...);      \
+        case 2048: return F<Passes<SH, 2048>>::run(args...);      \
+        case 4096: return F<Passes<SH, 4096>>::run(args...);      \
+        default: return -1;                                       \
+    }
+    switch (variant) {
+        case 0: CG_V_CASES(MvV0)
+        case 1: CG_V_CASES(MvV1)
+        case 2: CG_V_CASES(MvV2)
+        case 3: CG_V_CASES(MvV3)
+        default: return -1;
+    }
+#undef CG_V_CASES
 }
 
-template <typename C, int L>
-static int cols_convolve_t(const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
-    typedef ColCfg<L, sizeof(C)> Q;
-    const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
-    auto kern = k_cols_convolve<C, L>;
-    int e = set_smem(kern, smem);
-    if (e) return e;
-    const int grid = L / Q::CPB;
-    kern<<<grid, Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate);
-    return (int)cudaGetLastError();
-}
-
-template <typename C, typename CO, int L, int MODE>
-static int rows_inverse_t(const MatvecArgs &a, VecSel x, const double *xs, const void *b, VecSel y, double *npart,
-                          const DevState *st, int gate, cudaStream_t s) {
-    const size_t smem = (size_t)RowCfg<L>::RPC * Plan<L>::SMEM_ELEMS * sizeof(C);
-    auto kern = k_rows_inverse<C, CO, L, MODE>;
-    int e = set_smem(kern, smem);
-    if (e) return e;
-    const int grid = (a.N + RowCfg<L>::RPC - 1) / RowCfg<L>::RPC;
-    kern<<<grid, RowCfg<L>::THREADS, smem, s>>>((const C *)a.T, x, xs, (const C *)b, y, npart, (const C *)a.tw, a.N,
-                                                 st, gate);
-    return (int)cudaGetLastError();
-}
-
-template <int L> static int fft2d_full_t(double2 *A, const double2 *tw, cudaStream_t s) {
-    size_t smem = (size_t)RowCfg<L>::RPC * Plan<L>::SMEM_ELEMS * sizeof(double2);
-    auto kr = k_rows_fft_full<L>;
-    int e = set_smem(kr, smem);
-    if (e) return e;
-    kr<<<(L + RowCfg<L>::RPC - 1) / RowCfg<L>::RPC, RowCfg<L>::THREADS, smem, s>>>(A, tw);
-    e = (int)cudaGetLastError();
-    if (e) return e;
-    typedef ColCfg<L, 16> Q;
-    smem = (size_t)Q::SMEM_ELEMS * sizeof(double2);
-    auto kc = k_cols_fft_full<L>;
-    e = set_smem(kc, smem);
-    if (e) return e;
-    kc<<<L / Q::CPB, Q::THREADS, smem, s>>>(A, tw);
-    return (int)cudaGetLastError();
-}
-
-#define CG_FOR_EACH_L(X) X(16) X(32) X(64) X(128) X(256) X(512) X(1024) X(2048) X(4096)
+template <typename PS> struct FwdF {
+    static int run(int prec, const MatvecArgs *a, VecSel x, const double *xs, const DevState *st, int gate,
+                   cudaStream_t s) {
+        return PS::fwd(prec, *a, x, xs, st, gate, s);
+    }
+};
+template <typename PS> struct ColsF {
+    static int run(int prec, const MatvecArgs *a, const DevState *st, int gate, cudaStream_t s) {
+        return PS::cols(prec, *a, st, gate, s);
+    }
+};
+template <typename PS> struct InvF {
+    static int run(int prec, int mode, int out_prec, const MatvecArgs *a, VecSel x, const double *xs, const void *b,
+                   VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s) {
+        return PS::inv(prec, mode, out_prec, *a, x, xs, b, y, npart, st, gate, s);
+    }
+};
+template <typename PS> struct RpcF {
+    static int run() { return PS::rpc(); }
+};
 
 int fft_supported(int L) {
-    switch (L) {
-#define CASE(LL) case LL:
-        CG_FOR_EACH_L(CASE)
-#undef CASE
-        return 1;
-        default: return 0;
-    }
+    return L == 16 || L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 1024 || L == 2048 || L == 4096;
 }
 
-int rows_per_block(int prec, int L) {
-    (void)prec;
-    switch (L) {
-#define CASE(LL) \
-    case LL: return RowCfg<LL>::RPC;
-        CG_FOR_EACH_L(CASE)
-#undef CASE
-        default: return 1;
-    }
-}
+int matvec_variants(int L) { return L >= 256 ? MV_VARIANTS : 1; }
+
+int rows_per_block(int variant, int L) { return dispatch<RpcF>(variant, L); }
 
 int launch_rows_forward(int prec, const MatvecArgs &a, VecSel x, const double *xs, const DevState *st, int gate,
                         cudaStream_t s) {
-    switch (a.L) {
-#define CASE(LL)                                                                           \
-    case LL:                                                                               \
-        return prec == 0 ? rows_forward_t<double2, LL>(a, x, xs, st, gate, s)             \
-                         : rows_forward_t<float2, LL>(a, x, xs, st, gate, s);
-        CG_FOR_EACH_L(CASE)
-#undef CASE
-        default: return -1;
-    }
+    return dispatch<FwdF>(a.vfwd, a.L, prec, &a, x, xs, st, gate, s);
 }
 
 int launch_cols_convolve(int prec, const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
-    switch (a.L) {
-#define CASE(LL)                                                                                      \
-    case LL:                                                                                          \
-        return prec == 0 ? cols_convolve_t<double2, LL>(a, st, gate, s) : cols_convolve_t<float2, LL>(a, st, gate, s);
-        CG_FOR_EACH_L(CASE)
-#undef CASE
-        default: return -1;
-    }
+    return dispatch<ColsF>(a.vcols, a.L, prec, &a, st, gate, s);
 }
 
 int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xs,
                         const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s) {
-    switch (a.L) {
-#define CASE(LL)                                                                                         \
-    case LL:                                                                                             \
-        if (prec == 0) {                                                                                 \
-            if (mode == 0)                                                                               \
-                return rows_inverse_t<double2, double2, LL, 0>(a, x, xs, b, y, npart, st, gate, s);      \
-            return out_prec == 0 ? rows_inverse_t<double2, double2, LL, 1>(a, x, xs, b, y, npart, st, gate, s) \
-                                 : rows_inverse_t<double2, float2, LL, 1>(a, x, xs, b, y, npart, st, gate, s); \
-        }                                                                                                \
-        if (mode == 0) return rows_inverse_t<float2, float2, LL, 0>(a, x, xs, b, y, npart, st, gate, s); \
-        return rows_inverse_t<float2, float2, LL, 1>(a, x, xs, b, y, npart, st, gate, s);
-        CG_FOR_EACH_L(CASE)
-#undef CASE
-        default: return -1;
-    }
+    return dispatch<InvF>(a.vinv, a.L, prec, mode, out_prec, &a, x, xs, b, y, npart, st, gate, s);
+}
+
+template <int L> static int fft2d_full_t(double2 *A, const double2 *tw, cudaStream_t s) {
+    typedef RowCfg<L, MvV0> QR;
+    typedef ColCfg<L, MvV0, 16> QC;
+    size_t smem = (size_t)QR::SMEM_ELEMS * sizeof(double2);
+    auto kr = k_rows_fft_full<L>;
+    int e = set_smem(kr, smem);
+    if (e) return e;
+    kr<<<(L + QR::RPC - 1) / QR::RPC, QR::THREADS, smem, s>>>(A, tw);
+    e = (int)cudaGetLastError();
+    if (e) return e;
+    smem = (size_t)QC::SMEM_ELEMS * sizeof(double2);
+    auto kc = k_cols_fft_full<L>;
+    e = set_smem(kc, smem);
+    if (e) return e;
+    kc<<<L / QC::CPB, QC::THREADS, smem, s>>>(A, tw);
+    return (int)cudaGetLastError();
 }
 
 int launch_fft2d_full_fp64(int L, double2 *A, const double2 *tw, cudaStream_t s) {
     switch (L) {
-#define CASE(LL) \
-    case LL: return fft2d_full_t<LL>(A, tw, s);
-        CG_FOR_EACH_L(CASE)
-#undef CASE
+        case 16: return fft2d_full_t<16>(A, tw, s);
+        case 32: return fft2d_full_t<32>(A, tw, s);
+        case 64: return fft2d_full_t<64>(A, tw, s);
+        case 128: return fft2d_full_t<128>(A, tw, s);
+        case 256: return fft2d_full_t<256>(A, tw, s);
+        case 512: return fft2d_full_t<512>(A, tw, s);
+        case 1024: return fft2d_full_t<1024>(A, tw, s);
+        case 2048: return fft2d_full_t<2048>(A, tw, s);
+        case 4096: return fft2d_full_t<4096>(A, tw, s);
         default: return -1;
     }
 }

@@ -137,6 +137,7 @@ extern "C" int cugmres_matvec_noalloc(int N, const cg_c128 *g_block, const doubl
     cg::MatvecArgs a;
     a.N = N;
     a.L = L;
+    a.vfwd = a.vcols = a.vinv = 0;
     a.gq = quarter;
     a.cdiag = c;
     a.tw = tw;

@@ -74,6 +74,20 @@ def gaussian_field(N, seed, corr=4.0):
     return np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
 
 
+def sweep(nsys=256, seed=0, sides=(96, 128, 192, 256, 384, 512), lam_over_h=(15.0, 30.0), eps_range=(2.0, 12.0)):
+    """Seeded sweep of independent systems: grid side drawn from `sides`,
+    wavelength / cell size uniform in `lam_over_h`, eps_r uniform in
+    `eps_range`, one design seed each (the same field construction)."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nsys):
+        N = int(rng.choice(sides))
+        lh = float(rng.uniform(*lam_over_h))
+        eps = float(rng.uniform(*eps_range))
+        out.append(helmholtz(N, eps, seed=int(rng.integers(1 << 30)), cells_per_wavelength=lh))
+    return out
+
+
 def helmholtz(N, eps_r, seed=0, cells_per_wavelength=20.0, wavelength=1.0, corr=4.0, fill=0.75):
     k0 = 2.0 * np.pi / wavelength
     h = wavelength / cells_per_wavelength

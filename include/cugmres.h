@@ -121,6 +121,12 @@ int cugmres_set_operator(cg_ctx *ctx, int N, const cg_c128 *g_block, const doubl
  * its first N x N block is the g_block. */
 int cugmres_set_operator_circulant(cg_ctx *ctx, int N, const cg_c64 *g_prep, const double *chi, double chi_scale);
 int cugmres_grid_size(const cg_ctx *ctx, int *N, int *L);
+/* Launch shapes the autotuner chose for the three matvec passes (row forward,
+ * column convolution, row inverse) of `precision`; shapes[3] receives indices
+ * 0..3 (0 for embeddings L < 256).  Tuning runs in cugmres_set_operator and is
+ * cached per device in $CUGMRES_TUNE_CACHE (default
+ * ~/.cache/cugmres_b200/autotune.txt); CUGMRES_AUTOTUNE=0 keeps shape 0. */
+int cugmres_matvec_shapes(const cg_ctx *ctx, int precision, int *shapes);
 
 /* y = A x.  precision CG_PREC_FP64: x, y are cg_c128 arrays; CG_PREC_MIXED:
  * cg_c64 arrays computed with the FP32 spectrum. */
@@ -133,6 +139,26 @@ int cugmres_residual(cg_ctx *ctx, const cg_c128 *b, const cg_c128 *x, cg_c128 *r
  * relative residuals: [0] = ||b - A x0|| / ||b||, [i] = estimate after step i. */
 int cugmres_solve(cg_ctx *ctx, const cg_c128 *b, cg_c128 *x, const cg_opts *opts, double *res_hist,
                   int res_hist_len, cg_result *result);
+
+/* One independent system of a batched sweep (pointers host or device). */
+typedef struct {
+    int N;
+    const cg_c128 *g_block; /* N x N Green's block (cugmres_green_block)  */
+    const double *chi;      /* N x N contrast                              */
+    double chi_scale;       /* A = I - G diag(chi_scale * chi)             */
+    const cg_c128 *b;       /* right-hand side                             */
+    cg_c128 *x;             /* x0 on entry (unless opts->zero_x0), solution */
+} cg_system;
+
+/* Solves nsys independent systems (any mix of grid sizes) on `device` with
+ * `nworkers` concurrent contexts, each with its own stream; systems are taken
+ * largest grid first.  The batched counterpart of the reference's sweep over
+ * sizes and repetitions (CUDA_GMRES/launch_GMRES.cuh:88-235).  results[i]
+ * holds system i's status, iterations, residuals and latency (operator set-up
+ * plus solve, seconds).  Returns CG_OK unless a context could not be created
+ * or a CUDA error occurred; per-system convergence is in results[i].status. */
+int cugmres_solve_batch(int device, int nsys, const cg_system *systems, const cg_opts *opts, int nworkers,
+                        cg_result *results);
 
 /* Per-phase device timing of cugmres_solve, the counterpart of the reference's
  * clock_gettime step stamps (CUDA_GMRES/GMRES.cuh:39-445, labels in

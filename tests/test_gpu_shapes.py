@@ -1,0 +1,42 @@
+"""Every matvec launch shape the autotuner may pick gives the same operator."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+pytestmark = pytest.mark.gpu
+
+SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import cugmres_b200 as cg
+from cugmres_b200 import problems as P
+from oracle import oracle as O
+for N in (128, 300, 512):
+    pr = P.helmholtz(N, 4.0, seed=N)
+    s = cg.Solver(0).set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x = np.random.default_rng(N).standard_normal((N, N)) + 1j
+    y = s.matvec(x)
+    yo = O.matvec(O.spectrum(pr["g_block"], s.L), pr["chi"] * pr["chi_scale"], x)
+    e64 = np.abs(y - yo).max() / np.abs(yo).max()
+    y32 = s.matvec(x.astype(np.complex64), precision="fp32")
+    e32 = np.abs(y32 - yo).max() / np.abs(yo).max()
+    print(N, s.matvec_shapes("fp64"), s.matvec_shapes("fp32"), e64, e32)
+    assert e64 < 1e-13 and e32 < 2e-6, (e64, e32)
+"""
+
+
+@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "tuned"])
+def test_matvec_shape_parity(cuda_device, shape, tmp_path):
+    env = dict(os.environ)
+    env["CUGMRES_TUNE_CACHE"] = str(tmp_path / "tune.txt")
+    if shape != "tuned":
+        env["CUGMRES_MATVEC_SHAPE"] = shape
+    r = subprocess.run([sys.executable, "-c", SCRIPT, ROOT], env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stdout + r.stderr
+    if shape == "tuned":
+        assert os.path.exists(env["CUGMRES_TUNE_CACHE"])
