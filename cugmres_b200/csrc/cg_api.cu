@@ -229,7 +229,8 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
         CG_CU(cudaMalloc((void **)&c->kp.y, sizeof(double2) * mc));
         CG_CU(cudaMalloc((void **)&c->kp.hist, sizeof(double) * (ic + 1)));
         const size_t part_cgs2 = 2 * (size_t)dot_blocks(c) * (mc + 1);
-        const size_t part_dcgs2 = 4 * (size_t)dots2_blocks(c->sms) * (size_t)std::max(mc + 1, 32);
+        const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms), dots2_blocks(1, c->sms)) *
+                                  (size_t)dots2_part_ld(mc);
         CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(part_cgs2, part_dcgs2)));
         CG_CU(cudaMalloc((void **)&c->kp.npart, sizeof(double) * np));
         CG_CU(cudaMalloc((void **)&c->kp.Hm, sizeof(double2) * (size_t)(mc + 1) * (mc + 1)));
@@ -830,7 +831,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     vk1.koff = 1;
     VecSel xs = fixed_vec(xp);
     const int nrb = row_blocks(c);
-    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(c->sms);
+    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(prec, c->sms);
+    const int nax2 = axpy2_blocks(prec, c->sms, c->mcap);
     int status = CG_OK;
 
     CycleProf cp;
@@ -869,7 +871,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
                 CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
                 CG_LAUNCH(launch_dcgs2_step(kp, s));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, s));
-                CG_LAUNCH(launch_axpy2(prec, c->V, n, kp, nax, s));
+                CG_LAUNCH(launch_axpy2(prec, c->V, n, kp, nax2, s));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
                 continue;
             }

@@ -25,6 +25,8 @@
 // squares problem runs one step behind and a cycle of m columns makes m+1
 // operator applications.  The identities assume Q orthonormal; they were
 // checked against plain CGS2 (Q and H agree to 2e-15).
+#include <stdlib.h>
+
 #include "cg_common.cuh"
 #include "cg_internal.h"
 
@@ -32,15 +34,22 @@ namespace cg {
 
 static constexpr int D2_THREADS = 256;
 static constexpr int D2_WARPS = D2_THREADS / 32;
-static constexpr int D2_J = 4;  // basis vectors per warp work item
+// basis vectors per warp work item (J) and elements per lane per loop trip (U)
+// are template parameters of k_dots2; variant table below
 static constexpr int AX2_THREADS = 256;
 static constexpr int STEP_THREADS = 256;
 
-int dots2_blocks(int sms) { return 4 * sms; }
-
-static __device__ __forceinline__ int part_ld(const KrylovPtrs &kp) {
-    return kp.mcap + 1 > 32 ? kp.mcap + 1 : 32;
+// Grids are sized to whole waves: SMs x resident blocks per SM of the kernel.
+template <typename K> static int waves_grid(K kern, int threads, size_t smem, int sms) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    return per_sm * sms;
 }
+
+static __device__ __forceinline__ int part_ld(const KrylovPtrs &kp) { return dots2_part_ld(kp.mcap); }
 
 static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
     __shared__ bool is_last;
@@ -60,7 +69,7 @@ static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
 // For j = 0..k: D1[j] = <V_j, u_k>, D2[j] = <V_j, w> with u_k = V[k], w = V[k+1].
 // Work items: groups of D2_J basis vectors; when there are fewer groups than
 // warps, each group's element range is split into S slices.
-template <typename CV, bool COMP>
+template <typename CV, bool COMP, int D2_J, int U>
 __global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     DevState *st = kp.st;
     if (st->stop) return;
@@ -73,10 +82,25 @@ __global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, 
     const long long b0 = (long long)blockIdx.x * chunk < n ? (long long)blockIdx.x * chunk : n;
     const long long b1 = b0 + chunk < n ? b0 + chunk : n;
     const int ng = (nj + D2_J - 1) / D2_J;
-    const int S = ng >= D2_WARPS ? 1 : D2_WARPS / ng;
+    const int pld = part_ld(kp);
+    // split each group's element range into S slices so that the items fill
+    // whole rounds of the block's warps (S * nj partials must fit pld)
+    int S = 1;
+    {
+        double best = -1.0;
+        for (int cand = 1; cand <= 8; cand++) {
+            if (cand * nj > pld) break;
+            const int itc = ng * cand;
+            const int rounds = (itc + D2_WARPS - 1) / D2_WARPS;
+            const double eff = (double)itc / (double)(rounds * D2_WARPS) - 0.02 * cand;
+            if (eff > best) {
+                best = eff;
+                S = cand;
+            }
+        }
+    }
     const int items = ng * S;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int pld = part_ld(kp);
     for (int it = warp; it < items; it += D2_WARPS) {
         const int grp = it / S, sl = it % S;
         const int j0 = grp * D2_J;
@@ -110,7 +134,7 @@ __global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, 
 #pragma unroll
                     for (int q = 0; q < D2_J; q++) {
                         if (q < jn) {
-                            const CV a = vj[q][e];
+                            const CV a = __ldcs(vj[q] + e);
                             run[q][0] = fmaf(a.x, uu.x, fmaf(a.y, uu.y, run[q][0]));
                             run[q][1] = fmaf(a.x, uu.y, fmaf(-a.y, uu.x, run[q][1]));
                             run[q][2] = fmaf(a.x, ww.x, fmaf(a.y, ww.y, run[q][2]));
@@ -138,25 +162,35 @@ __global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, 
 #pragma unroll
                 for (int r = 0; r < 4; r++) acc[q][r] = 0;
             long long e = e0 + lane;
-            for (; e + 32 < e1; e += 64) {
-                const CV u0 = u[e], w0 = w[e], u1 = u[e + 32], w1 = w[e + 32];
+            for (; e + 32 * (U - 1) < e1; e += 32 * U) {
+                CV uu[U], ww[U];
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    uu[t] = u[e + 32 * t];
+                    ww[t] = w[e + 32 * t];
+                }
 #pragma unroll
                 for (int q = 0; q < D2_J; q++) {
                     if (q < jn) {
-                        const CV a0 = vj[q][e], a1 = vj[q][e + 32];
-                        acc[q][0] += a0.x * u0.x + a0.y * u0.y + (a1.x * u1.x + a1.y * u1.y);
-                        acc[q][1] += a0.x * u0.y - a0.y * u0.x + (a1.x * u1.y - a1.y * u1.x);
-                        acc[q][2] += a0.x * w0.x + a0.y * w0.y + (a1.x * w1.x + a1.y * w1.y);
-                        acc[q][3] += a0.x * w0.y - a0.y * w0.x + (a1.x * w1.y - a1.y * w1.x);
+                        CV a[U];
+#pragma unroll
+                        for (int t = 0; t < U; t++) a[t] = __ldcs(vj[q] + e + 32 * t);
+#pragma unroll
+                        for (int t = 0; t < U; t++) {
+                            acc[q][0] += a[t].x * uu[t].x + a[t].y * uu[t].y;
+                            acc[q][1] += a[t].x * uu[t].y - a[t].y * uu[t].x;
+                            acc[q][2] += a[t].x * ww[t].x + a[t].y * ww[t].y;
+                            acc[q][3] += a[t].x * ww[t].y - a[t].y * ww[t].x;
+                        }
                     }
                 }
             }
-            if (e < e1) {
+            for (; e < e1; e += 32) {
                 const CV u0 = u[e], w0 = w[e];
 #pragma unroll
                 for (int q = 0; q < D2_J; q++) {
                     if (q < jn) {
-                        const CV a0 = vj[q][e];
+                        const CV a0 = __ldcs(vj[q] + e);
                         acc[q][0] += a0.x * u0.x + a0.y * u0.y;
                         acc[q][1] += a0.x * u0.y - a0.y * u0.x;
                         acc[q][2] += a0.x * w0.x + a0.y * w0.y;
@@ -346,7 +380,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
 // --------------------------------------------------------------- axpy2
 // q_k = cu u - sum_j P_j q_j into V[k];  u_{k+1} = cw w + du u - sum_j S_j q_j into V[k+1]
 // (k = st->k - 1: the step kernel has advanced the index).
-template <typename CV>
+template <typename CV, int JU>
 __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
@@ -391,14 +425,18 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
         const CV uu = u[e], ww = w[e];
         CV sp = czero<CV>(), ss = czero<CV>();
         int j = 0;
-        for (; j + 4 <= k; j += 4) {
-            const CV q0 = V[(long long)j * n + e], q1 = V[(long long)(j + 1) * n + e];
-            const CV q2 = V[(long long)(j + 2) * n + e], q3 = V[(long long)(j + 3) * n + e];
-            sp = cadd(sp, cadd(cadd(cmul(Pc[j], q0), cmul(Pc[j + 1], q1)), cadd(cmul(Pc[j + 2], q2), cmul(Pc[j + 3], q3))));
-            ss = cadd(ss, cadd(cadd(cmul(Sc[j], q0), cmul(Sc[j + 1], q1)), cadd(cmul(Sc[j + 2], q2), cmul(Sc[j + 3], q3))));
+        for (; j + JU <= k; j += JU) {
+            CV q[JU];
+#pragma unroll
+            for (int t = 0; t < JU; t++) q[t] = __ldcs(V + (long long)(j + t) * n + e);
+#pragma unroll
+            for (int t = 0; t < JU; t++) {
+                sp = cadd(sp, cmul(Pc[j + t], q[t]));
+                ss = cadd(ss, cmul(Sc[j + t], q[t]));
+            }
         }
         for (; j < k; j++) {
-            const CV q0 = V[(long long)j * n + e];
+            const CV q0 = __ldcs(V + (long long)j * n + e);
             sp = cadd(sp, cmul(Pc[j], q0));
             ss = cadd(ss, cmul(Sc[j], q0));
         }
@@ -408,9 +446,58 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 }
 
 // ------------------------------------------------------------- launchers
+// Shapes of the two streaming passes: (J, U) of k_dots2 and the j-unroll of
+// k_axpy2, per precision.  The defaults were chosen by measurement on B200 at
+// N = 1024, restart 100 (300 steps, k = 0..99): FP64 dots (2,4) 81.7 ms vs
+// (4,2) 92.9 ms, FP32 dots (2,2) 80.3 ms vs (4,2) 99.4 ms; FP64 axpy unroll 4,
+// FP32 axpy unroll 8 (36.4 ms vs 43.2 ms).  CUGMRES_DOTS2_SHAPE /
+// CUGMRES_AXPY2_SHAPE override both precisions (diagnostics).
+static int env_shape(const char *name, int nshapes) {
+    const char *e = getenv(name);
+    if (!e || !*e) return -1;
+    const int v = atoi(e);
+    return (v >= 0 && v < nshapes) ? v : -1;
+}
+static int dots2_shape(int prec_v) {
+    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 5);
+    return v >= 0 ? v : (prec_v == 0 ? 4 : 1);
+}
+static int axpy2_shape(int prec_v) {
+    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 3);
+    return v >= 0 ? v : (prec_v == 0 ? 0 : 2);
+}
+
+template <typename CV, bool COMP> struct Dots2Table {
+    typedef void (*K)(const CV *, long long, KrylovPtrs);
+    static K get(int v) {
+        switch (v) {
+            case 1: return k_dots2<CV, COMP, 2, 2>;
+            case 2: return k_dots2<CV, COMP, 4, 1>;
+            case 3: return k_dots2<CV, COMP, 8, 1>;
+            case 4: return k_dots2<CV, COMP, 2, 4>;
+            default: return k_dots2<CV, COMP, 4, 2>;
+        }
+    }
+};
+template <typename CV> struct Axpy2Table {
+    typedef void (*K)(CV *, long long, KrylovPtrs);
+    static K get(int v) {
+        switch (v) {
+            case 1: return k_axpy2<CV, 2>;
+            case 2: return k_axpy2<CV, 8>;
+            default: return k_axpy2<CV, 4>;
+        }
+    }
+};
+
+int dots2_blocks(int prec_v, int sms) {
+    return prec_v == 0 ? waves_grid(Dots2Table<double2, false>::get(dots2_shape(0)), D2_THREADS, 0, sms)
+                       : waves_grid(Dots2Table<float2, true>::get(dots2_shape(1)), D2_THREADS, 0, sms);
+}
+
 int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s) {
-    if (prec_v == 0) k_dots2<double2, false><<<nblk, D2_THREADS, 0, s>>>((const double2 *)V, n, kp);
-    else k_dots2<float2, true><<<nblk, D2_THREADS, 0, s>>>((const float2 *)V, n, kp);
+    if (prec_v == 0) Dots2Table<double2, false>::get(dots2_shape(0))<<<nblk, D2_THREADS, 0, s>>>((const double2 *)V, n, kp);
+    else Dots2Table<float2, true>::get(dots2_shape(1))<<<nblk, D2_THREADS, 0, s>>>((const float2 *)V, n, kp);
     return (int)cudaGetLastError();
 }
 
@@ -425,21 +512,29 @@ int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s) {
     return (int)cudaGetLastError();
 }
 
+template <typename CV> static int axpy2_prepare(size_t smem) {
+    if (smem > 48 * 1024)
+        return (int)cudaFuncSetAttribute(Axpy2Table<CV>::get(axpy2_shape(sizeof(CV) == sizeof(double2) ? 0 : 1)), cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    return 0;
+}
+
+int axpy2_blocks(int prec_v, int sms, int mcap) {
+    const size_t smem = 2 * (size_t)(mcap + 1) * (prec_v == 0 ? sizeof(double2) : sizeof(float2));
+    if (prec_v == 0) {
+        axpy2_prepare<double2>(smem);
+        return waves_grid(Axpy2Table<double2>::get(axpy2_shape(0)), AX2_THREADS, smem, sms);
+    }
+    axpy2_prepare<float2>(smem);
+    return waves_grid(Axpy2Table<float2>::get(axpy2_shape(1)), AX2_THREADS, smem, sms);
+}
+
 int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s) {
     const size_t smem = 2 * (size_t)(kp.mcap + 1) * (prec_v == 0 ? sizeof(double2) : sizeof(float2));
-    if (prec_v == 0) {
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k_axpy2<double2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return (int)e;
-        }
-        k_axpy2<double2><<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
-    } else {
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(k_axpy2<float2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return (int)e;
-        }
-        k_axpy2<float2><<<nblk, AX2_THREADS, smem, s>>>((float2 *)V, n, kp);
-    }
+    int e = prec_v == 0 ? axpy2_prepare<double2>(smem) : axpy2_prepare<float2>(smem);
+    if (e) return e;
+    if (prec_v == 0) Axpy2Table<double2>::get(axpy2_shape(0))<<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
+    else Axpy2Table<float2>::get(axpy2_shape(1))<<<nblk, AX2_THREADS, smem, s>>>((float2 *)V, n, kp);
     return (int)cudaGetLastError();
 }
 

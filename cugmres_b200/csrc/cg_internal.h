@@ -103,7 +103,10 @@ int launch_givens(const KrylovPtrs &kp, cudaStream_t s);
 int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
 int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s);
 int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
-int dots2_blocks(int sms);
+int dots2_blocks(int prec_v, int sms);
+int axpy2_blocks(int prec_v, int sms, int mcap);
+// partials per block of the two-RHS dot pass
+__host__ __device__ inline int dots2_part_ld(int mcap) { return 2 * (mcap + 1) > 64 ? 2 * (mcap + 1) : 64; }
 int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s);
 int launch_cycle_begin(const KrylovPtrs &kp, int nparts, cudaStream_t s);
 int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
