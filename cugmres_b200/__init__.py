@@ -154,10 +154,23 @@ class Solver:
                                           ctypes.byref(rel)), "residual")
         return r, rel.value
 
+    def set_preconditioner(self, net, k0h=None):
+        """Attach a learned.FNO (or None to detach) for solve(preconditioner="learned");
+        k0h = k0 * h of the current operator."""
+        if net is None:
+            check(_lib.lib().cugmres_set_preconditioner(self._ctx, None, 0.0), "set_preconditioner")
+            self._net = None
+            return
+        check(_lib.lib().cugmres_set_preconditioner(self._ctx, net._net, float(k0h)), "set_preconditioner")
+        self._net = net  # keep the network alive while attached
+
     def solve(self, b, x0=None, restart=100, max_iter=10000, tol=1e-10, precision="fp64", givens="unitary",
-              inner_tol=1e-5, fixed_iterations=False, timeout_s=0.0, ortho="dcgs2", raise_on_failure=False):
+              inner_tol=1e-5, fixed_iterations=False, timeout_s=0.0, ortho="dcgs2", raise_on_failure=False,
+              preconditioner=None, learned_x0=False):
         """Solve A x = b.  Returns (x, info) where info holds status, iterations,
-        cycles, rel_residual_true / _estimate, seconds and res_hist."""
+        cycles, rel_residual_true / _estimate, seconds and res_hist.
+        preconditioner="learned": flexible GMRES with the attached network
+        (learned_x0: also start from x0 = M(b) when x0 is None)."""
         o = _lib.CgOpts()
         _lib.lib().cugmres_default_opts(ctypes.byref(o))
         o.restart = int(restart)
@@ -169,6 +182,8 @@ class Solver:
         o.fixed_iterations = int(bool(fixed_iterations))
         o.timeout_s = float(timeout_s)
         o.ortho = _ORTHO[ortho]
+        o.preconditioner = {None: 0, "none": 0, "learned": 1}[preconditioner]
+        o.learned_x0 = int(bool(learned_x0))
         bp, bk = _arg(b, np.complex128)
         if x0 is None:
             o.zero_x0 = 1
@@ -185,7 +200,8 @@ class Solver:
             raise CugmresError(st, "cugmres_solve")
         info = dict(status=st, status_text=_lib.strerror(st), iterations=res.iterations, cycles=res.cycles,
                     rel_residual_estimate=res.rel_residual_estimate, rel_residual_true=res.rel_residual_true,
-                    seconds=res.seconds, res_hist=hist[: res.iterations + 1].copy())
+                    seconds=res.seconds, res_hist=hist[: res.iterations + 1].copy(),
+                    preconditioned_cycles=res.preconditioned_cycles, x0_learned=res.x0_learned)
         return xk, info
 
 

@@ -37,10 +37,12 @@ EXPORTS = (
     "cugmres_set_stream", "cugmres_synchronize", "cugmres_green_block", "cugmres_set_operator",
     "cugmres_set_operator_circulant", "cugmres_grid_size", "cugmres_matvec", "cugmres_residual",
     "cugmres_solve", "cugmres_fast_gmres", "cugmres_profile", "cugmres_profile_read", "cugmres_matvec_noalloc",
-    "cugmres_matvec_shapes", "cugmres_solve_batch",
+    "cugmres_matvec_shapes", "cugmres_solve_batch", "cugmres_fno_create", "cugmres_fno_destroy",
+    "cugmres_fno_info", "cugmres_fno_get_params", "cugmres_fno_set_params", "cugmres_fno_forward",
+    "cugmres_fno_loss_grad", "cugmres_fno_train_step", "cugmres_set_preconditioner", "cugmres_gemm_bf16",
 )
 
-PHASES = ("matvec", "dots", "axpy", "small", "update", "residual")
+PHASES = ("matvec", "dots", "axpy", "small", "update", "residual", "precond")
 
 
 class CgOpts(ctypes.Structure):
@@ -55,7 +57,9 @@ class CgOpts(ctypes.Structure):
         ("fixed_iterations", ctypes.c_int),
         ("timeout_s", ctypes.c_double),
         ("ortho", ctypes.c_int),
-        ("reserved", ctypes.c_int * 7),
+        ("preconditioner", ctypes.c_int),
+        ("learned_x0", ctypes.c_int),
+        ("reserved", ctypes.c_int * 5),
     ]
 
 
@@ -67,6 +71,21 @@ class CgResult(ctypes.Structure):
         ("rel_residual_estimate", ctypes.c_double),
         ("rel_residual_true", ctypes.c_double),
         ("seconds", ctypes.c_double),
+        ("preconditioned_cycles", ctypes.c_int),
+        ("x0_learned", ctypes.c_int),
+    ]
+
+
+class CgFnoInfo(ctypes.Structure):
+    _fields_ = [
+        ("layers", ctypes.c_int),
+        ("width", ctypes.c_int),
+        ("modes1", ctypes.c_int),
+        ("modes2", ctypes.c_int),
+        ("hidden", ctypes.c_int),
+        ("in_features", ctypes.c_int),
+        ("num_params", ctypes.c_longlong),
+        ("steps", ctypes.c_longlong),
     ]
 
 
@@ -132,8 +151,20 @@ def _declare(L):
                                       ctypes.POINTER(CgResult)]
     L.cugmres_profile.argtypes = [P, I]
     L.cugmres_profile_read.argtypes = [P, ctypes.POINTER(CgPhaseStats)]
+    LL, ULL = ctypes.c_longlong, ctypes.c_ulonglong
+    L.cugmres_fno_create.argtypes = [ctypes.POINTER(P), I, ULL]
+    L.cugmres_fno_destroy.argtypes = [P]
+    L.cugmres_fno_destroy.restype = None
+    L.cugmres_fno_info.argtypes = [P, ctypes.POINTER(CgFnoInfo)]
+    L.cugmres_fno_get_params.argtypes = [P, P]
+    L.cugmres_fno_set_params.argtypes = [P, P]
+    L.cugmres_fno_forward.argtypes = [P, I, I, I, P, P, P, P]
+    L.cugmres_fno_loss_grad.argtypes = [P, I, I, I, P, P, P, P, ctypes.POINTER(F), P]
+    L.cugmres_fno_train_step.argtypes = [P, I, I, I, P, P, P, P, F, ctypes.POINTER(F)]
+    L.cugmres_set_preconditioner.argtypes = [P, P, D]
+    L.cugmres_gemm_bf16.argtypes = [I, LL, I, I, P, P, P]
     for name in EXPORTS:
-        if name not in ("cugmres_strerror", "cugmres_default_opts"):
+        if name not in ("cugmres_strerror", "cugmres_default_opts", "cugmres_fno_destroy"):
             getattr(L, name).restype = I
 
 

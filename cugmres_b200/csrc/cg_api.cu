@@ -28,6 +28,7 @@
 
 #include "../../include/cugmres.h"
 #include "cg_common.cuh"
+#include "cg_fno.h"
 #include "cg_internal.h"
 
 using namespace cg;
@@ -44,6 +45,7 @@ struct cg_ctx {
     float2 *gq32 = nullptr;
     double *c64 = nullptr;
     float *c32 = nullptr;
+    float *chi32 = nullptr;  // chi itself (without chi_scale), input of the learned preconditioner
     double2 *tw64 = nullptr;
     float2 *tw32 = nullptr;
     void *T = nullptr;  // N x L complex128 intermediate (also used as complex64)
@@ -67,6 +69,11 @@ struct cg_ctx {
     bool prof = false;
     std::vector<cudaEvent_t> evpool;
     cg_phase_stats stats[CG_NPHASES] = {};
+    // learned preconditioner (flexible GMRES)
+    cg_fno *net = nullptr;
+    double k0h = 0.0;
+    void *Z = nullptr;  // preconditioned basis z_j = M(v_j), restart + 1 vectors
+    size_t zcap_bytes = 0;
 };
 
 namespace {
@@ -142,11 +149,12 @@ __global__ void k_quarter(const double2 *__restrict__ full, double2 *__restrict_
 }
 
 __global__ void k_scale_real(const double *__restrict__ a, double s, double *__restrict__ o64, float *__restrict__ o32,
-                             long long n) {
+                             float *__restrict__ raw32, long long n) {
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
         const double v = a[e] * s;
         o64[e] = v;
         o32[e] = (float)v;
+        raw32[e] = (float)a[e];
     }
 }
 
@@ -171,6 +179,7 @@ void free_operator(cg_ctx *c) {
     dfree_t(c->gq32);
     dfree_t(c->c64);
     dfree_t(c->c32);
+    dfree_t(c->chi32);
     dfree_t(c->tw64);
     dfree_t(c->tw32);
     dfree(c->T);
@@ -199,6 +208,8 @@ void free_krylov(cg_ctx *c) {
     dfree_t(c->kp.tv);
     dfree_t(c->kp.P);
     dfree_t(c->kp.S);
+    dfree(c->Z);
+    c->zcap_bytes = 0;
     c->mcap = 0;
     c->itcap = 0;
     c->vcap_bytes = 0;
@@ -604,6 +615,14 @@ int cugmres_matvec_shapes(const cg_ctx *c, int precision, int *shapes) {
     return CG_OK;
 }
 
+int cugmres_set_preconditioner(cg_ctx *c, cg_fno *net, double k0h) {
+    if (!c || (net && !(k0h > 0.0 && isfinite(k0h)))) return CG_ERR_INVALID;
+    if (net && fno::device_of(net) != c->device) return CG_ERR_INVALID;
+    c->net = net;
+    c->k0h = net ? k0h : 0.0;
+    return CG_OK;
+}
+
 int cugmres_grid_size(const cg_ctx *c, int *N, int *L) {
     if (!c || !c->have_op) return CG_ERR_NO_OPERATOR;
     if (N) *N = c->N;
@@ -622,7 +641,7 @@ static int set_operator_dev(cg_ctx *c, int N, const double2 *g_dev, const double
     if (e == 0) {
         k_quarter<<<grid_for((long long)(L / 2 + 1) * (L / 2 + 1), 8 * c->sms), 256, 0, c->stream>>>(
             full, c->gq64, c->gq32, L, 1.0 / ((double)L * (double)L));
-        k_scale_real<<<grid_for(n, 8 * c->sms), 256, 0, c->stream>>>(chi_dev, chi_scale, c->c64, c->c32, n);
+        k_scale_real<<<grid_for(n, 8 * c->sms), 256, 0, c->stream>>>(chi_dev, chi_scale, c->c64, c->c32, c->chi32, n);
     }
     cudaError_t ce = cudaStreamSynchronize(c->stream);
     cudaFree(full);
@@ -652,6 +671,7 @@ int cugmres_set_operator(cg_ctx *c, int N, const cg_c128 *g_block, const double 
         CG_CU(cudaMalloc((void **)&c->gq32, sizeof(float2) * (size_t)Lq * Lq));
         CG_CU(cudaMalloc((void **)&c->c64, sizeof(double) * n));
         CG_CU(cudaMalloc((void **)&c->c32, sizeof(float) * n));
+        CG_CU(cudaMalloc((void **)&c->chi32, sizeof(float) * n));
         CG_CU(cudaMalloc((void **)&c->tw64, sizeof(double2) * 2 * L));
         CG_CU(cudaMalloc((void **)&c->tw32, sizeof(float2) * 2 * L));
         CG_CU(cudaMalloc(&c->T, sizeof(double2) * (size_t)N * L));
@@ -777,8 +797,12 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     else cugmres_default_opts(&o);
     if (o.restart < 1 || o.max_iter < 0 || !(o.tol >= 0.0) || (o.precision != CG_PREC_FP64 && o.precision != CG_PREC_MIXED) ||
         (o.givens != CG_GIVENS_UNITARY && o.givens != CG_GIVENS_REFERENCE) ||
-        (o.ortho != CG_ORTHO_DCGS2 && o.ortho != CG_ORTHO_CGS2))
+        (o.ortho != CG_ORTHO_DCGS2 && o.ortho != CG_ORTHO_CGS2) ||
+        (o.preconditioner != CG_PRECOND_NONE && o.preconditioner != CG_PRECOND_LEARNED))
         return CG_ERR_INVALID;
+    const bool learned = o.preconditioner == CG_PRECOND_LEARNED;
+    if (learned && !c->net) return CG_ERR_INVALID;
+    if (learned && (c->N < 32 || c->N > 1024)) return CG_ERR_NOT_IMPLEMENTED;
     // per-cycle coefficient arrays live in shared memory (<= 227 KB per block)
     if (o.restart > 4500 || (o.fixed_iterations && o.max_iter > 4500)) return CG_ERR_NOT_IMPLEMENTED;
     CG_CU(cudaSetDevice(c->device));
@@ -786,8 +810,20 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     const int m = o.fixed_iterations ? std::max(1, o.max_iter) : o.restart;
     const long long n = (long long)c->N * c->N;
     const size_t bytes = sizeof(double2) * n;
-    CG_TRY(ensure_krylov(c, m, std::max(1, o.max_iter), prec == 0 ? sizeof(double2) : sizeof(float2)));
+    const size_t esz = prec == 0 ? sizeof(double2) : sizeof(float2);
+    CG_TRY(ensure_krylov(c, m, std::max(1, o.max_iter), esz));
     cudaStream_t s = c->stream;
+    if (learned) {
+        // flexible GMRES keeps z_j = M(v_j) next to the basis
+        const size_t zb = (size_t)(m + 1) * (size_t)n * esz;
+        if (c->zcap_bytes < zb) {
+            dfree(c->Z);
+            c->zcap_bytes = 0;
+            CG_CU(cudaMalloc(&c->Z, zb));
+            c->zcap_bytes = zb;
+        }
+        CG_TRY(fno::prepare(c->net, c->N, (float)c->k0h));
+    }
 
     // inputs
     const bool bd = is_device_ptr(b), xd = is_device_ptr(x);
@@ -814,7 +850,9 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     h.fixed = o.fixed_iterations ? 1 : 0;
     h.tol = o.tol;
     h.inner_tol = prec == 1 ? o.inner_tol : 0.0;
-    h.ortho = o.ortho == CG_ORTHO_CGS2 ? 1 : 0;
+    // the flexible variant stores z_j explicitly, so it uses the CGS2 path (the delayed
+    // reorthogonalisation would need A M(.) to be linear)
+    h.ortho = (o.ortho == CG_ORTHO_CGS2 || learned) ? 1 : 0;
     const bool delayed = h.ortho == 0;
     *c->st_host = h;
     CG_CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(DevState), cudaMemcpyHostToDevice, s));
@@ -830,14 +868,25 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     VecSel vk1 = vk;  // V_{k+1}
     vk1.koff = 1;
     VecSel xs = fixed_vec(xp);
+    VecSel zk = vk;  // Z_k (input of the flexible Arnoldi matvec)
+    zk.base = c->Z;
     const int nrb = row_blocks(c);
     const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(prec, c->sms);
     const int nax2 = axpy2_blocks(prec, c->sms, c->mcap);
     int status = CG_OK;
 
+    bool use_prec = learned;     // this cycle runs the learned preconditioner
+    int prec_cycles = 0, x0_learned = 0;
+    double cycle_start_res = -1.0;  // true residual at the start of the last preconditioned cycle
+    if (learned && o.learned_x0 && o.zero_x0) {
+        // initial guess x0 = M(b) (FP64 application); kept only if it lowers the residual
+        CG_TRY(fno::apply(c->net, s, c->N, 0, bp, c->chi32, (float)c->k0h, xp, nullptr));
+        x0_learned = 1;
+    }
+
     CycleProf cp;
     int it_prev = 0;
-    const double nd = (double)n, esz = prec == 0 ? 16.0 : 8.0;
+    const double nd = (double)n, esz_d = prec == 0 ? 16.0 : 8.0;
     for (;;) {
         if (cp.used == 0) CG_TRY(prof_mark(c, cp, -1, -1, s));
         // true residual r = b - A x (FP64) into V_0, then cycle decisions on device
@@ -851,14 +900,30 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_CU(cudaEventRecord(c->ev, s));
         CG_CU(cudaEventSynchronize(c->ev));
         const DevState hs = *c->st_host;
-        CG_TRY(prof_collect(c, cp, nd, esz, hs.it - it_prev + (delayed ? 1 : 0), delayed));
+        CG_TRY(prof_collect(c, cp, nd, esz_d, hs.it - it_prev + (delayed ? 1 : 0), delayed));
         it_prev = hs.it;
+        if (x0_learned == 1 && hs.cycles == 1 && hs.status == 0 && !(hs.true_res < 1.0)) {
+            // M(b) did not beat x0 = 0: restart from zero (the cycle counter and budget are unchanged
+            // because no Arnoldi step ran)
+            CG_CU(cudaMemsetAsync(xp, 0, bytes, s));
+            x0_learned = 0;
+            DevState h2 = hs;
+            h2.cycles = 0;
+            *c->st_host = h2;
+            CG_CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(DevState), cudaMemcpyHostToDevice, s));
+            continue;
+        }
+        if (use_prec && cycle_start_res >= 0.0 && !(hs.true_res < 0.9 * cycle_start_res)) use_prec = false;
         if (hs.status != 0) break;
         if (o.timeout_s > 0.0 && now_s() - t0 > o.timeout_s) {
             status = CG_ERR_TIMEOUT;
             break;
         }
         CG_TRY(prof_mark(c, cp, -1, -1, s));
+        if (use_prec) {
+            cycle_start_res = hs.true_res;
+            prec_cycles++;
+        }
         const int steps = std::min(m, o.max_iter - hs.it) + (delayed ? 1 : 0);
         for (int i = 0; i < steps; i++) {
             if (delayed) {
@@ -875,9 +940,16 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
                 CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
                 continue;
             }
-            CG_LAUNCH(launch_rows_forward(prec, ap, vk, kp.scale, c->st, GATE_STOP, s));
+            if (use_prec) {
+                // z_i = M(v_i) on the unnormalised stored vector (M is positively homogeneous)
+                CG_TRY(fno::apply(c->net, s, c->N, prec, (const char *)c->V + (size_t)i * n * esz, c->chi32,
+                                  (float)c->k0h, (char *)c->Z + (size_t)i * n * esz, &c->st->stop));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_PRECOND, i, s));
+            }
+            const VecSel &min = use_prec ? zk : vk;
+            CG_LAUNCH(launch_rows_forward(prec, ap, min, kp.scale, c->st, GATE_STOP, s));
             CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, s));
-            CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, kp.scale, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
+            CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, min, kp.scale, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
             CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, s));
             CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h1, 0, ndot, GATE_STOP, s));
             CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
@@ -892,9 +964,10 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         }
         CG_LAUNCH(launch_backsolve(kp, s));
         CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, s));
-        CG_LAUNCH(launch_axpy(prec, 0, c->V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, s));
+        CG_LAUNCH(launch_axpy(prec, 0, use_prec ? c->Z : c->V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, s));
         CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, s));
     }
+    if (learned) CG_TRY(fno::check_error(c->net));
 
     const DevState hs = *c->st_host;
     if (status == CG_OK) {
@@ -919,6 +992,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         result->rel_residual_estimate = hs.est;
         result->rel_residual_true = hs.true_res;
         result->seconds = now_s() - t0;
+        result->preconditioned_cycles = prec_cycles;
+        result->x0_learned = x0_learned;
     }
     return status;
 }

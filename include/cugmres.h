@@ -22,6 +22,8 @@
 #ifndef CUGMRES_H
 #define CUGMRES_H
 
+#include <stdint.h>
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -84,8 +86,19 @@ typedef struct {
                              tol is an absolute threshold on ||b - A x0|| only                 */
     double timeout_s;   /* <= 0: none; otherwise the solve returns CG_ERR_TIMEOUT after this    */
     int ortho;          /* CG_ORTHO_*                                                          */
-    int reserved[7];
+    int preconditioner; /* CG_PRECOND_*; CG_PRECOND_LEARNED needs cugmres_set_preconditioner  */
+    int learned_x0;     /* 1: with a preconditioner attached and zero_x0, start from x0 = M(b)
+                           (kept only if ||b - A x0|| < ||b||, otherwise x0 = 0)             */
+    int reserved[5];
 } cg_opts;
+
+/* right preconditioning */
+enum {
+    CG_PRECOND_NONE = 0,    /* plain GMRES                                                     */
+    CG_PRECOND_LEARNED = 1  /* flexible GMRES with the attached spectral-convolution network;
+                               a cycle that fails to reduce the true residual switches the
+                               rest of the solve to plain GMRES                                */
+};
 
 typedef struct {
     int status;                   /* CG_OK, CG_ERR_NOT_CONVERGED, CG_ERR_BREAKDOWN, ...   */
@@ -94,6 +107,8 @@ typedef struct {
     double rel_residual_estimate; /* last |g_{k+1}| / ||b||                               */
     double rel_residual_true;     /* ||b - A x|| / ||b|| of the returned x (FP64 matvec)  */
     double seconds;               /* wall time of the solve                               */
+    int preconditioned_cycles;    /* cycles run with the learned preconditioner           */
+    int x0_learned;               /* 1: the solve started from x0 = M(b)                  */
 } cg_result;
 
 const char *cugmres_strerror(int status);
@@ -173,7 +188,7 @@ int cugmres_solve_batch(int device, int nsys, const cg_system *systems, const cg
  *   RESIDUAL  FP64 r = b - A x per cycle, 16 n 16 (model of one FP64 matvec)
  * Enabling resets the counters; they accumulate over solves while enabled. */
 enum { CG_PHASE_MATVEC = 0, CG_PHASE_DOTS, CG_PHASE_AXPY, CG_PHASE_SMALL, CG_PHASE_UPDATE, CG_PHASE_RESIDUAL,
-       CG_NPHASES };
+       CG_PHASE_PRECOND, CG_NPHASES };
 typedef struct {
     double ms;          /* summed device time                 */
     double bytes;       /* summed algorithmic bytes           */
@@ -216,6 +231,57 @@ int cugmres_fast_gmres(const cg_c64 *g_prep, const unsigned char *mask, cg_c64 *
 #define CUGMRES_NOALLOC_MAX_N 256
 int cugmres_matvec_noalloc(int N, const cg_c128 *g_block, const double *chi, double chi_scale, const cg_c128 *x,
                            cg_c128 *y, void *stream);
+
+/* ---------------------------------------------------------------------------
+ * Learned preconditioner: a spectral-convolution network (Fourier neural
+ * operator: lift 4 -> 32 channels, 4 Fourier layers of 32 channels keeping
+ * 2*16 x 16 modes, projection 32 -> 128 -> 2) that maps (chi, k0 h, r) to an
+ * estimate of A^{-1} r.  M(r) = r + s * net(0.1 chi, k0 h, r / s), s = rms(r).
+ * BF16 activations and tensor-core weights (FP32 accumulation), FP32 master
+ * parameters and Adam.  No counterpart in the reference.
+ *
+ * Arrays are [batch, H, W] row-major; chi FP32, r / x / z complex64, k0h FP32
+ * [batch]; host or device pointers.  H >= 32, 32 <= W <= 1024.  A network is
+ * used by one host thread at a time; it must not be trained while a context
+ * it is attached to is solving.
+ * ------------------------------------------------------------------------- */
+typedef struct cg_fno cg_fno;
+
+typedef struct {
+    int layers, width, modes1, modes2, hidden, in_features;
+    long long num_params; /* length of the flat FP32 parameter vector            */
+    long long steps;      /* optimiser steps taken since the parameters were set */
+} cg_fno_info;
+
+int cugmres_fno_create(cg_fno **net, int device, unsigned long long seed);
+void cugmres_fno_destroy(cg_fno *net);
+int cugmres_fno_info(const cg_fno *net, cg_fno_info *info);
+/* Flat FP32 parameters, in order: P [32 x 4], p [32]; per layer l = 0..3:
+ * R_l [32 k1][16 k2][32 in][32 out] complex (re, im), W_l [32 out x 32 in],
+ * b_l [32]; Q1 [128 x 32], bq1 [128], Q2 [2 x 128], bq2 [2].  set_params
+ * also resets the optimiser state. */
+int cugmres_fno_get_params(cg_fno *net, float *params);
+int cugmres_fno_set_params(cg_fno *net, const float *params);
+/* z = M(r) for a batch. */
+int cugmres_fno_forward(cg_fno *net, int batch, int H, int W, const float *chi, const float *k0h, const cg_c64 *r,
+                        cg_c64 *z);
+/* Loss L = (1/batch) sum_b ||net_b - t_b||^2 / ||t_b||^2 with t = (x - r) / s
+ * (x: the solution of A x = r) and its gradient (flat, like the parameters;
+ * grad may be NULL). */
+int cugmres_fno_loss_grad(cg_fno *net, int batch, int H, int W, const float *chi, const float *k0h,
+                          const cg_c64 *r, const cg_c64 *x, float *loss, float *grad);
+/* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss above. */
+int cugmres_fno_train_step(cg_fno *net, int batch, int H, int W, const float *chi, const float *k0h,
+                           const cg_c64 *r, const cg_c64 *x, float lr, float *loss);
+/* Attach (net != NULL) or detach the network to a context's solves;
+ * k0h = k0 * h of the operator set with cugmres_set_operator, whose chi /
+ * chi_scale give the contrast.  N of the operator must satisfy 32 <= N <= 1024. */
+int cugmres_set_preconditioner(cg_ctx *ctx, cg_fno *net, double k0h);
+
+/* C = A B^T on the tcgen05 tensor cores: A [M x K], B [N x K] BF16 row-major
+ * (raw bits), C [M x N] FP32; N, K in {32, 128}; host pointers.  The
+ * self-test of the kernel the network's channel mixing runs on. */
+int cugmres_gemm_bf16(int device, long long M, int N, int K, const uint16_t *A, const uint16_t *B, float *C);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,178 @@
+"""Learned preconditioner on the GPU: the tcgen05 GEMM, the network's
+forward pass and gradients against the CPU oracle, training, and flexible
+GMRES with the trained network (gain over plain GMRES, fallback)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from cugmres_b200 import _lib, learned, problems
+from oracle import fno_oracle as FO
+
+pytestmark = pytest.mark.gpu
+
+
+def _bf16_bits(a):
+    """float32 -> (BF16 bits as uint16, the rounded float32 values), round to nearest even."""
+    u = np.ascontiguousarray(a, np.float32).view(np.uint32).astype(np.uint64)
+    r = ((u + 0x7FFF + ((u >> 16) & 1)) >> 16).astype(np.uint16)
+    return r, (r.astype(np.uint32) << 16).view(np.float32)
+
+
+@pytest.mark.parametrize("M,N,K", [(1000, 32, 32), (128 * 300, 32, 32), (777, 128, 32), (4096, 32, 128),
+                                   (513, 128, 128)])
+def test_tcgen05_gemm(cuda_device, M, N, K):
+    rng = np.random.default_rng(M + N + K)
+    a16, a = _bf16_bits(rng.standard_normal((M, K)).astype(np.float32))
+    b16, b = _bf16_bits(rng.standard_normal((N, K)).astype(np.float32))
+    c = np.empty((M, N), np.float32)
+    st = _lib.lib().cugmres_gemm_bf16(0, M, N, K, a16.ctypes.data_as(ctypes.c_void_p),
+                                      b16.ctypes.data_as(ctypes.c_void_p), c.ctypes.data_as(ctypes.c_void_p))
+    assert st == 0, _lib.strerror(st)
+    ref = a.astype(np.float64) @ b.astype(np.float64).T
+    # BF16 x BF16 products are exact in FP32; only the FP32 accumulation order differs
+    assert np.max(np.abs(c - ref)) <= 1e-5 * np.max(np.abs(ref)) + 1e-6
+
+
+def _params(seed):
+    """Random parameters with activations of order one (R larger than the default init)."""
+    net_p = np.random.default_rng(seed)
+    p = net_p.uniform(-1, 1, FO.NPARAM).astype(np.float32)
+    p[FO.OFF_P:FO.OFF_L0] *= 0.5
+    for l in range(FO.LAYERS):
+        o = FO.off_r(l)
+        p[o:o + FO.RSZ] *= 4.0 / (FO.C * FO.C)
+        p[o + FO.RSZ:o + FO.LSZ] *= 1.0 / np.sqrt(FO.C)
+    p[FO.OFF_Q1:FO.OFF_Q2] *= 1.0 / np.sqrt(FO.C)
+    p[FO.OFF_Q2:] *= 1.0 / np.sqrt(FO.HID)
+    return p
+
+
+def _inputs(B, H, W, seed):
+    rng = np.random.default_rng(seed)
+    chi = ((rng.random((B, H, W)) > 0.5) * rng.uniform(1, 11, (B, 1, 1))).astype(np.float32)
+    k0h = rng.uniform(0.2, 0.42, B).astype(np.float32)
+    r = (rng.standard_normal((B, H, W)) + 1j * rng.standard_normal((B, H, W))).astype(np.complex64)
+    x = (r + 0.5 * (rng.standard_normal((B, H, W)) + 1j * rng.standard_normal((B, H, W)))).astype(np.complex64)
+    return chi, k0h, r, x
+
+
+@pytest.fixture(scope="module")
+def net(cuda_device):
+    n = learned.FNO(0, seed=0)
+    yield n
+    n.close()
+
+
+def test_fno_params_roundtrip(net):
+    info = net.info()
+    assert (info["layers"], info["width"], info["modes1"], info["modes2"], info["hidden"]) == (4, 32, 16, 16, 128)
+    assert info["num_params"] == FO.NPARAM
+    p = _params(3)
+    net.set_params(p)
+    assert np.array_equal(net.get_params(), p)
+
+
+@pytest.mark.parametrize("B,H,W", [(2, 32, 48), (1, 64, 64), (3, 40, 96)])
+def test_fno_forward_matches_oracle(net, B, H, W):
+    p = _params(1)
+    net.set_params(p)
+    chi, k0h, r, _ = _inputs(B, H, W, 7)
+    z = net.forward(chi, k0h, r)
+    ref = FO.forward(p, chi, k0h, r, bf16=True)
+    s = ref["s"].numpy().reshape(-1, 1, 1)
+    corr = (z - r) / s
+    corr_ref = (ref["z"].numpy() - r) / s
+    err = np.linalg.norm(corr - corr_ref) / np.linalg.norm(corr_ref)
+    # BF16 storage of activations: isolated one-ulp differences propagate through 5 layers
+    assert err < 2e-2, err
+
+
+def test_fno_gradients_match_oracle(net):
+    p = _params(2)
+    net.set_params(p)
+    chi, k0h, r, x = _inputs(2, 32, 40, 11)
+    loss, g = net.loss_grad(chi, k0h, r, x)
+    loss_ref, g_ref = FO.loss_grad(p, chi, k0h, r, x, bf16=True)
+    assert abs(loss - loss_ref) <= 5e-3 * abs(loss_ref), (loss, loss_ref)
+    blocks = {"P": (FO.OFF_P, FO.OFF_L0), "Q1": (FO.OFF_Q1, FO.OFF_Q2), "Q2": (FO.OFF_Q2, FO.NPARAM)}
+    for l in range(FO.LAYERS):
+        o = FO.off_r(l)
+        blocks[f"R{l}"] = (o, o + FO.RSZ)
+        blocks[f"W{l}"] = (o + FO.RSZ, o + FO.LSZ)
+    for name, (a, b) in blocks.items():
+        e = np.linalg.norm(g[a:b] - g_ref[a:b]) / np.linalg.norm(g_ref[a:b])
+        # the oracle mirrors every BF16 rounding of the GPU; the rest is FP32 summation order
+        assert e < 5e-2, (name, e)
+
+
+def test_fno_zero_input_gives_zero(net):
+    net.set_params(_params(4))
+    chi, k0h, r, _ = _inputs(1, 32, 32, 5)
+    z = net.forward(chi, k0h, np.zeros_like(r))
+    assert np.all(z == 0)
+
+
+@pytest.fixture(scope="module")
+def trained(cuda_device):
+    """A network trained on solver-generated pairs at 48 x 48 (small, for the test's time budget)."""
+    data = learned.generate_pairs(48, designs=48, seed=1000, eps_range=(2.0, 6.0), random_per_design=3,
+                                  solve_tol=1e-7)
+    n = learned.FNO(0, seed=1)
+    l0 = learned.evaluate_loss(n, data)
+    hist = learned.train(n, data, steps=600, batch=16, lr=2e-3)
+    l1 = learned.evaluate_loss(n, data)
+    yield n, data, l0, l1, hist
+    n.close()
+
+
+def test_fno_training_reduces_loss(trained):
+    _, data, l0, l1, hist = trained
+    assert data["unconverged"] == 0
+    assert l1 < 0.5 * l0, (l0, l1)
+
+
+def test_fgmres_learned_gain_and_parity(trained, solver):
+    n = trained[0]
+    gains = []
+    for seed in (20001, 20002, 20003):
+        pr = problems.helmholtz(48, 4.0, seed=seed, cells_per_wavelength=20.0)
+        solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+        solver.set_preconditioner(n, pr["k0"] * pr["h"])
+        x0, i0 = solver.solve(pr["b"], restart=200, max_iter=2000, tol=1e-10)
+        x1, i1 = solver.solve(pr["b"], restart=200, max_iter=2000, tol=1e-10, preconditioner="learned")
+        solver.set_preconditioner(None)
+        assert i0["status"] == 0 and i1["status"] == 0
+        assert i1["rel_residual_true"] <= 1e-10
+        assert i1["preconditioned_cycles"] >= 1
+        # both solve the same system: solutions agree to the tolerance's conditioning
+        assert np.linalg.norm(x1 - x0) / np.linalg.norm(x0) < 1e-7
+        gains.append(i0["iterations"] / max(1, i1["iterations"]))
+    assert np.median(gains) > 1.0, gains
+
+
+def test_fgmres_fallback_with_bad_network(solver, cuda_device):
+    bad = learned.FNO(0, seed=2)
+    p = bad.get_params()
+    p[FO.OFF_Q2:] *= 1e4  # a network whose corrections are huge and useless
+    bad.set_params(p)
+    pr = problems.helmholtz(48, 4.0, seed=20004)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    solver.set_preconditioner(bad, pr["k0"] * pr["h"])
+    x, info = solver.solve(pr["b"], restart=60, max_iter=3000, tol=1e-10, preconditioner="learned",
+                           learned_x0=True)
+    solver.set_preconditioner(None)
+    bad.close()
+    assert info["status"] == 0 and info["rel_residual_true"] <= 1e-10
+    assert info["x0_learned"] == 0  # M(b) did not lower the residual and was discarded
+
+
+def test_fgmres_mixed_precision_learned(trained, solver):
+    n = trained[0]
+    pr = problems.helmholtz(48, 4.0, seed=20005)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    solver.set_preconditioner(n, pr["k0"] * pr["h"])
+    x, info = solver.solve(pr["b"], restart=100, max_iter=3000, tol=1e-10, precision="mixed",
+                           preconditioner="learned", learned_x0=True)
+    solver.set_preconditioner(None)
+    assert info["status"] == 0 and info["rel_residual_true"] <= 1e-10
