@@ -133,15 +133,17 @@ class Solver:
         self._grid()
         return self
 
-    def matvec(self, x, precision="fp64", out=None):
-        """y = A x; precision 'fp64' (complex128) or 'fp32' (complex64)."""
+    def matvec(self, x, precision="fp64", out=None, transpose=False):
+        """y = A x (transpose: y = A^T x = x - diag(c) G x); precision 'fp64'
+        (complex128) or 'fp32' (complex64)."""
         prec = _PREC[precision]
         dt = np.complex128 if prec == _lib.CG_PREC_FP64 else np.complex64
         xp, xk = _arg(x, dt)
         if out is None:
             out = np.empty((self.N, self.N), dt) if not _is_torch(x) else x.new_empty(x.shape)
         yp, yk = _arg(out, dt)
-        check(_lib.lib().cugmres_matvec(self._ctx, xp, yp, prec), "matvec")
+        fn = _lib.lib().cugmres_matvec_transpose if transpose else _lib.lib().cugmres_matvec
+        check(fn(self._ctx, xp, yp, prec), "matvec")
         return yk
 
     def residual(self, b, x):
@@ -166,11 +168,12 @@ class Solver:
 
     def solve(self, b, x0=None, restart=100, max_iter=10000, tol=1e-10, precision="fp64", givens="unitary",
               inner_tol=1e-5, fixed_iterations=False, timeout_s=0.0, ortho="dcgs2", raise_on_failure=False,
-              preconditioner=None, learned_x0=False):
+              preconditioner=None, learned_x0=False, transpose=False):
         """Solve A x = b.  Returns (x, info) where info holds status, iterations,
         cycles, rel_residual_true / _estimate, seconds and res_hist.
         preconditioner="learned": flexible GMRES with the attached network
-        (learned_x0: also start from x0 = M(b) when x0 is None)."""
+        (learned_x0: also start from x0 = M(b) when x0 is None).
+        transpose=True solves A^T x = b (the adjoint system of the gradient path)."""
         o = _lib.CgOpts()
         _lib.lib().cugmres_default_opts(ctypes.byref(o))
         o.restart = int(restart)
@@ -184,6 +187,7 @@ class Solver:
         o.ortho = _ORTHO[ortho]
         o.preconditioner = {None: 0, "none": 0, "learned": 1}[preconditioner]
         o.learned_x0 = int(bool(learned_x0))
+        o.transpose = int(bool(transpose))
         bp, bk = _arg(b, np.complex128)
         if x0 is None:
             o.zero_x0 = 1
@@ -277,8 +281,9 @@ def matvec(x, eps, k, qweq=False, transpose=False, g=None, device=0):
     """x - G (k^2 eps x) on the GPU, the reference's matvec(x, eps, k)
     (PyGMRES/GMRES.py:47-57).  x: N^2 vector, eps: N^2 real column, k: wavenumber,
     g: optional (2N-1)^2 circulant (as get_toeplitz_mat returns).  Returns an
-    (N^2, 1) complex128 column.  ``qweq`` returns (G_block, G) as the reference.
-    ``transpose`` (x - chi G x) is not provided by this build."""
+    (N^2, 1) complex128 column.  ``qweq`` returns (G_block, G) as the reference;
+    ``transpose`` gives x - chi G x (k^2 eps = chi), the reference's transposed
+    operator."""
     x = np.asarray(x).reshape(-1)
     n = x.size
     N = int(round(np.sqrt(n)))
@@ -290,8 +295,6 @@ def matvec(x, eps, k, qweq=False, transpose=False, g=None, device=0):
         block = np.asarray(g)[:N, :N]
     if qweq:
         return block, (get_toeplitz_mat(block) if g is None else g)
-    if transpose:
-        raise NotImplementedError("transpose=True (x - chi G x) is not part of this build")
     chi = np.asarray(eps, dtype=np.float64).reshape(N, N)
     key = (device, N)
     s = _mv_cache.get(key)
@@ -299,7 +302,7 @@ def matvec(x, eps, k, qweq=False, transpose=False, g=None, device=0):
         s = Solver(device)
         _mv_cache[key] = s
     s.set_operator(block, chi, float(k) ** 2)
-    return s.matvec(x.reshape(N, N).astype(np.complex128)).reshape(-1, 1)
+    return s.matvec(x.reshape(N, N).astype(np.complex128), transpose=transpose).reshape(-1, 1)
 
 
 def fast_gmres(g_prep, mask, solution, maxiter, tolerance, chi_value, rhs=None, precision="fp64"):

@@ -40,6 +40,7 @@ EXPORTS = (
     "cugmres_matvec_shapes", "cugmres_solve_batch", "cugmres_fno_create", "cugmres_fno_destroy",
     "cugmres_fno_info", "cugmres_fno_get_params", "cugmres_fno_set_params", "cugmres_fno_forward",
     "cugmres_fno_loss_grad", "cugmres_fno_train_step", "cugmres_set_preconditioner", "cugmres_gemm_bf16",
+    "cugmres_matvec_transpose", "cugmres_fno_forward_train", "cugmres_fno_backward",
 )
 
 PHASES = ("matvec", "dots", "axpy", "small", "update", "residual", "precond")
@@ -59,7 +60,8 @@ class CgOpts(ctypes.Structure):
         ("ortho", ctypes.c_int),
         ("preconditioner", ctypes.c_int),
         ("learned_x0", ctypes.c_int),
-        ("reserved", ctypes.c_int * 5),
+        ("transpose", ctypes.c_int),
+        ("reserved", ctypes.c_int * 4),
     ]
 
 
@@ -142,6 +144,7 @@ def _declare(L):
     L.cugmres_set_operator_circulant.argtypes = [P, I, P, P, D]
     L.cugmres_grid_size.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(I)]
     L.cugmres_matvec.argtypes = [P, P, P, I]
+    L.cugmres_matvec_transpose.argtypes = [P, P, P, I]
     L.cugmres_residual.argtypes = [P, P, P, P, ctypes.POINTER(D)]
     L.cugmres_solve.argtypes = [P, P, P, ctypes.POINTER(CgOpts), P, I, ctypes.POINTER(CgResult)]
     L.cugmres_fast_gmres.argtypes = [P, P, P, P, ctypes.POINTER(U), F, ctypes.POINTER(I), U, U, F, P, I]
@@ -162,6 +165,8 @@ def _declare(L):
     L.cugmres_fno_loss_grad.argtypes = [P, I, I, I, P, P, P, P, ctypes.POINTER(F), P]
     L.cugmres_fno_train_step.argtypes = [P, I, I, I, P, P, P, P, F, ctypes.POINTER(F)]
     L.cugmres_set_preconditioner.argtypes = [P, P, D]
+    L.cugmres_fno_forward_train.argtypes = [P, I, I, I, P, P, P, P]
+    L.cugmres_fno_backward.argtypes = [P, P, P, F]
     L.cugmres_gemm_bf16.argtypes = [I, LL, I, I, P, P, P]
     for name in EXPORTS:
         if name not in ("cugmres_strerror", "cugmres_default_opts", "cugmres_fno_destroy"):

@@ -260,8 +260,9 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
     return CG_OK;
 }
 
-MatvecArgs margs(const cg_ctx *c, int prec) {
+MatvecArgs margs(const cg_ctx *c, int prec, int transpose = 0) {
     MatvecArgs a;
+    a.transpose = transpose;
     a.N = c->N;
     a.L = c->L;
     a.vfwd = c->var[prec][0];
@@ -413,8 +414,9 @@ int autotune(cg_ctx *c, int prec) {
 }
 
 // y = A x (mode 0) or y = b - A x (mode 1) on explicit vectors, no gating.
-int apply_explicit(cg_ctx *c, int prec, int mode, int out_prec, const void *x, const void *b, void *y, double *npart) {
-    MatvecArgs a = margs(c, prec);
+int apply_explicit(cg_ctx *c, int prec, int mode, int out_prec, const void *x, const void *b, void *y, double *npart,
+                   int transpose = 0) {
+    MatvecArgs a = margs(c, prec, transpose);
     CG_LAUNCH(launch_rows_forward(prec, a, fixed_vec(x), nullptr, nullptr, GATE_NONE, c->stream));
     CG_LAUNCH(launch_cols_convolve(prec, a, nullptr, GATE_NONE, c->stream));
     CG_LAUNCH(launch_rows_inverse(prec, mode, out_prec, a, fixed_vec(x), nullptr, b, fixed_vec(y), npart, nullptr,
@@ -734,7 +736,7 @@ int cugmres_set_operator_circulant(cg_ctx *c, int N, const cg_c64 *g_prep, const
     return cugmres_set_operator(c, N, g.data(), chi, chi_scale);
 }
 
-int cugmres_matvec(cg_ctx *c, const void *x, void *y, int precision) {
+static int matvec_impl(cg_ctx *c, const void *x, void *y, int precision, int transpose) {
     if (!c || !x || !y) return CG_ERR_INVALID;
     if (!c->have_op) return CG_ERR_NO_OPERATOR;
     if (precision != CG_PREC_FP64 && precision != CG_PREC_MIXED) return CG_ERR_INVALID;
@@ -750,9 +752,15 @@ int cugmres_matvec(cg_ctx *c, const void *x, void *y, int precision) {
         xp = c->xbuf;
     }
     if (!yd) yp = c->rbuf;
-    CG_TRY(apply_explicit(c, prec, 0, prec, xp, nullptr, yp, nullptr));
+    CG_TRY(apply_explicit(c, prec, 0, prec, xp, nullptr, yp, nullptr, transpose));
     if (!yd) CG_CU(cudaMemcpyAsync(y, yp, bytes, cudaMemcpyDeviceToHost, c->stream));
     return cuerr(cudaStreamSynchronize(c->stream));
+}
+
+int cugmres_matvec(cg_ctx *c, const void *x, void *y, int precision) { return matvec_impl(c, x, y, precision, 0); }
+
+int cugmres_matvec_transpose(cg_ctx *c, const void *x, void *y, int precision) {
+    return matvec_impl(c, x, y, precision, 1);
 }
 
 int cugmres_residual(cg_ctx *c, const cg_c128 *b, const cg_c128 *x, cg_c128 *r, double *rel) {
@@ -802,6 +810,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         return CG_ERR_INVALID;
     const bool learned = o.preconditioner == CG_PRECOND_LEARNED;
     if (learned && !c->net) return CG_ERR_INVALID;
+    if (learned && o.transpose) return CG_ERR_NOT_IMPLEMENTED;  // the network approximates A^-1, not A^-T
     if (learned && (c->N < 32 || c->N > 1024)) return CG_ERR_NOT_IMPLEMENTED;
     // per-cycle coefficient arrays live in shared memory (<= 227 KB per block)
     if (o.restart > 4500 || (o.fixed_iterations && o.max_iter > 4500)) return CG_ERR_NOT_IMPLEMENTED;
@@ -859,8 +868,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     CG_LAUNCH(launch_norm2(0, bp, n, c->kp.npart, &c->st->counter[2], &c->st->nb, axpy_blocks(c, n), s));
 
     KrylovPtrs kp = c->kp;
-    MatvecArgs a64 = margs(c, 0);
-    MatvecArgs ap = margs(c, prec);
+    MatvecArgs a64 = margs(c, 0, o.transpose ? 1 : 0);
+    MatvecArgs ap = margs(c, prec, o.transpose ? 1 : 0);
     VecSel vk;  // V_k (input of the Arnoldi matvec)
     vk.base = c->V;
     vk.stride = n;

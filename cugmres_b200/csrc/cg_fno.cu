@@ -579,6 +579,17 @@ k_loss(float *__restrict__ o, const cg_c64 *__restrict__ x, const cg_c64 *__rest
     }
 }
 
+// dL/do from a caller's dL/dM (M = r + s (o0 + i o1), gradients as d/dRe + i d/dIm).
+__global__ void k_dout_from_dm(float *__restrict__ o, const cg_c64 *__restrict__ dm, const float *__restrict__ s,
+                               long long hw, long long cells) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cells;
+         e += (long long)gridDim.x * blockDim.x) {
+        const float sc = s[e / hw];
+        o[2 * e] = sc * dm[e].re;
+        o[2 * e + 1] = sc * dm[e].im;
+    }
+}
+
 // Projection backward on the CUDA cores: thread j = hidden unit over a chunk
 // of cells: dzq = (Q2^T do) GELU'(zq); partials of dQ2 = sum do GELU(zq)^T and
 // dbq2 = sum do.  Partial layout per block: [Q2 (2 x HID), bq2 (2)].
@@ -811,6 +822,7 @@ struct cg_fno {
     int tw_H = 0, tw_W = 0;
     float2 *twh = nullptr, *tww = nullptr;
     float apply_k0h = -1.f;  // k0 h held in k0h[0] for single-vector applications
+    int fwd_B = 0, fwd_H = 0, fwd_W = 0;  // batch kept by cugmres_fno_forward_train
     std::mutex mu;
 };
 
@@ -1024,13 +1036,19 @@ int forward(cg_fno *f, cudaStream_t s, int B, int H, int W, const RT *r, const f
 }
 
 // Backward pass (after forward(train = true) with targets x): gradients into f->g, loss into f->dloss.
-int backward(cg_fno *f, cudaStream_t s, int B, int H, int W, const cg_c64 *r, const cg_c64 *x, const float *chi) {
+// With x: the loss of cugmres_fno_loss_grad; with dm (x null): dL/dM given by the caller.
+int backward(cg_fno *f, cudaStream_t s, int B, int H, int W, const cg_c64 *r, const cg_c64 *x, const float *chi,
+             const cg_c64 *dm) {
     const long long hw = (long long)H * W, cells = B * hw, lines = (long long)B * H;
     const int HC = (H + HCH - 1) / HCH;
     const int nred = reduction_blocks(f, cells);
-    double *lpart = reinterpret_cast<double *>(f->part);
-    k_loss<<<nred, RED_THREADS, 0, s>>>(f->out2, x, r, f->inv_s, f->wts, hw, cells, lpart);
-    k_reduce_d<<<1, 32, 0, s>>>(lpart, nred, f->dloss);
+    if (x) {
+        double *lpart = reinterpret_cast<double *>(f->part);
+        k_loss<<<nred, RED_THREADS, 0, s>>>(f->out2, x, r, f->inv_s, f->wts, hw, cells, lpart);
+        k_reduce_d<<<1, 32, 0, s>>>(lpart, nred, f->dloss);
+    } else {
+        k_dout_from_dm<<<nred, RED_THREADS, 0, s>>>(f->out2, dm, f->s, hw, cells);
+    }
     FN_K(cudaGetLastError());
     // projection
     k_proj_bwd<<<nred, HID, 0, s>>>(f->zq, f->out2, f->p, cells, f->dzq, f->part);
@@ -1108,6 +1126,7 @@ int stage(cg_fno *f, void *dst, const void *src, size_t bytes) {
 int stage_inputs(cg_fno *f, int B, int H, int W, const float *chi, const float *k0h, const cg_c64 *r,
                  const cg_c64 *x) {
     const size_t cells = (size_t)B * H * W;
+    f->fwd_B = 0;
     FN_TRY(stage(f, f->chi_in, chi, cells * 4));
     FN_TRY(stage(f, f->k0h, k0h, (size_t)B * 4));
     f->apply_k0h = -1.f;
@@ -1135,6 +1154,7 @@ int apply(cg_fno *net, cudaStream_t s, int N, int prec, const void *r, const flo
     if (!net || !r || !z || !chi) return CG_ERR_INVALID;
     if (net->cap_cells < (long long)N * N || net->tw_H != N || net->tw_W != N || net->apply_k0h != k0h)
         return CG_ERR_INVALID;  // prepare(net, N, k0h) first
+    net->fwd_B = 0;
     FN_TRY(ensure_maps(net, (long long)N * N));
     if (prec == 0)
         return forward<double2>(net, s, 1, N, N, (const double2 *)r, chi, (double2 *)z, false, nullptr, gate);
@@ -1247,6 +1267,7 @@ extern "C" int cugmres_fno_set_params(cg_fno *f, const float *params) {
     FN_CU(cudaMemset(f->v, 0, sizeof(float) * NPARAM));
     FN_CU(cudaMemset(f->err, 0, sizeof(int)));
     f->step = 0;
+    f->fwd_B = 0;
     FN_TRY(pack_weights(f, f->stream));
     for (int l = 0; l < LAYERS; l++) {
         if (make_map(&f->mapW[l], f->wb + l * C * C, C, C, C)) return CG_ERR_CUDA;
@@ -1280,7 +1301,7 @@ static int loss_grad_impl(cg_fno *f, int B, int H, int W, const float *chi, cons
     FN_TRY(stage_inputs(f, B, H, W, chi, k0h, r, x));
     FN_TRY(forward<float2>(f, f->stream, B, H, W, (const float2 *)f->r_in, f->chi_in, nullptr, true, f->x_in,
                            nullptr));
-    FN_TRY(backward(f, f->stream, B, H, W, f->r_in, f->x_in, f->chi_in));
+    FN_TRY(backward(f, f->stream, B, H, W, f->r_in, f->x_in, f->chi_in, nullptr));
     if (loss) {
         double l = 0.0;
         FN_CU(cudaMemcpyAsync(&l, f->dloss, sizeof(double), cudaMemcpyDeviceToHost, f->stream));
@@ -1301,19 +1322,56 @@ extern "C" int cugmres_fno_loss_grad(cg_fno *f, int B, int H, int W, const float
     return read_err(f);
 }
 
-extern "C" int cugmres_fno_train_step(cg_fno *f, int B, int H, int W, const float *chi, const float *k0h,
-                                      const cg_c64 *r, const cg_c64 *x, float lr, float *loss) {
-    if (!f || B < 1 || !chi || !k0h || !r || !x || !(lr >= 0.f)) return CG_ERR_INVALID;
-    std::lock_guard<std::mutex> lk(f->mu);
-    FN_CU(cudaSetDevice(f->device));
-    FN_TRY(loss_grad_impl(f, B, H, W, chi, k0h, r, x, loss));
+static int adam_step(cg_fno *f, float lr) {
     f->step++;
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = (float)(1.0 / (1.0 - pow((double)b1, (double)f->step)));
     const float c2 = (float)(1.0 / (1.0 - pow((double)b2, (double)f->step)));
     k_adam<<<4 * f->sms, 256, 0, f->stream>>>(f->p, f->g, f->m, f->v, NPARAM, lr, b1, b2, 1e-8f, c1, c2);
     FN_K(cudaGetLastError());
-    FN_TRY(pack_weights(f, f->stream));
+    return pack_weights(f, f->stream);
+}
+
+extern "C" int cugmres_fno_train_step(cg_fno *f, int B, int H, int W, const float *chi, const float *k0h,
+                                      const cg_c64 *r, const cg_c64 *x, float lr, float *loss) {
+    if (!f || B < 1 || !chi || !k0h || !r || !x || !(lr >= 0.f)) return CG_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(f->mu);
+    FN_CU(cudaSetDevice(f->device));
+    FN_TRY(loss_grad_impl(f, B, H, W, chi, k0h, r, x, loss));
+    FN_TRY(adam_step(f, lr));
+    FN_CU(cudaStreamSynchronize(f->stream));
+    return read_err(f);
+}
+
+extern "C" int cugmres_fno_forward_train(cg_fno *f, int B, int H, int W, const float *chi, const float *k0h,
+                                         const cg_c64 *r, cg_c64 *z) {
+    if (!f || B < 1 || !chi || !k0h || !r || !z) return CG_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(f->mu);
+    FN_CU(cudaSetDevice(f->device));
+    FN_TRY(prepare_grid(f, B, H, W));
+    FN_TRY(stage_inputs(f, B, H, W, chi, k0h, r, nullptr));
+    FN_TRY(forward<float2>(f, f->stream, B, H, W, (const float2 *)f->r_in, f->chi_in, (float2 *)f->z_out, true,
+                           nullptr, nullptr));
+    const size_t cells = (size_t)B * H * W;
+    const cudaMemcpyKind k = dev_ptr(z) ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    FN_CU(cudaMemcpyAsync(z, f->z_out, cells * 8, k, f->stream));
+    FN_CU(cudaStreamSynchronize(f->stream));
+    f->fwd_B = B, f->fwd_H = H, f->fwd_W = W;
+    return read_err(f);
+}
+
+extern "C" int cugmres_fno_backward(cg_fno *f, const cg_c64 *dm, float *grad, float lr) {
+    if (!f || !dm || !(lr >= 0.f)) return CG_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(f->mu);
+    if (f->fwd_B < 1) return CG_ERR_INVALID;  // needs cugmres_fno_forward_train first
+    FN_CU(cudaSetDevice(f->device));
+    const int B = f->fwd_B, H = f->fwd_H, W = f->fwd_W;
+    const size_t cells = (size_t)B * H * W;
+    FN_TRY(stage(f, f->x_in, dm, cells * 8));  // x_in is free in this mode
+    FN_TRY(backward(f, f->stream, B, H, W, f->r_in, nullptr, f->chi_in, f->x_in));
+    f->fwd_B = 0;
+    if (grad) FN_CU(cudaMemcpyAsync(grad, f->g, sizeof(float) * NPARAM, cudaMemcpyDeviceToHost, f->stream));
+    if (lr > 0.f) FN_TRY(adam_step(f, lr));
     FN_CU(cudaStreamSynchronize(f->stream));
     return read_err(f);
 }

@@ -69,6 +69,7 @@ struct MatvecArgs {
     const void *cdiag;  // N x N real diagonal k0^2 chi (R)
     const void *tw;     // L twiddles (C)
     void *T;            // N x L intermediate (C)
+    int transpose = 0;  // 1: A^T x = x - diag(c) G x (contrast applied after the convolution)
 };
 
 // Reference to a basis vector selected by the device-side Arnoldi index:

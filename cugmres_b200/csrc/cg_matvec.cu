@@ -95,7 +95,7 @@ k_rows_forward(VecSel xs, const double *__restrict__ xscale, const typename real
         reg[p] = czero<C>();
         if (p < E / 2 && live && idx < N) {
             const C v = x[rb + idx];
-            const R c = cdiag[rb + idx] * s;
+            const R c = cdiag ? cdiag[rb + idx] * s : s;  // cdiag == null: transpose operator
             reg[p] = cscale(v, c);
         }
     }
@@ -152,7 +152,8 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
 template <typename C, typename CO, int L, int MODE, typename SH>
 __global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
 k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xscale, const C *__restrict__ bvec,
-               VecSel ys, double *__restrict__ npart, const C *__restrict__ tw, int N, const DevState *st, int gate) {
+               VecSel ys, double *__restrict__ npart, const C *__restrict__ tw, int N, const DevState *st, int gate,
+               const typename real_of<C>::type *__restrict__ cout) {
     typedef typename real_of<C>::type R;
     typedef typename real_of<CO>::type RO;
     typedef Plan<L, SH::E> P;
@@ -188,6 +189,7 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
             const int idx = t + p * TPR;
             if (idx < N) {
                 const C xv = x[rb + idx];
+                if (cout) reg[p] = cscale(reg[p], cout[rb + idx]);  // transpose: contrast after G
                 C o;
                 if (MODE == 0) {
                     o = csub(cscale(xv, s), reg[p]);
@@ -273,15 +275,15 @@ template <typename SH, int L> struct Passes {
             auto kern = k_rows_forward<double2, L, SH>;
             int e = set_smem(kern, smem);
             if (e) return e;
-            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, (const double *)a.cdiag, (double2 *)a.T,
-                                                (const double2 *)a.tw, a.N, st, gate);
+            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, a.transpose ? nullptr : (const double *)a.cdiag,
+                                                (double2 *)a.T, (const double2 *)a.tw, a.N, st, gate);
         } else {
             const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(float2);
             auto kern = k_rows_forward<float2, L, SH>;
             int e = set_smem(kern, smem);
             if (e) return e;
-            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, (const float *)a.cdiag, (float2 *)a.T, (const float2 *)a.tw,
-                                                a.N, st, gate);
+            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, a.transpose ? nullptr : (const float *)a.cdiag,
+                                                (float2 *)a.T, (const float2 *)a.tw, a.N, st, gate);
         }
         return (int)cudaGetLastError();
     }
@@ -308,8 +310,9 @@ template <typename SH, int L> struct Passes {
         int e = set_smem(kern, smem);
         if (e) return e;
         const int grid = (a.N + Q::RPC - 1) / Q::RPC;
+        typedef typename real_of<C>::type R;
         kern<<<grid, Q::THREADS, smem, s>>>((const C *)a.T, x, xs, (const C *)b, y, npart, (const C *)a.tw, a.N,
-                                              st, gate);
+                                              st, gate, a.transpose ? (const R *)a.cdiag : nullptr);
         return (int)cudaGetLastError();
     }
     static int inv(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xs, const void *b,

@@ -115,6 +115,27 @@ class FNO:
               "fno_train_step")
         return loss.value
 
+    def forward_train(self, chi, k0h, r):
+        """M(r) for a batch, keeping what backward() needs."""
+        B, H, W, chi, k0h, r = self._batch(chi, k0h, r)
+        cp, ck = _carr(chi, np.float32)
+        kp, kk = _carr(k0h, np.float32)
+        rp, rk = _carr(r, np.complex64)
+        z = np.empty((B, H, W), np.complex64)
+        check(_lib.lib().cugmres_fno_forward_train(self._net, B, H, W, cp, kp, rp,
+                                                   z.ctypes.data_as(ctypes.c_void_p)), "fno_forward_train")
+        return z
+
+    def backward(self, dm, lr=0.0, want_grad=False):
+        """Backward pass from dL/dM (complex, d/dRe + i d/dIm) of the last
+        forward_train batch; Adam step when lr > 0.  Returns the gradient if asked."""
+        d = np.ascontiguousarray(dm, np.complex64)
+        g = np.empty(self.num_params, np.float32) if want_grad else None
+        check(_lib.lib().cugmres_fno_backward(self._net, d.ctypes.data_as(ctypes.c_void_p),
+                                              g.ctypes.data_as(ctypes.c_void_p) if want_grad else None,
+                                              float(lr)), "fno_backward")
+        return g
+
     def save(self, path, **meta):
         np.savez_compressed(path, params=self.get_params(), **{k: np.asarray(v) for k, v in meta.items()})
 
@@ -181,6 +202,88 @@ def generate_pairs(N, designs, seed, eps_range=(2.0, 12.0), lh_range=(15.0, 30.0
         s.close()
     return dict(N=N, chi=np.stack(chis), k0h=np.asarray(k0hs, np.float32), r=np.stack(rs), x=np.stack(xs),
                 unconverged=unconverged, seconds=time.time() - t0)
+
+
+class DesignSet:
+    """Seeded random designs with one solver context each (operators set once),
+    for training on the residual-space loss."""
+
+    def __init__(self, N, count, seed, eps_range=(2.0, 12.0), lh_range=(15.0, 30.0), device=0, krylov=12):
+        from . import Solver
+        from . import problems
+        rng = np.random.default_rng(seed)
+        self.N = N
+        self.items = []
+        for _ in range(count):
+            eps = float(rng.uniform(*eps_range))
+            lh = float(rng.uniform(*lh_range))
+            pr = problems.helmholtz(N, eps, seed=int(rng.integers(1 << 30)), cells_per_wavelength=lh)
+            s = Solver(device)
+            s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+            th = rng.uniform(0, 2 * np.pi)
+            xc = (np.arange(N) + 0.5) * pr["h"]
+            b = np.exp(1j * pr["k0"] * (np.cos(th) * xc[:, None] + np.sin(th) * xc[None, :]))
+            kv = [b / np.linalg.norm(b)]  # Krylov sequence A^j b (normalised)
+            for _ in range(krylov):
+                v = s.matvec(kv[-1])
+                kv.append(v / np.linalg.norm(v))
+            self.items.append(dict(solver=s, chi=pr["chi"].astype(np.float32), k0h=pr["k0"] * pr["h"], b=b,
+                                   krylov=np.stack(kv), eps=eps, lh=lh, k0=pr["k0"], h=pr["h"]))
+
+    def close(self):
+        for it in self.items:
+            it["solver"].close()
+        self.items = []
+
+    def A(self, i, z):
+        return self.items[i]["solver"].matvec(np.ascontiguousarray(z, np.complex128))
+
+    def AH(self, i, e):
+        """A^H e = conj(A^T conj(e))."""
+        return np.conj(self.items[i]["solver"].matvec(np.ascontiguousarray(np.conj(e), np.complex128),
+                                                      transpose=True))
+
+    def sample_input(self, i, rng):
+        """A right-hand side of the kinds M meets: Krylov vectors, plane waves, smooth and white fields."""
+        it, N = self.items[i], self.N
+        u = rng.random()
+        if u < 0.4:
+            return it["krylov"][rng.integers(len(it["krylov"]))]
+        if u < 0.55:
+            return it["b"]
+        if u < 0.85:
+            return smooth_field(N, rng, rng.uniform(0.5, 8.0))
+        w = rng.standard_normal((N, N)) + 1j * rng.standard_normal((N, N))
+        return w / np.sqrt(2.0)
+
+
+def train_residual(net, designs, steps=1000, batch=16, lr=1e-3, lr_min=1e-5, seed=0, log=None, log_every=100):
+    """Adam on the preconditioning loss (1/B) sum ||A M(r) - r||^2 / ||r||^2 over
+    inputs drawn by DesignSet.sample_input; dL/dM = 2 A^H (A M(r) - r) / (B ||r||^2)."""
+    rng = np.random.default_rng(seed)
+    n = len(designs.items)
+    hist = []
+    t0 = time.time()
+    for it in range(steps):
+        idx = rng.integers(0, n, size=batch)
+        r = np.stack([designs.sample_input(i, rng) for i in idx]).astype(np.complex64)
+        chi = np.stack([designs.items[i]["chi"] for i in idx])
+        k0h = np.asarray([designs.items[i]["k0h"] for i in idx], np.float32)
+        z = net.forward_train(chi, k0h, r)
+        dm = np.empty_like(z)
+        loss = 0.0
+        for q, i in enumerate(idx):
+            rr = r[q].astype(np.complex128)
+            e = designs.A(i, z[q].astype(np.complex128)) - rr
+            nr = np.vdot(rr, rr).real
+            loss += np.vdot(e, e).real / nr / batch
+            dm[q] = (2.0 / (batch * nr)) * designs.AH(i, e)
+        a = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * it / max(1, steps)))
+        net.backward(dm, lr=a)
+        hist.append(loss)
+        if log and (it % log_every == 0 or it == steps - 1):
+            log(f"  step {it:5d}  residual loss {np.mean(hist[-log_every:]):.4f}  lr {a:.2e}  {time.time() - t0:.1f} s")
+    return np.asarray(hist)
 
 
 def train(net, data, steps=2000, batch=16, lr=1e-3, lr_min=1e-5, seed=0, log=None, log_every=200):

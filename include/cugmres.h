@@ -89,7 +89,10 @@ typedef struct {
     int preconditioner; /* CG_PRECOND_*; CG_PRECOND_LEARNED needs cugmres_set_preconditioner  */
     int learned_x0;     /* 1: with a preconditioner attached and zero_x0, start from x0 = M(b)
                            (kept only if ||b - A x0|| < ||b||, otherwise x0 = 0)             */
-    int reserved[5];
+    int transpose;      /* 1: solve A^T x = b, A^T = I - diag(c) G (the adjoint system of the
+                           reference's gradient path, CUDA_GMRES/GMRES.cuh:97-111; the adjoint
+                           A^H x = b is conj of the A^T solve with conj(b))                    */
+    int reserved[4];
 } cg_opts;
 
 /* right preconditioning */
@@ -146,6 +149,11 @@ int cugmres_matvec_shapes(const cg_ctx *ctx, int precision, int *shapes);
 /* y = A x.  precision CG_PREC_FP64: x, y are cg_c128 arrays; CG_PREC_MIXED:
  * cg_c64 arrays computed with the FP32 spectrum. */
 int cugmres_matvec(cg_ctx *ctx, const void *x, void *y, int precision);
+/* y = A^T x = x - diag(c) G x (G symmetric), the operator of PyGMRES
+ * matvec(..., transpose=True) (PyGMRES/GMRES.py:47-57) and of the reference's
+ * adjoint/gradient solve (CUDA_GMRES/GMRES.cuh:97-111, mask applied at the
+ * crop, GMRES_kernels.cuh:305-326).  A^H x = conj(A^T conj(x)). */
+int cugmres_matvec_transpose(cg_ctx *ctx, const void *x, void *y, int precision);
 /* r = b - A x in FP64; *rel = ||r|| / ||b|| (either output may be NULL). */
 int cugmres_residual(cg_ctx *ctx, const cg_c128 *b, const cg_c128 *x, cg_c128 *r, double *rel);
 
@@ -273,6 +281,14 @@ int cugmres_fno_loss_grad(cg_fno *net, int batch, int H, int W, const float *chi
 /* One Adam step (beta1 0.9, beta2 0.999, eps 1e-8) on the loss above. */
 int cugmres_fno_train_step(cg_fno *net, int batch, int H, int W, const float *chi, const float *k0h,
                            const cg_c64 *r, const cg_c64 *x, float lr, float *loss);
+/* Training with a caller-defined loss: forward_train computes z = M(r) and
+ * keeps what the backward pass needs; backward takes dL/dM (complex64
+ * [batch, H, W], as d/dRe + i d/dIm), writes the flat gradient (grad may be
+ * NULL) and, for lr > 0, takes one Adam step.  Any other network call in
+ * between discards the kept batch. */
+int cugmres_fno_forward_train(cg_fno *net, int batch, int H, int W, const float *chi, const float *k0h,
+                              const cg_c64 *r, cg_c64 *z);
+int cugmres_fno_backward(cg_fno *net, const cg_c64 *dm, float *grad, float lr);
 /* Attach (net != NULL) or detach the network to a context's solves;
  * k0h = k0 * h of the operator set with cugmres_set_operator, whose chi /
  * chi_scale give the contrast.  N of the operator must satisfy 32 <= N <= 1024. */

@@ -131,6 +131,16 @@ def matvec(ghat, chi, x, b=None, precision="c128"):
     return y
 
 
+def matvec_transpose(ghat, chi, x, precision="c128"):
+    """A^T x = x - chi G x (G symmetric): the transposed operator of the
+    reference's PyGMRES matvec(..., transpose=True) (PyGMRES/GMRES.py:52-53)
+    and of its CUDA gradient path (CUDA_GMRES/GMRES_kernels.cuh:305-326).
+    Built from the forward restatement: G x = x - (x - G (1 x))."""
+    x = np.asarray(x)
+    gx = x - matvec(ghat, np.ones(x.shape), x, precision=precision)
+    return x - np.asarray(chi) * gx
+
+
 def gmres_reference(ghat, chi, b, x0, maxiter, tol, precision="c128"):
     """Step-for-step restatement of FFT_GMRES_with_MKL (fixed maxiter, MGS,
     explicit Givens accumulation, LU solve).  Returns (x, res_hist, n, res_vs_tol, info)."""

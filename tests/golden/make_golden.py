@@ -24,7 +24,8 @@ Nothing at test time reads the reference checkout; the tests read only the
 * ``ref_results.json`` -- the published relative-error and residual histories
   (Results/relative_errors_256_0.npy, Results/residuals_256_0.npy).
 * ``pygmres_matvec.npz`` -- outputs of the reference's own NumPy functions
-  ``get_green_matrix``, ``get_toeplitz_mat`` and ``matvec`` (PyGMRES/GMRES.py:23-69)
+  ``get_green_matrix``, ``get_toeplitz_mat`` and ``matvec`` (also with
+  ``transpose=True``) (PyGMRES/GMRES.py:23-69)
   on seeded inputs.  Only the function definitions of GMRES.py are executed;
   its module-level benchmark loop (GMRES.py:95-221) is skipped.
 """
@@ -106,12 +107,14 @@ def main():
         x = (rng.standard_normal(n * n) + 1j * rng.standard_normal(n * n))
         eps = (rng.random((n * n, 1)) < 0.4).astype(np.float64) * 1.25
         y = ns["matvec"](x, eps, k)
+        yt = ns["matvec"](x, eps, k, transpose=True)
         gb = ns["get_green_matrix"](k, n)
         gt = ns["get_toeplitz_mat"](gb)
         out[f"x_{n}"] = x
         out[f"eps_{n}"] = eps
         out[f"k_{n}"] = np.float64(k)
         out[f"y_{n}"] = np.asarray(y).reshape(-1)
+        out[f"yt_{n}"] = np.asarray(yt).reshape(-1)
         out[f"green_block_{n}"] = gb
         out[f"toeplitz_{n}"] = gt
     np.savez_compressed(os.path.join(HERE, "pygmres_matvec.npz"), **out)

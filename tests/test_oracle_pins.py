@@ -45,6 +45,16 @@ def test_oracle_matvec_matches_pygmres(oracle, N):
     assert np.abs(yo - y).max() / np.abs(y).max() < 2e-7
 
 
+@pytest.mark.parametrize("N", [8, 16, 32])
+def test_oracle_transpose_matches_reference_pygmres(oracle, N):
+    """The reference's own matvec(x, eps, k, transpose=True) = x - chi G x."""
+    d = golden("pygmres_matvec.npz")
+    x, eps, k, yt = d[f"x_{N}"], d[f"eps_{N}"], float(d[f"k_{N}"]), d[f"yt_{N}"]
+    gh = oracle.spectrum(d[f"green_block_{N}"], 2 * N)
+    yo = oracle.matvec_transpose(gh, (k * k * eps).reshape(N, N), x.reshape(N, N)).ravel()
+    assert np.abs(yo - yt).max() / np.abs(yt).max() < 2e-7
+
+
 def test_oracle_fft_matches_numpy(oracle):
     rng = np.random.default_rng(0)
     for L in (8, 16, 12, 48, 64):
