@@ -40,7 +40,7 @@ EXPORTS = (
     "cugmres_matvec_shapes", "cugmres_solve_batch", "cugmres_fno_create", "cugmres_fno_destroy",
     "cugmres_fno_info", "cugmres_fno_get_params", "cugmres_fno_set_params", "cugmres_fno_forward",
     "cugmres_fno_loss_grad", "cugmres_fno_train_step", "cugmres_set_preconditioner", "cugmres_gemm_bf16",
-    "cugmres_matvec_transpose", "cugmres_fno_forward_train", "cugmres_fno_backward",
+    "cugmres_matvec_transpose", "cugmres_fno_forward_train", "cugmres_fno_backward", "cugmres_fno_set_local_last",
 )
 
 PHASES = ("matvec", "dots", "axpy", "small", "update", "residual", "precond")
@@ -167,6 +167,7 @@ def _declare(L):
     L.cugmres_set_preconditioner.argtypes = [P, P, D]
     L.cugmres_fno_forward_train.argtypes = [P, I, I, I, P, P, P, P]
     L.cugmres_fno_backward.argtypes = [P, P, P, F]
+    L.cugmres_fno_set_local_last.argtypes = [P, I]
     L.cugmres_gemm_bf16.argtypes = [I, LL, I, I, P, P, P]
     for name in EXPORTS:
         if name not in ("cugmres_strerror", "cugmres_default_opts", "cugmres_fno_destroy"):

@@ -240,7 +240,7 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
         CG_CU(cudaMalloc((void **)&c->kp.y, sizeof(double2) * mc));
         CG_CU(cudaMalloc((void **)&c->kp.hist, sizeof(double) * (ic + 1)));
         const size_t part_cgs2 = 2 * (size_t)dot_blocks(c) * (mc + 1);
-        const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms), dots2_blocks(1, c->sms)) *
+        const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms, mc), dots2_blocks(1, c->sms, mc)) *
                                   (size_t)dots2_part_ld(mc);
         CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(part_cgs2, part_dcgs2)));
         CG_CU(cudaMalloc((void **)&c->kp.npart, sizeof(double) * np));
@@ -880,7 +880,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     VecSel zk = vk;  // Z_k (input of the flexible Arnoldi matvec)
     zk.base = c->Z;
     const int nrb = row_blocks(c);
-    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(prec, c->sms);
+    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(prec, c->sms, c->mcap);
     const int nax2 = axpy2_blocks(prec, c->sms, c->mcap);
     int status = CG_OK;
 

@@ -69,6 +69,106 @@ static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
 // For j = 0..k: D1[j] = <V_j, u_k>, D2[j] = <V_j, w> with u_k = V[k], w = V[k+1].
 // Work items: groups of D2_J basis vectors; when there are fewer groups than
 // warps, each group's element range is split into S slices.
+// Tile-major variant of the two-right-hand-side dot pass: each warp owns
+// tiles of 32*U consecutive elements, keeps u and w of its tile in registers
+// and streams every basis vector q_j (j = 0..k) over the tile exactly once;
+// the four real sums of (q_j^H u, q_j^H w) are reduced across the warp with
+// shuffles in FP64 and added to the warp's own shared-memory slots, which the
+// block then sums in a fixed order (deterministic).  u and w are read once
+// from HBM instead of once per group of basis vectors.  FP32 vectors form
+// their products in FP32 over the U elements of a lane (FMA), everything after
+// that is FP64.  Shared memory: D2_WARPS * (mcap + 1) * 4 doubles.
+template <typename CV, int U>
+__global__ void __launch_bounds__(D2_THREADS) k_dots2t(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    typedef typename real_of<CV>::type R;
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int nj = k + 1;
+    const CV *u = V + (long long)k * n;
+    const CV *w = V + (long long)(k + 1) * n;
+    extern __shared__ double sacc[];  // [D2_WARPS][nj][4]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *my = sacc + (size_t)warp * nj * 4;
+    for (int q = lane; q < nj * 4; q += 32) my[q] = 0.0;
+    __syncwarp();
+    const long long TILE = 32LL * U;
+    const long long ntile = (n + TILE - 1) / TILE;
+    const long long nw = (long long)gridDim.x * D2_WARPS;
+    for (long long tile = (long long)blockIdx.x * D2_WARPS + warp; tile < ntile; tile += nw) {
+        const long long e0 = tile * TILE + lane;
+        const bool full = tile * TILE + TILE <= n;
+        CV uu[U], ww[U];
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            const long long e = e0 + 32 * t;
+            const bool ok = full || e < n;
+            uu[t] = ok ? u[e] : mk<CV>(0, 0);
+            ww[t] = ok ? w[e] : mk<CV>(0, 0);
+        }
+        CV a[U];
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            const long long e = e0 + 32 * t;
+            a[t] = (full || e < n) ? __ldcs(V + e) : mk<CV>(0, 0);
+        }
+        for (int j = 0; j < nj; j++) {
+            R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+            for (int t = 0; t < U; t++) {
+                s0 += a[t].x * uu[t].x + a[t].y * uu[t].y;
+                s1 += a[t].x * uu[t].y - a[t].y * uu[t].x;
+                s2 += a[t].x * ww[t].x + a[t].y * ww[t].y;
+                s3 += a[t].x * ww[t].y - a[t].y * ww[t].x;
+            }
+            if (j + 1 < nj) {  // next vector's tile in flight during the reduction
+                const CV *vn = V + (long long)(j + 1) * n;
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
+                }
+            }
+            double d0 = warp_sum((double)s0), d1 = warp_sum((double)s1);
+            double d2 = warp_sum((double)s2), d3 = warp_sum((double)s3);
+            if (lane == 0) {
+                my[4 * j] += d0;
+                my[4 * j + 1] += d1;
+                my[4 * j + 2] += d2;
+                my[4 * j + 3] += d3;
+            }
+        }
+    }
+    __syncthreads();
+    const int pld = part_ld(kp);
+    for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) {
+        double t = 0.0;
+        for (int wq = 0; wq < D2_WARPS; wq++) t += sacc[(size_t)wq * nj * 4 + q];
+        kp.part[4 * (size_t)blockIdx.x * pld + q] = t;
+    }
+    if (last_block2(&st->counter[3])) {
+        const int nparts = (int)gridDim.x;
+        for (int j = warp; j < nj; j += D2_WARPS) {
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            for (int b = lane; b < nparts; b += 32) {
+                const double *p = kp.part + 4 * ((size_t)b * pld + j);
+                s0 += __ldcg(p);
+                s1 += __ldcg(p + 1);
+                s2 += __ldcg(p + 2);
+                s3 += __ldcg(p + 3);
+            }
+            s0 = warp_sum(s0);
+            s1 = warp_sum(s1);
+            s2 = warp_sum(s2);
+            s3 = warp_sum(s3);
+            if (lane == 0) {
+                kp.D1[j] = make_double2(s0, s1);
+                kp.D2[j] = make_double2(s2, s3);
+            }
+        }
+    }
+}
+
 template <typename CV, bool COMP, int D2_J, int U>
 __global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     DevState *st = kp.st;
@@ -459,7 +559,7 @@ static int env_shape(const char *name, int nshapes) {
     return (v >= 0 && v < nshapes) ? v : -1;
 }
 static int dots2_shape(int prec_v) {
-    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 5);
+    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 7);
     return v >= 0 ? v : (prec_v == 0 ? 4 : 1);
 }
 static int axpy2_shape(int prec_v) {
@@ -475,6 +575,8 @@ template <typename CV, bool COMP> struct Dots2Table {
             case 2: return k_dots2<CV, COMP, 4, 1>;
             case 3: return k_dots2<CV, COMP, 8, 1>;
             case 4: return k_dots2<CV, COMP, 2, 4>;
+            case 5: return k_dots2t<CV, 4>;
+            case 6: return k_dots2t<CV, 8>;
             default: return k_dots2<CV, COMP, 4, 2>;
         }
     }
@@ -490,14 +592,34 @@ template <typename CV> struct Axpy2Table {
     }
 };
 
-int dots2_blocks(int prec_v, int sms) {
-    return prec_v == 0 ? waves_grid(Dots2Table<double2, false>::get(dots2_shape(0)), D2_THREADS, 0, sms)
-                       : waves_grid(Dots2Table<float2, true>::get(dots2_shape(1)), D2_THREADS, 0, sms);
+// Shape actually used: the tile-major shapes need D2_WARPS * (mcap+1) * 32 bytes
+// of shared memory and fall back to shape 0 above 96 KB (restart > 383).
+static size_t dots2_smem(int v, int mcap) {
+    return (v == 5 || v == 6) ? (size_t)D2_WARPS * (size_t)(mcap + 1) * 4 * sizeof(double) : 0;
+}
+static int dots2_shape_for(int prec_v, int mcap) {
+    const int v = dots2_shape(prec_v);
+    if ((v == 5 || v == 6) && dots2_smem(v, mcap) > 96 * 1024) return 0;
+    return v;
+}
+template <typename CV, bool COMP> static typename Dots2Table<CV, COMP>::K dots2_kernel(int v, size_t smem) {
+    typename Dots2Table<CV, COMP>::K kern = Dots2Table<CV, COMP>::get(v);
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return kern;
+}
+
+int dots2_blocks(int prec_v, int sms, int mcap) {
+    const int v = dots2_shape_for(prec_v, mcap);
+    const size_t smem = dots2_smem(v, mcap);
+    return prec_v == 0 ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
+                       : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
 }
 
 int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s) {
-    if (prec_v == 0) Dots2Table<double2, false>::get(dots2_shape(0))<<<nblk, D2_THREADS, 0, s>>>((const double2 *)V, n, kp);
-    else Dots2Table<float2, true>::get(dots2_shape(1))<<<nblk, D2_THREADS, 0, s>>>((const float2 *)V, n, kp);
+    const int v = dots2_shape_for(prec_v, kp.mcap);
+    const size_t smem = dots2_smem(v, kp.mcap);
+    if (prec_v == 0) dots2_kernel<double2, false>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const double2 *)V, n, kp);
+    else dots2_kernel<float2, true>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const float2 *)V, n, kp);
     return (int)cudaGetLastError();
 }
 

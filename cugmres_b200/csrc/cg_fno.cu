@@ -579,6 +579,42 @@ k_loss(float *__restrict__ o, const cg_c64 *__restrict__ x, const cg_c64 *__rest
     }
 }
 
+// Spectral-only last layer (no pointwise path): v = b + spectral (BF16), and
+// its backward dz_prev = dspec * GELU'(z_prev).
+__global__ void k_spec_bias(const float *__restrict__ spec, const float *__restrict__ bias, __nv_bfloat16 *__restrict__ v,
+                            long long cells, const int *gate) {
+    if (gated(gate)) return;
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cells;
+         e += (long long)gridDim.x * blockDim.x) {
+        float a[32];
+        const float4 *sp = reinterpret_cast<const float4 *>(spec + e * C);
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const float4 s4 = sp[q];
+            a[4 * q] = s4.x + bias[4 * q], a[4 * q + 1] = s4.y + bias[4 * q + 1];
+            a[4 * q + 2] = s4.z + bias[4 * q + 2], a[4 * q + 3] = s4.w + bias[4 * q + 3];
+        }
+        st_bf16x32(v + e * C, a);
+    }
+}
+__global__ void k_spec_bwd(const float *__restrict__ dspec, const __nv_bfloat16 *__restrict__ zprev,
+                           __nv_bfloat16 *__restrict__ dz, long long cells) {
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < cells;
+         e += (long long)gridDim.x * blockDim.x) {
+        float d[32], z[32];
+        const float4 *sp = reinterpret_cast<const float4 *>(dspec + e * C);
+#pragma unroll
+        for (int q = 0; q < 8; q++) {
+            const float4 s4 = sp[q];
+            d[4 * q] = s4.x, d[4 * q + 1] = s4.y, d[4 * q + 2] = s4.z, d[4 * q + 3] = s4.w;
+        }
+        ld_bf16x32(zprev + e * C, z);
+#pragma unroll
+        for (int q = 0; q < 32; q++) d[q] *= gelu_d(z[q]);
+        st_bf16x32(dz + e * C, d);
+    }
+}
+
 // dL/do from a caller's dL/dM (M = r + s (o0 + i o1), gradients as d/dRe + i d/dIm).
 __global__ void k_dout_from_dm(float *__restrict__ o, const cg_c64 *__restrict__ dm, const float *__restrict__ s,
                                long long hw, long long cells) {
@@ -822,6 +858,7 @@ struct cg_fno {
     int tw_H = 0, tw_W = 0;
     float2 *twh = nullptr, *tww = nullptr;
     float apply_k0h = -1.f;  // k0 h held in k0h[0] for single-vector applications
+    bool local_last = true;  // false: the last Fourier layer has no pointwise path (W_3 unused, held at 0)
     int fwd_B = 0, fwd_H = 0, fwd_W = 0;  // batch kept by cugmres_fno_forward_train
     std::mutex mu;
 };
@@ -1012,6 +1049,11 @@ int forward(cg_fno *f, cudaStream_t s, int B, int H, int W, const RT *r, const f
     FN_K(cudaGetLastError());
     for (int l = 0; l < LAYERS; l++) {
         FN_K(spectral_fwd(f, f->act[l], B, H, W, l, train ? f->X2s[l] : nullptr, gate, s));
+        if (l == LAYERS - 1 && !f->local_last) {
+            k_spec_bias<<<lb, 256, 0, s>>>(f->spec, f->p + off_b(l), f->act[l + 1], cells, gate);
+            FN_K(cudaGetLastError());
+            continue;
+        }
         EpiLayer e;
         e.bias = f->p + off_b(l);
         e.spec = f->spec;
@@ -1068,6 +1110,8 @@ int backward(cg_fno *f, cudaStream_t s, int B, int H, int W, const cg_c64 *r, co
     for (int l = LAYERS - 1; l >= 0; l--) {
         k_wgrad<C, C><<<nred, RED_THREADS, 0, s>>>(f->dz[cur], f->act[l], cells, f->part);
         k_reduce<<<(C * C + C + 255) / 256, 256, 0, s>>>(f->part, nred, C * C + C, f->g + off_w(l));
+        const bool spec_only = l == LAYERS - 1 && !f->local_last;
+        if (spec_only) FN_CU(cudaMemsetAsync(f->g + off_w(l), 0, sizeof(float) * C * C, s));
         // spectral adjoint: dY1 = adjoint of the inverse column DFT, then rows, modes, rows, columns
         k_dft_w_fwd<<<(unsigned)lines, 512, dft_w_fwd_smem(W), s>>>(f->dz[cur], W, f->tww, f->X1, inv, 2.f * inv,
                                                                       nullptr);
@@ -1076,6 +1120,12 @@ int backward(cg_fno *f, cudaStream_t s, int B, int H, int W, const cg_c64 *r, co
         k_dft_h_inv<<<dim3(B * HC, NJ / 128), 128, H * 8, s>>>(f->Y2, H, HC, f->twh, f->X1, nullptr);
         k_dft_w_inv<<<(unsigned)lines, 256, dft_w_inv_smem(W), s>>>(f->X1, W, f->tww, f->spec, 1.f, 1.f, nullptr);
         FN_K(cudaGetLastError());
+        if (spec_only) {  // dv = dspec only; l - 1 >= 0 has GELU
+            k_spec_bwd<<<nred, 256, 0, s>>>(f->spec, f->zpre[l - 1], f->dz[cur ^ 1], cells);
+            FN_K(cudaGetLastError());
+            cur ^= 1;
+            continue;
+        }
         EpiBwd e;
         e.dspec = f->spec;
         if (l > 0) {
@@ -1233,6 +1283,14 @@ extern "C" void cugmres_fno_destroy(cg_fno *f) {
     if (f->stream) cudaStreamDestroy(f->stream);
     cudaGetLastError();
     delete f;
+}
+
+extern "C" int cugmres_fno_set_local_last(cg_fno *f, int on) {
+    if (!f) return CG_ERR_INVALID;
+    std::lock_guard<std::mutex> lk(f->mu);
+    f->local_last = on != 0;
+    f->fwd_B = 0;
+    return CG_OK;
 }
 
 extern "C" int cugmres_fno_info(const cg_fno *f, cg_fno_info *info) {

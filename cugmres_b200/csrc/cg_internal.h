@@ -104,7 +104,7 @@ int launch_givens(const KrylovPtrs &kp, cudaStream_t s);
 int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
 int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s);
 int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
-int dots2_blocks(int prec_v, int sms);
+int dots2_blocks(int prec_v, int sms, int mcap);
 int axpy2_blocks(int prec_v, int sms, int mcap);
 // partials per block of the two-RHS dot pass
 __host__ __device__ inline int dots2_part_ld(int mcap) { return 2 * (mcap + 1) > 64 ? 2 * (mcap + 1) : 64; }

@@ -49,6 +49,10 @@ class FNO:
         except Exception:
             pass
 
+    def set_local_last(self, on):
+        """False: the last Fourier layer is spectral only (band-limited correction)."""
+        check(_lib.lib().cugmres_fno_set_local_last(self._net, int(bool(on))), "fno_set_local_last")
+
     def info(self):
         i = _lib.CgFnoInfo()
         check(_lib.lib().cugmres_fno_info(self._net, ctypes.byref(i)), "fno_info")

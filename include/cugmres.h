@@ -264,6 +264,11 @@ typedef struct {
 int cugmres_fno_create(cg_fno **net, int device, unsigned long long seed);
 void cugmres_fno_destroy(cg_fno *net);
 int cugmres_fno_info(const cg_fno *net, cg_fno_info *info);
+/* on = 1 (default): every Fourier layer has its pointwise path W_l; on = 0:
+ * the last layer is spectral only (v_4 = b_3 + S_3(v_3), W_3 unused and its
+ * gradient 0), so the correction the network adds is band-limited before the
+ * projection. */
+int cugmres_fno_set_local_last(cg_fno *net, int on);
 /* Flat FP32 parameters, in order: P [32 x 4], p [32]; per layer l = 0..3:
  * R_l [32 k1][16 k2][32 in][32 out] complex (re, im), W_l [32 out x 32 in],
  * b_l [32]; Q1 [128 x 32], bq1 [128], Q2 [2 x 128], bq2 [2].  set_params

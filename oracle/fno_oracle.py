@@ -117,9 +117,10 @@ def features(chi, k0h, r):
     return f, s, inv_s
 
 
-def forward(flat, chi, k0h, r, bf16=True, keep=False):
+def forward(flat, chi, k0h, r, bf16=True, keep=False, local_last=True):
     """M(r) (complex64 [B,H,W]), the raw outputs o [B,H,W,2] and, with keep,
-    the intermediates of the backward pass."""
+    the intermediates of the backward pass.  local_last=False: the last
+    Fourier layer has no pointwise path (W_3 is not used)."""
     p = unpack(flat)
     f, s, inv_s = features(chi, k0h, r)
     v = _rb(f @ p["P"].T + p["pb"], bf16)
@@ -127,6 +128,8 @@ def forward(flat, chi, k0h, r, bf16=True, keep=False):
     for l in range(LAYERS):
         Wl = _rb(p[f"W{l}"], bf16)
         sp = spectral(v, p[f"R{l}"])
+        if l == LAYERS - 1 and not local_last:
+            Wl = torch.zeros_like(Wl)
         z = v @ Wl.T + p[f"b{l}"] + sp
         zs.append(_rb(z, bf16))
         v = _rb(gelu(z) if l < LAYERS - 1 else z, bf16)
@@ -151,9 +154,9 @@ def _targets(r, x, inv_s):
     return t, wts
 
 
-def loss_grad(flat, chi, k0h, r, x, bf16=True):
+def loss_grad(flat, chi, k0h, r, x, bf16=True, local_last=True):
     """(loss, grad flat float32) by the manual backward pass of the GPU."""
-    fw = forward(flat, chi, k0h, r, bf16=bf16, keep=True)
+    fw = forward(flat, chi, k0h, r, bf16=bf16, keep=True, local_last=local_last)
     p, o, inv_s = fw["p"], fw["o"], fw["inv_s"]
     t, wts = _targets(r, x, inv_s)
     w = wts.reshape(-1, 1, 1, 1)
@@ -179,7 +182,11 @@ def loss_grad(flat, chi, k0h, r, x, bf16=True):
         out = spectral(vv, RR)
         gv, gR = torch.autograd.grad(out, (vv, RR), grad_outputs=dz)
         g[f"R{l}"] = gR  # torch's gradient of a real loss w.r.t. a complex leaf is d/dRe + i d/dIm
-        dv = dz @ _rb(p[f"W{l}"], bf16) + gv
+        if l == LAYERS - 1 and not local_last:
+            g[f"W{l}"] = torch.zeros_like(g[f"W{l}"])
+            dv = gv
+        else:
+            dv = dz @ _rb(p[f"W{l}"], bf16) + gv
         if l > 0:
             dz = _rb(dv * gelu_d(fw["zs"][l - 1]), bf16)
         else:
@@ -189,7 +196,7 @@ def loss_grad(flat, chi, k0h, r, x, bf16=True):
     return loss, pack(g)
 
 
-def loss_grad_autograd(flat, chi, k0h, r, x, dtype=torch.float64):
+def loss_grad_autograd(flat, chi, k0h, r, x, dtype=torch.float64, local_last=True):
     """(loss, grad) of the same loss by torch autograd, without BF16 rounding."""
     p = {k: v.to(dtype if not v.is_complex() else torch.complex128).clone().requires_grad_(True)
          for k, v in unpack(flat).items()}
@@ -197,7 +204,8 @@ def loss_grad_autograd(flat, chi, k0h, r, x, dtype=torch.float64):
     f = f.to(dtype)
     v = f @ p["P"].T + p["pb"]
     for l in range(LAYERS):
-        z = v @ p[f"W{l}"].T + p[f"b{l}"] + spectral(v, p[f"R{l}"])
+        Wl = p[f"W{l}"] if (l < LAYERS - 1 or local_last) else 0.0 * p[f"W{l}"]
+        z = v @ Wl.T + p[f"b{l}"] + spectral(v, p[f"R{l}"])
         v = gelu(z) if l < LAYERS - 1 else z
     o = gelu(v @ p["Q1"].T + p["bq1"]) @ p["Q2"].T + p["bq2"]
     t, wts = _targets(r, x, inv_s)

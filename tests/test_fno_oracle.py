@@ -19,10 +19,14 @@ def _setup(seed=0, B=2, H=32, W=40):
     return p, chi, k0h, r, x
 
 
-def test_manual_backward_matches_autograd():
+import pytest
+
+
+@pytest.mark.parametrize("local_last", [True, False])
+def test_manual_backward_matches_autograd(local_last):
     p, chi, k0h, r, x = _setup()
-    l1, g1 = FO.loss_grad(p, chi, k0h, r, x, bf16=False)
-    l2, g2 = FO.loss_grad_autograd(p, chi, k0h, r, x)
+    l1, g1 = FO.loss_grad(p, chi, k0h, r, x, bf16=False, local_last=local_last)
+    l2, g2 = FO.loss_grad_autograd(p, chi, k0h, r, x, local_last=local_last)
     assert abs(l1 - l2) <= 1e-6 * abs(l2)
     assert np.linalg.norm(g1 - g2) <= 1e-5 * np.linalg.norm(g2)
 

@@ -88,18 +88,25 @@ def test_fno_forward_matches_oracle(net, B, H, W):
     assert err < 2e-2, err
 
 
-def test_fno_gradients_match_oracle(net):
+@pytest.mark.parametrize("local_last", [True, False])
+def test_fno_gradients_match_oracle(net, local_last):
     p = _params(2)
     net.set_params(p)
+    net.set_local_last(local_last)
     chi, k0h, r, x = _inputs(2, 32, 40, 11)
     loss, g = net.loss_grad(chi, k0h, r, x)
-    loss_ref, g_ref = FO.loss_grad(p, chi, k0h, r, x, bf16=True)
+    net.set_local_last(True)
+    loss_ref, g_ref = FO.loss_grad(p, chi, k0h, r, x, bf16=True, local_last=local_last)
     assert abs(loss - loss_ref) <= 5e-3 * abs(loss_ref), (loss, loss_ref)
     blocks = {"P": (FO.OFF_P, FO.OFF_L0), "Q1": (FO.OFF_Q1, FO.OFF_Q2), "Q2": (FO.OFF_Q2, FO.NPARAM)}
     for l in range(FO.LAYERS):
         o = FO.off_r(l)
         blocks[f"R{l}"] = (o, o + FO.RSZ)
         blocks[f"W{l}"] = (o + FO.RSZ, o + FO.LSZ)
+    if not local_last:
+        o = FO.off_r(FO.LAYERS - 1) + FO.RSZ
+        assert np.all(g[o:o + FO.C * FO.C] == 0)
+        blocks[f"W{FO.LAYERS - 1}"] = (o + FO.C * FO.C, o + FO.C * FO.C + FO.C)  # b_3 only
     for name, (a, b) in blocks.items():
         e = np.linalg.norm(g[a:b] - g_ref[a:b]) / np.linalg.norm(g_ref[a:b])
         # the oracle mirrors every BF16 rounding of the GPU; the rest is FP32 summation order
