@@ -77,78 +77,82 @@ static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
 // block then sums in a fixed order (deterministic).  u and w are read once
 // from HBM instead of once per group of basis vectors.  FP32 vectors form
 // their products in FP32 over the U elements of a lane (FMA), everything after
-// that is FP64.  Shared memory: D2_WARPS * (mcap + 1) * 4 doubles.
+// that is FP64.  The basis is processed in chunks of cs = min(mcap + 1,
+// D2T_CHUNK) vectors (u and w are re-read once per chunk), so shared memory is
+// D2_WARPS * cs * 4 doubles (at most 64 KB) whatever the restart length.
+static constexpr int D2T_CHUNK = 256;
 template <typename CV, int U>
 __global__ void __launch_bounds__(D2_THREADS) k_dots2t(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
     const int k = st->k;
-    const int nj = k + 1;
+    const int njt = k + 1;
     const CV *u = V + (long long)k * n;
     const CV *w = V + (long long)(k + 1) * n;
-    extern __shared__ double sacc[];  // [D2_WARPS][nj][4]
+    extern __shared__ double sacc[];  // [D2_WARPS][cs][4]
+    const int cs = kp.mcap + 1 < D2T_CHUNK ? kp.mcap + 1 : D2T_CHUNK;  // chunk of basis vectors
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double *my = sacc + (size_t)warp * nj * 4;
-    for (int q = lane; q < nj * 4; q += 32) my[q] = 0.0;
-    __syncwarp();
+    double *my = sacc + (size_t)warp * cs * 4;
+    const int pld = part_ld(kp);
     const long long TILE = 32LL * U;
     const long long ntile = (n + TILE - 1) / TILE;
     const long long nw = (long long)gridDim.x * D2_WARPS;
-    for (long long tile = (long long)blockIdx.x * D2_WARPS + warp; tile < ntile; tile += nw) {
-        const long long e0 = tile * TILE + lane;
-        const bool full = tile * TILE + TILE <= n;
-        CV uu[U], ww[U];
-#pragma unroll
-        for (int t = 0; t < U; t++) {
-            const long long e = e0 + 32 * t;
-            const bool ok = full || e < n;
-            uu[t] = ok ? u[e] : mk<CV>(0, 0);
-            ww[t] = ok ? w[e] : mk<CV>(0, 0);
-        }
-        CV a[U];
-#pragma unroll
-        for (int t = 0; t < U; t++) {
-            const long long e = e0 + 32 * t;
-            a[t] = (full || e < n) ? __ldcs(V + e) : mk<CV>(0, 0);
-        }
-        for (int j = 0; j < nj; j++) {
-            R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int jc = 0; jc < njt; jc += cs) {
+        const int nj = njt - jc < cs ? njt - jc : cs;
+        const CV *Vc = V + (long long)jc * n;
+        for (int q = lane; q < nj * 4; q += 32) my[q] = 0.0;
+        __syncwarp();
+        for (long long tile = (long long)blockIdx.x * D2_WARPS + warp; tile < ntile; tile += nw) {
+            const long long e0 = tile * TILE + lane;
+            const bool full = tile * TILE + TILE <= n;
+            CV uu[U], ww[U], a[U];
 #pragma unroll
             for (int t = 0; t < U; t++) {
-                s0 += a[t].x * uu[t].x + a[t].y * uu[t].y;
-                s1 += a[t].x * uu[t].y - a[t].y * uu[t].x;
-                s2 += a[t].x * ww[t].x + a[t].y * ww[t].y;
-                s3 += a[t].x * ww[t].y - a[t].y * ww[t].x;
+                const long long e = e0 + 32 * t;
+                const bool ok = full || e < n;
+                uu[t] = ok ? u[e] : mk<CV>(0, 0);
+                ww[t] = ok ? w[e] : mk<CV>(0, 0);
+                a[t] = ok ? __ldcs(Vc + e) : mk<CV>(0, 0);
             }
-            if (j + 1 < nj) {  // next vector's tile in flight during the reduction
-                const CV *vn = V + (long long)(j + 1) * n;
+            for (int j = 0; j < nj; j++) {
+                R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
                 for (int t = 0; t < U; t++) {
-                    const long long e = e0 + 32 * t;
-                    a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
+                    s0 += a[t].x * uu[t].x + a[t].y * uu[t].y;
+                    s1 += a[t].x * uu[t].y - a[t].y * uu[t].x;
+                    s2 += a[t].x * ww[t].x + a[t].y * ww[t].y;
+                    s3 += a[t].x * ww[t].y - a[t].y * ww[t].x;
+                }
+                if (j + 1 < nj) {  // next vector's tile in flight during the reduction
+                    const CV *vn = Vc + (long long)(j + 1) * n;
+#pragma unroll
+                    for (int t = 0; t < U; t++) {
+                        const long long e = e0 + 32 * t;
+                        a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
+                    }
+                }
+                const double d0 = warp_sum((double)s0), d1 = warp_sum((double)s1);
+                const double d2 = warp_sum((double)s2), d3 = warp_sum((double)s3);
+                if (lane == 0) {
+                    my[4 * j] += d0;
+                    my[4 * j + 1] += d1;
+                    my[4 * j + 2] += d2;
+                    my[4 * j + 3] += d3;
                 }
             }
-            double d0 = warp_sum((double)s0), d1 = warp_sum((double)s1);
-            double d2 = warp_sum((double)s2), d3 = warp_sum((double)s3);
-            if (lane == 0) {
-                my[4 * j] += d0;
-                my[4 * j + 1] += d1;
-                my[4 * j + 2] += d2;
-                my[4 * j + 3] += d3;
-            }
         }
-    }
-    __syncthreads();
-    const int pld = part_ld(kp);
-    for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) {
-        double t = 0.0;
-        for (int wq = 0; wq < D2_WARPS; wq++) t += sacc[(size_t)wq * nj * 4 + q];
-        kp.part[4 * (size_t)blockIdx.x * pld + q] = t;
+        __syncthreads();
+        for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) {
+            double t = 0.0;
+            for (int wq = 0; wq < D2_WARPS; wq++) t += sacc[(size_t)wq * cs * 4 + q];
+            kp.part[4 * ((size_t)blockIdx.x * pld + jc) + q] = t;
+        }
+        __syncthreads();
     }
     if (last_block2(&st->counter[3])) {
         const int nparts = (int)gridDim.x;
-        for (int j = warp; j < nj; j += D2_WARPS) {
+        for (int j = warp; j < njt; j += D2_WARPS) {
             double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
             for (int b = lane; b < nparts; b += 32) {
                 const double *p = kp.part + 4 * ((size_t)b * pld + j);
@@ -546,11 +550,13 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 }
 
 // ------------------------------------------------------------- launchers
-// Shapes of the two streaming passes: (J, U) of k_dots2 and the j-unroll of
-// k_axpy2, per precision.  The defaults were chosen by measurement on B200 at
-// N = 1024, restart 100 (300 steps, k = 0..99): FP64 dots (2,4) 81.7 ms vs
-// (4,2) 92.9 ms, FP32 dots (2,2) 80.3 ms vs (4,2) 99.4 ms; FP64 axpy unroll 4,
-// FP32 axpy unroll 8 (36.4 ms vs 43.2 ms).  CUGMRES_DOTS2_SHAPE /
+// Shapes of the two streaming passes: the dot pass's variant (0-4: (J, U) of
+// k_dots2; 5, 6: tile-major k_dots2t with U = 4, 8) and the j-unroll of
+// k_axpy2, per precision.  Measured on B200 at N = 1024, restart 100 (300
+// steps, k = 0..99): FP64 dots 91.6 ms (shape 0), 81.0 (4), 61.4 (5), 54.2 ms
+// (6, 4.9 TB/s); FP32 97.6, 78.8 (1), 58.7 (5), 42.9 ms (6).  Shape 6 is the
+// default for both precisions.  FP64
+// axpy unroll 4, FP32 unroll 8 (36.4 ms vs 43.2 ms).  CUGMRES_DOTS2_SHAPE /
 // CUGMRES_AXPY2_SHAPE override both precisions (diagnostics).
 static int env_shape(const char *name, int nshapes) {
     const char *e = getenv(name);
@@ -558,9 +564,9 @@ static int env_shape(const char *name, int nshapes) {
     const int v = atoi(e);
     return (v >= 0 && v < nshapes) ? v : -1;
 }
-static int dots2_shape(int prec_v) {
+static int dots2_shape(int) {
     static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 7);
-    return v >= 0 ? v : (prec_v == 0 ? 4 : 1);
+    return v >= 0 ? v : 6;
 }
 static int axpy2_shape(int prec_v) {
     static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 3);
@@ -595,12 +601,12 @@ template <typename CV> struct Axpy2Table {
 // Shape actually used: the tile-major shapes need D2_WARPS * (mcap+1) * 32 bytes
 // of shared memory and fall back to shape 0 above 96 KB (restart > 383).
 static size_t dots2_smem(int v, int mcap) {
-    return (v == 5 || v == 6) ? (size_t)D2_WARPS * (size_t)(mcap + 1) * 4 * sizeof(double) : 0;
+    const int jc = mcap + 1 < D2T_CHUNK ? mcap + 1 : D2T_CHUNK;
+    return (v == 5 || v == 6) ? (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double) : 0;
 }
 static int dots2_shape_for(int prec_v, int mcap) {
-    const int v = dots2_shape(prec_v);
-    if ((v == 5 || v == 6) && dots2_smem(v, mcap) > 96 * 1024) return 0;
-    return v;
+    (void)mcap;
+    return dots2_shape(prec_v);
 }
 template <typename CV, bool COMP> static typename Dots2Table<CV, COMP>::K dots2_kernel(int v, size_t smem) {
     typename Dots2Table<CV, COMP>::K kern = Dots2Table<CV, COMP>::get(v);
