@@ -55,6 +55,8 @@ def parse():
     ap.add_argument("--cpu-sample-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and 256^2 side measurements")
+    ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner side measurement")
+    ap.add_argument("--learned-steps", type=int, default=1500)
     return ap.parse_args()
 
 
@@ -204,6 +206,48 @@ def side_measurements(args, stream):
     return out
 
 
+def learned_side(args, stream):
+    """The learned+mixed arm: a spectral-convolution network trained here on
+    the solver's own operators (64^2 designs, eps_r ~ U(2, 6), residual loss,
+    not timed) as initial guess and flexible right preconditioner of the
+    mixed-precision solve, on the same capped 1024^2 solve and on a 256^2
+    time-to-tol solve, next to plain FP64 on the same systems."""
+    import torch
+    import cugmres_b200 as cg
+    from cugmres_b200 import learned as Lr
+    from cugmres_b200 import problems as P
+    out = {}
+    t0 = time.perf_counter()
+    ds = Lr.DesignSet(64, 64, seed=500, eps_range=(2.0, 6.0))
+    net = Lr.FNO(torch.cuda.current_device(), seed=1)
+    hist = Lr.train_residual(net, ds, steps=args.learned_steps, batch=16, lr=1e-3)
+    ds.close()
+    out["training"] = {"designs": 64, "grid": 64, "steps": args.learned_steps, "seconds": time.perf_counter() - t0,
+                       "final_residual_loss": float(np.mean(hist[-100:]))}
+    for N, restart, maxit in ((args.N, args.restart, args.max_iter), (256, 2500, 2500)):
+        pr = P.helmholtz(N, args.eps, seed=args.seed)
+        s = cg.Solver(torch.cuda.current_device())
+        s.set_stream(stream.cuda_stream)
+        s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+        s.set_preconditioner(net, pr["k0"] * pr["h"])
+        b = torch.from_numpy(pr["b"]).cuda()
+        row = {}
+        for name, kw in (("plain_fp64", dict(precision="fp64")),
+                         ("learned_mixed", dict(precision="mixed", preconditioner="learned", learned_x0=True,
+                                                inner_tol=1e-6))):
+            kw.update(restart=restart, max_iter=maxit, tol=args.tol)
+            s.solve(b, **kw)
+            ms, info = timed_solves(s, b, kw, 1, stream)
+            row[name] = {"s": ms / 1e3, "steps": info["iterations"], "status": info["status_text"],
+                         "rel_residual_true": info["rel_residual_true"],
+                         "preconditioned_cycles": info["preconditioned_cycles"], "x0_learned": info["x0_learned"]}
+        s.set_preconditioner(None)
+        s.close()
+        out[f"{N}x{N}_restart{restart}_max_iter{maxit}"] = row
+    net.close()
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference's CPU GMRES (oracle port: MKL absent) on the host cores."""
     if rank != 0:
@@ -312,11 +356,15 @@ def main():
             "e2e": {"value": e2e_wall, "unit": "s", "h2d_bytes_per_step": int(pr["b"].nbytes),
                     "d2h_bytes_per_step": int(pr["b"].nbytes)},
             "gpu_launches": None, "clocks": clk}
-    # our kernels per solve (delayed CGS2): 6 per Arnoldi step (3 matvec passes, dots, step, axpy),
-    # per cycle one extra step plus 3 residual passes, cycle set-up, back-solve, update; 1 norm of b
-    line["gpu_launches"] = int(args.steps * (6 * last["iterations"] + 12 * last["cycles"] + 5))
+    # our kernels per solve (delayed CGS2, one CUDA-graph replay per cycle): 6 per Arnoldi step
+    # (3 matvec passes, dots, step, axpy) for restart+1 steps per cycle (steps after the device stops
+    # the cycle return at once), back-solve, update, 3 residual passes and the cycle set-up per cycle,
+    # plus the norm of b, the first residual and cycle set-up
+    line["gpu_launches"] = int(args.steps * (last["cycles"] * (6 * (args.restart + 1) + 6) + 5))
     if rank == 0 and world == 1 and not args.no_extras:
         line["side"] = side_measurements(args, stream)
+        if not args.no_learned:
+            line["side"]["learned"] = learned_side(args, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, pr, last["iterations"])
     if rank == 0:

@@ -69,6 +69,10 @@ struct cg_ctx {
     bool prof = false;
     std::vector<cudaEvent_t> evpool;
     cg_phase_stats stats[CG_NPHASES] = {};
+    // CUDA graph of one restart cycle (replayed with one launch per cycle)
+    cudaStream_t cap_stream = nullptr;  // capture only; the graph is launched on `stream`
+    cudaGraphExec_t gexec = nullptr;
+    unsigned char gkey[256] = {0};
     // learned preconditioner (flexible GMRES)
     cg_fno *net = nullptr;
     double k0h = 0.0;
@@ -91,6 +95,16 @@ int cuerr(cudaError_t e) { return e == cudaSuccess ? CG_OK : (e == cudaErrorMemo
         int _e = (expr);                                 \
         if (_e != 0) return CG_ERR_CUDA;                 \
     } while (0)
+
+// CUGMRES_GRAPHS=0 launches every kernel directly instead of replaying the
+// captured restart cycle.
+bool graphs_enabled() {
+    static const bool on = [] {
+        const char *e = getenv("CUGMRES_GRAPHS");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
 
 bool is_device_ptr(const void *p) {
     if (!p) return false;
@@ -189,7 +203,13 @@ void free_operator(cg_ctx *c) {
     c->have_op = false;
 }
 
+void free_graph(cg_ctx *c) {
+    if (c->gexec) cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+}
+
 void free_krylov(cg_ctx *c) {
+    free_graph(c);
     dfree(c->V);
     dfree_t(c->kp.scale);
     dfree_t(c->kp.h1);
@@ -574,6 +594,8 @@ int cugmres_destroy(cg_ctx *c) {
     if (c->st_host) cudaFreeHost(c->st_host);
     if (c->ev) cudaEventDestroy(c->ev);
     for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
+    free_graph(c);
+    if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CG_OK;
@@ -884,7 +906,6 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     const int nax2 = axpy2_blocks(prec, c->sms, c->mcap);
     int status = CG_OK;
 
-    bool use_prec = learned;     // this cycle runs the learned preconditioner
     int prec_cycles = 0, x0_learned = 0;
     double cycle_start_res = -1.0;  // true residual at the start of the last preconditioned cycle
     if (learned && o.learned_x0 && o.zero_x0) {
@@ -896,16 +917,115 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     CycleProf cp;
     int it_prev = 0;
     const double nd = (double)n, esz_d = prec == 0 ? 16.0 : 8.0;
+
+    // True residual r = b - A x (FP64) into V_0, the cycle decisions on the
+    // device, and the copy of the state to the host.
+    auto enqueue_begin = [&](cudaStream_t q) -> int {
+        CG_LAUNCH(launch_rows_forward(0, a64, xs, nullptr, nullptr, GATE_NONE, q));
+        CG_LAUNCH(launch_cols_convolve(0, a64, nullptr, GATE_NONE, q));
+        CG_LAUNCH(launch_rows_inverse(0, 1, prec, a64, xs, nullptr, bp, fixed_vec(c->V), kp.npart, nullptr, GATE_NONE, q));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_RESIDUAL, -1, q));
+        CG_LAUNCH(launch_cycle_begin(kp, nrb, q));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
+        CG_CU(cudaMemcpyAsync(c->st_host, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, q));
+        return CG_OK;
+    };
+    // One restart cycle: `steps` Arnoldi steps (launches after the device
+    // stops the cycle return at once), back-solve and solution update.
+    bool use_prec = learned;  // this cycle runs the learned preconditioner
+    auto enqueue_cycle = [&](int steps, cudaStream_t q) -> int {
+        for (int i = 0; i < steps; i++) {
+            if (delayed) {
+                // w = A u_k into V[k+1]; one dot pass; normalisation + Givens; one axpy pass
+                CG_LAUNCH(launch_rows_forward(prec, ap, vk, nullptr, c->st, GATE_STOP, q));
+                CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, q));
+                CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, nullptr, nullptr, vk1, nullptr, c->st, GATE_STOP, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, q));
+                CG_LAUNCH(launch_dots2(prec, c->V, n, kp, ndot2, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, q));
+                CG_LAUNCH(launch_dcgs2_step(kp, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, q));
+                CG_LAUNCH(launch_axpy2(prec, c->V, n, kp, nax2, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, q));
+                continue;
+            }
+            if (use_prec) {
+                // z_i = M(v_i) on the unnormalised stored vector (M is positively homogeneous)
+                CG_TRY(fno::apply(c->net, q, c->N, prec, (const char *)c->V + (size_t)i * n * esz, c->chi32,
+                                  (float)c->k0h, (char *)c->Z + (size_t)i * n * esz, &c->st->stop));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_PRECOND, i, q));
+            }
+            const VecSel &min = use_prec ? zk : vk;
+            CG_LAUNCH(launch_rows_forward(prec, ap, min, kp.scale, c->st, GATE_STOP, q));
+            CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, q));
+            CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, min, kp.scale, nullptr, vk1, nullptr, c->st, GATE_STOP, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, q));
+            CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h1, 0, ndot, GATE_STOP, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, q));
+            CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h1, -1.0, NJ_K_PLUS_1, vk1, 0, 1, nax, GATE_STOP, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, q));
+            CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h2, 0, ndot, GATE_STOP, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, q));
+            CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h2, -1.0, NJ_K_PLUS_1, vk1, 1, 1, nax, GATE_STOP, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, q));
+            CG_LAUNCH(launch_givens(kp, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, q));
+        }
+        CG_LAUNCH(launch_backsolve(kp, q));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
+        CG_LAUNCH(launch_axpy(prec, 0, use_prec ? c->Z : c->V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, q));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, q));
+        return CG_OK;
+    };
+    // Graph replay of [cycle + next residual/decisions] when nothing in it
+    // changes between cycles (not while profiling, not with the network).
+    const bool graphs = !c->prof && !learned && graphs_enabled();
+    unsigned char key[256];
+    memset(key, 0, sizeof(key));
+    {
+        struct K {
+            int prec, delayed, m, transpose, ndot, nax, ndot2, nax2, nrb, mcap, var[2][3];
+            long long n;
+            const void *V, *x, *b, *st, *scale, *part;
+        } kk;
+        memset(&kk, 0, sizeof(kk));
+        kk.prec = prec, kk.delayed = delayed, kk.m = m, kk.transpose = o.transpose, kk.ndot = ndot, kk.nax = nax;
+        kk.ndot2 = ndot2, kk.nax2 = nax2, kk.nrb = nrb, kk.mcap = c->mcap, kk.n = n;
+        memcpy(kk.var, c->var, sizeof(kk.var));
+        kk.V = c->V, kk.x = xp, kk.b = bp, kk.st = c->st, kk.scale = kp.scale, kk.part = kp.part;
+        static_assert(sizeof(K) <= sizeof(key), "graph key");
+        memcpy(key, &kk, sizeof(kk));
+    }
+    auto launch_cycle_graph = [&]() -> int {
+        if (!c->gexec || memcmp(c->gkey, key, sizeof(key)) != 0) {
+            free_graph(c);
+            if (!c->cap_stream) CG_CU(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
+            cudaGraph_t g = nullptr;
+            CG_CU(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
+            int e1 = enqueue_cycle(m + (delayed ? 1 : 0), c->cap_stream);
+            int e2 = e1 == CG_OK ? enqueue_begin(c->cap_stream) : e1;
+            cudaError_t ce = cudaStreamEndCapture(c->cap_stream, &g);
+            if (e2 != CG_OK || ce != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                cudaGetLastError();
+                return e2 != CG_OK ? e2 : CG_ERR_CUDA;
+            }
+            ce = cudaGraphInstantiate(&c->gexec, g, 0);
+            cudaGraphDestroy(g);
+            if (ce != cudaSuccess) {
+                c->gexec = nullptr;
+                cudaGetLastError();
+                return CG_ERR_CUDA;
+            }
+            memcpy(c->gkey, key, sizeof(key));
+        }
+        CG_CU(cudaGraphLaunch(c->gexec, s));
+        return CG_OK;
+    };
+
+    if (cp.used == 0) CG_TRY(prof_mark(c, cp, -1, -1, s));
+    CG_TRY(enqueue_begin(s));
     for (;;) {
-        if (cp.used == 0) CG_TRY(prof_mark(c, cp, -1, -1, s));
-        // true residual r = b - A x (FP64) into V_0, then cycle decisions on device
-        CG_LAUNCH(launch_rows_forward(0, a64, xs, nullptr, nullptr, GATE_NONE, s));
-        CG_LAUNCH(launch_cols_convolve(0, a64, nullptr, GATE_NONE, s));
-        CG_LAUNCH(launch_rows_inverse(0, 1, prec, a64, xs, nullptr, bp, fixed_vec(c->V), kp.npart, nullptr, GATE_NONE, s));
-        CG_TRY(prof_mark(c, cp, CG_PHASE_RESIDUAL, -1, s));
-        CG_LAUNCH(launch_cycle_begin(kp, nrb, s));
-        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, s));
-        CG_CU(cudaMemcpyAsync(c->st_host, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
         CG_CU(cudaEventRecord(c->ev, s));
         CG_CU(cudaEventSynchronize(c->ev));
         const DevState hs = *c->st_host;
@@ -920,6 +1040,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             h2.cycles = 0;
             *c->st_host = h2;
             CG_CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(DevState), cudaMemcpyHostToDevice, s));
+            if (cp.used == 0) CG_TRY(prof_mark(c, cp, -1, -1, s));
+            CG_TRY(enqueue_begin(s));
             continue;
         }
         if (use_prec && cycle_start_res >= 0.0 && !(hs.true_res < 0.9 * cycle_start_res)) use_prec = false;
@@ -933,48 +1055,13 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             cycle_start_res = hs.true_res;
             prec_cycles++;
         }
-        const int steps = std::min(m, o.max_iter - hs.it) + (delayed ? 1 : 0);
-        for (int i = 0; i < steps; i++) {
-            if (delayed) {
-                // w = A u_k into V[k+1]; one dot pass; normalisation + Givens; one axpy pass
-                CG_LAUNCH(launch_rows_forward(prec, ap, vk, nullptr, c->st, GATE_STOP, s));
-                CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, s));
-                CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, nullptr, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
-                CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, s));
-                CG_LAUNCH(launch_dots2(prec, c->V, n, kp, ndot2, s));
-                CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
-                CG_LAUNCH(launch_dcgs2_step(kp, s));
-                CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, s));
-                CG_LAUNCH(launch_axpy2(prec, c->V, n, kp, nax2, s));
-                CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
-                continue;
-            }
-            if (use_prec) {
-                // z_i = M(v_i) on the unnormalised stored vector (M is positively homogeneous)
-                CG_TRY(fno::apply(c->net, s, c->N, prec, (const char *)c->V + (size_t)i * n * esz, c->chi32,
-                                  (float)c->k0h, (char *)c->Z + (size_t)i * n * esz, &c->st->stop));
-                CG_TRY(prof_mark(c, cp, CG_PHASE_PRECOND, i, s));
-            }
-            const VecSel &min = use_prec ? zk : vk;
-            CG_LAUNCH(launch_rows_forward(prec, ap, min, kp.scale, c->st, GATE_STOP, s));
-            CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, s));
-            CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, min, kp.scale, nullptr, vk1, nullptr, c->st, GATE_STOP, s));
-            CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, s));
-            CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h1, 0, ndot, GATE_STOP, s));
-            CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
-            CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h1, -1.0, NJ_K_PLUS_1, vk1, 0, 1, nax, GATE_STOP, s));
-            CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
-            CG_LAUNCH(launch_dots(prec, c->V, n, kp, vk1, kp.h2, 0, ndot, GATE_STOP, s));
-            CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, s));
-            CG_LAUNCH(launch_axpy(prec, prec, c->V, n, kp, kp.h2, -1.0, NJ_K_PLUS_1, vk1, 1, 1, nax, GATE_STOP, s));
-            CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, s));
-            CG_LAUNCH(launch_givens(kp, s));
-            CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, s));
+        if (graphs) {
+            CG_TRY(launch_cycle_graph());
+        } else {
+            CG_TRY(enqueue_cycle(std::min(m, o.max_iter - hs.it) + (delayed ? 1 : 0), s));
+            CG_TRY(prof_mark(c, cp, -1, -1, s));
+            CG_TRY(enqueue_begin(s));
         }
-        CG_LAUNCH(launch_backsolve(kp, s));
-        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, s));
-        CG_LAUNCH(launch_axpy(prec, 0, use_prec ? c->Z : c->V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, s));
-        CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, s));
     }
     if (learned) CG_TRY(fno::check_error(c->net));
 
