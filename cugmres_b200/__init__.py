@@ -133,6 +133,17 @@ class Solver:
         self._grid()
         return self
 
+    def set_operator_green(self, N, chi, chi_scale, k0=0.0, h=0.0, kind="helmholtz"):
+        """Operator set-up entirely on the GPU: Green's block of `kind` ('helmholtz',
+        'reference', 'pygmres'), embedding and spectrum; only chi is copied."""
+        kinds = {"helmholtz": _lib.CG_GREEN_HELMHOLTZ, "reference": _lib.CG_GREEN_REFERENCE,
+                 "pygmres": _lib.CG_GREEN_PYGMRES}
+        cp, ck = _arg(chi, np.float64)
+        check(_lib.lib().cugmres_set_operator_green(self._ctx, kinds[kind], int(N), float(k0), float(h), cp,
+                                                    float(chi_scale)), "set_operator_green")
+        self._grid()
+        return self
+
     def matvec(self, x, precision="fp64", out=None, transpose=False):
         """y = A x (transpose: y = A^T x = x - diag(c) G x); precision 'fp64'
         (complex128) or 'fp32' (complex64)."""
@@ -210,25 +221,28 @@ class Solver:
 
 
 def solve_batch(systems, device=0, workers=8, restart=100, max_iter=10000, tol=1e-10, precision="fp64",
-                givens="unitary", inner_tol=1e-5, ortho="dcgs2"):
+                givens="unitary", inner_tol=1e-5, ortho="dcgs2", device_green=False):
     """Solve many independent systems concurrently (cugmres_solve_batch).
 
-    systems: iterable of dicts with g_block, chi, chi_scale, b and optionally x0.
+    systems: iterable of dicts with g_block (or k0 and h: the GFIEM block is
+    then built on the GPU; device_green=True forces that), chi, chi_scale, b
+    and optionally x0.
     Returns (xs, infos): solutions (complex128 N x N) and per-system dicts with
     status, iterations, rel_residual_true and seconds (set-up + solve latency)."""
     systems = list(systems)
     keep, arr = [], (_lib.CgSystem * max(1, len(systems)))()
     xs = []
     for i, sysd in enumerate(systems):
-        N = int(sysd["g_block"].shape[0])
-        g = np.ascontiguousarray(sysd["g_block"], np.complex128)
         c = np.ascontiguousarray(sysd["chi"], np.float64)
+        N = int(c.shape[0])
+        g = None if device_green or sysd.get("g_block") is None else np.ascontiguousarray(sysd["g_block"], np.complex128)
         b = np.ascontiguousarray(sysd["b"], np.complex128)
         x = np.zeros((N, N), np.complex128) if sysd.get("x0") is None else np.array(sysd["x0"], np.complex128)
         keep += [g, c, b]
         xs.append(x)
-        arr[i] = _lib.CgSystem(N, g.ctypes.data, c.ctypes.data, float(sysd.get("chi_scale", 1.0)), b.ctypes.data,
-                               x.ctypes.data)
+        arr[i] = _lib.CgSystem(N, g.ctypes.data if g is not None else None, c.ctypes.data,
+                               float(sysd.get("chi_scale", 1.0)), b.ctypes.data, x.ctypes.data,
+                               float(sysd.get("k0", 0.0)), float(sysd.get("h", 0.0)))
     o = _lib.CgOpts()
     _lib.lib().cugmres_default_opts(ctypes.byref(o))
     o.restart, o.max_iter, o.tol = int(restart), int(max_iter), float(tol)

@@ -41,6 +41,7 @@ EXPORTS = (
     "cugmres_fno_info", "cugmres_fno_get_params", "cugmres_fno_set_params", "cugmres_fno_forward",
     "cugmres_fno_loss_grad", "cugmres_fno_train_step", "cugmres_set_preconditioner", "cugmres_gemm_bf16",
     "cugmres_matvec_transpose", "cugmres_fno_forward_train", "cugmres_fno_backward", "cugmres_fno_set_local_last",
+    "cugmres_set_operator_green", "cugmres_green_block_device",
 )
 
 PHASES = ("matvec", "dots", "axpy", "small", "update", "residual", "precond")
@@ -99,6 +100,8 @@ class CgSystem(ctypes.Structure):
         ("chi_scale", ctypes.c_double),
         ("b", ctypes.c_void_p),
         ("x", ctypes.c_void_p),
+        ("k0", ctypes.c_double),
+        ("h", ctypes.c_double),
     ]
 
 
@@ -142,6 +145,8 @@ def _declare(L):
     L.cugmres_green_block.argtypes = [I, I, D, D, P]
     L.cugmres_set_operator.argtypes = [P, I, P, P, D]
     L.cugmres_set_operator_circulant.argtypes = [P, I, P, P, D]
+    L.cugmres_set_operator_green.argtypes = [P, I, I, D, D, P, D]
+    L.cugmres_green_block_device.argtypes = [I, I, D, D, P, P]
     L.cugmres_grid_size.argtypes = [P, ctypes.POINTER(I), ctypes.POINTER(I)]
     L.cugmres_matvec.argtypes = [P, P, P, I]
     L.cugmres_matvec_transpose.argtypes = [P, P, P, I]

@@ -741,6 +741,36 @@ int cugmres_set_operator(cg_ctx *c, int N, const cg_c128 *g_block, const double 
     return CG_OK;
 }
 
+static int green_args_ok(int kind, int N, double k0, double h) {
+    if (N < 1) return 0;
+    if (kind == CG_GREEN_REFERENCE) return 1;
+    if (kind == CG_GREEN_PYGMRES) return k0 > 0.0 && isfinite(k0);
+    if (kind == CG_GREEN_HELMHOLTZ) return k0 > 0.0 && h > 0.0 && isfinite(k0) && isfinite(h);
+    return 0;
+}
+
+int cugmres_green_block_device(int kind, int N, double k0, double h, cg_c128 *out, void *stream) {
+    if (!out || !green_args_ok(kind, N, k0, h)) return CG_ERR_INVALID;
+    if (!is_device_ptr(out)) return CG_ERR_INVALID;
+    int dev = 0, sms = 148;
+    CG_CU(cudaGetDevice(&dev));
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    CG_LAUNCH(launch_green_block(kind, N, k0, h, (double2 *)out, sms, (cudaStream_t)stream));
+    return CG_OK;
+}
+
+int cugmres_set_operator_green(cg_ctx *c, int kind, int N, double k0, double h, const double *chi, double chi_scale) {
+    if (!c || !chi || !green_args_ok(kind, N, k0, h) || !isfinite(chi_scale)) return CG_ERR_INVALID;
+    CG_CU(cudaSetDevice(c->device));
+    double2 *g = nullptr;
+    CG_CU(cudaMalloc((void **)&g, sizeof(double2) * (size_t)N * N));
+    int st = launch_green_block(kind, N, k0, h, g, c->sms, c->stream) ? CG_ERR_CUDA : CG_OK;
+    if (st == CG_OK) st = cugmres_set_operator(c, N, (const cg_c128 *)g, chi, chi_scale);
+    cudaStreamSynchronize(c->stream);
+    cudaFree(g);
+    return st;
+}
+
 int cugmres_set_operator_circulant(cg_ctx *c, int N, const cg_c64 *g_prep, const double *chi, double chi_scale) {
     if (!c || !g_prep || N < 1) return CG_ERR_INVALID;
     const int M = 2 * N - 1;

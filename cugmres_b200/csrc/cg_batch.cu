@@ -32,7 +32,9 @@ extern "C" int cugmres_solve_batch(int device, int nsys, const cg_system *sys, c
                                    cg_result *results) {
     if (nsys < 0 || (nsys > 0 && (!sys || !results)) || nworkers < 1) return CG_ERR_INVALID;
     for (int i = 0; i < nsys; i++)
-        if (sys[i].N < 1 || !sys[i].g_block || !sys[i].chi || !sys[i].b || !sys[i].x) return CG_ERR_INVALID;
+        if (sys[i].N < 1 || !sys[i].chi || !sys[i].b || !sys[i].x ||
+            (!sys[i].g_block && !(sys[i].k0 > 0.0 && sys[i].h > 0.0)))
+            return CG_ERR_INVALID;
     std::vector<int> order(nsys);
     for (int i = 0; i < nsys; i++) order[i] = i;
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return sys[a].N > sys[b].N; });
@@ -53,7 +55,8 @@ extern "C" int cugmres_solve_batch(int device, int nsys, const cg_system *sys, c
             const cg_system &s = sys[i];
             const double t0 = now_s();
             cg_result r = {};
-            st = cugmres_set_operator(ctx, s.N, s.g_block, s.chi, s.chi_scale);
+            st = s.g_block ? cugmres_set_operator(ctx, s.N, s.g_block, s.chi, s.chi_scale)
+                           : cugmres_set_operator_green(ctx, CG_GREEN_HELMHOLTZ, s.N, s.k0, s.h, s.chi, s.chi_scale);
             if (st == CG_OK) st = cugmres_solve(ctx, s.b, s.x, opts, nullptr, 0, &r);
             r.status = st;
             r.seconds = now_s() - t0;

@@ -93,6 +93,8 @@ int matvec_variants(int L);
 
 // full (unpruned) forward 2D transform of an L x L FP64 array, used to build the spectrum
 int launch_fft2d_full_fp64(int L, double2 *a, const double2 *tw, cudaStream_t s);
+// Green's-function block g[d1*N + d2] of `kind` (CG_GREEN_*) on the device.
+int launch_green_block(int kind, int N, double k0, double h, double2 *out, int sms, cudaStream_t s);
 
 // kernel launchers (cg_krylov.cu)
 int launch_dots(int prec_v, const void *V, long long n, const KrylovPtrs &kp, VecSel w, double2 *out, int ctr,

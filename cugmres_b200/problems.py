@@ -74,7 +74,8 @@ def gaussian_field(N, seed, corr=4.0):
     return np.real(np.fft.ifft2(np.fft.fft2(w) * filt))
 
 
-def sweep(nsys=256, seed=0, sides=(96, 128, 192, 256, 384, 512), lam_over_h=(15.0, 30.0), eps_range=(2.0, 12.0)):
+def sweep(nsys=256, seed=0, sides=(96, 128, 192, 256, 384, 512), lam_over_h=(15.0, 30.0), eps_range=(2.0, 12.0),
+          with_green=True):
     """Seeded sweep of independent systems: grid side drawn from `sides`,
     wavelength / cell size uniform in `lam_over_h`, eps_r uniform in
     `eps_range`, one design seed each (the same field construction)."""
@@ -84,11 +85,14 @@ def sweep(nsys=256, seed=0, sides=(96, 128, 192, 256, 384, 512), lam_over_h=(15.
         N = int(rng.choice(sides))
         lh = float(rng.uniform(*lam_over_h))
         eps = float(rng.uniform(*eps_range))
-        out.append(helmholtz(N, eps, seed=int(rng.integers(1 << 30)), cells_per_wavelength=lh))
+        out.append(helmholtz(N, eps, seed=int(rng.integers(1 << 30)), cells_per_wavelength=lh,
+                             with_green=with_green))
     return out
 
 
-def helmholtz(N, eps_r, seed=0, cells_per_wavelength=20.0, wavelength=1.0, corr=4.0, fill=0.75):
+def helmholtz(N, eps_r, seed=0, cells_per_wavelength=20.0, wavelength=1.0, corr=4.0, fill=0.75, with_green=True):
+    """with_green=False leaves out the host-built g_block (Solver.set_operator_green
+    and solve_batch build it on the GPU from k0 and h)."""
     k0 = 2.0 * np.pi / wavelength
     h = wavelength / cells_per_wavelength
     fld = gaussian_field(N, seed, corr)
@@ -98,5 +102,7 @@ def helmholtz(N, eps_r, seed=0, cells_per_wavelength=20.0, wavelength=1.0, corr=
     chi = np.where(inside & (fld > 0), float(eps_r) - 1.0, 0.0)
     x = (np.arange(N) + 0.5) * h
     b = np.repeat(np.exp(1j * k0 * x)[:, None], N, axis=1)
-    return dict(N=N, k0=k0, h=h, eps_r=float(eps_r), seed=seed, chi=chi, chi_scale=k0 * k0,
-                g_block=green_block("helmholtz", N, k0, h), b=b)
+    out = dict(N=N, k0=k0, h=h, eps_r=float(eps_r), seed=seed, chi=chi, chi_scale=k0 * k0, b=b)
+    if with_green:
+        out["g_block"] = green_block("helmholtz", N, k0, h)
+    return out

@@ -134,6 +134,13 @@ int cugmres_green_block(int kind, int N, double k0, double h, cg_c128 *out);
  * Builds the L x L circulant spectrum (L = smallest power of two >= 2N-1) on
  * the GPU in FP64 and keeps FP64 and FP32 copies of its even quarter. */
 int cugmres_set_operator(cg_ctx *ctx, int N, const cg_c128 *g_block, const double *chi, double chi_scale);
+/* The whole set-up on the GPU: the Green's block of `kind` (CG_GREEN_*, same
+ * formulas as cugmres_green_block, evaluated with CUDA's double-precision
+ * Bessel functions), embedding and spectrum; only chi is read from the host. */
+int cugmres_set_operator_green(cg_ctx *ctx, int kind, int N, double k0, double h, const double *chi,
+                               double chi_scale);
+/* The Green's block into device memory `out` (N*N cg_c128) on `stream`. */
+int cugmres_green_block_device(int kind, int N, double k0, double h, cg_c128 *out, void *stream);
 /* Same from the reference's spatial (2N-1) x (2N-1) circulant G_prep
  * (CUDA_GMRES/Release/input/G_prep_N.txt layout, row-major, complex64);
  * its first N x N block is the g_block. */
@@ -166,11 +173,13 @@ int cugmres_solve(cg_ctx *ctx, const cg_c128 *b, cg_c128 *x, const cg_opts *opts
 /* One independent system of a batched sweep (pointers host or device). */
 typedef struct {
     int N;
-    const cg_c128 *g_block; /* N x N Green's block (cugmres_green_block)  */
+    const cg_c128 *g_block; /* N x N Green's block (cugmres_green_block), or NULL:
+                               the GFIEM block of k0, h built on the GPU      */
     const double *chi;      /* N x N contrast                              */
     double chi_scale;       /* A = I - G diag(chi_scale * chi)             */
     const cg_c128 *b;       /* right-hand side                             */
     cg_c128 *x;             /* x0 on entry (unless opts->zero_x0), solution */
+    double k0, h;           /* wavenumber and cell size (used when g_block is NULL) */
 } cg_system;
 
 /* Solves nsys independent systems (any mix of grid sizes) on `device` with
