@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and 256^2 side measurements")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner side measurement")
     ap.add_argument("--learned-steps", type=int, default=1500)
+    ap.add_argument("--sweep", type=int, default=0, help="also solve a sweep of this many systems (config 4)")
+    ap.add_argument("--sweep-max-iter", type=int, default=3000)
     return ap.parse_args()
 
 
@@ -248,6 +250,28 @@ def learned_side(args, stream):
     return out
 
 
+def sweep_side(args):
+    """Config 4: independent systems with sides drawn from {96,...,512}, lambda/h
+    ~ U(15, 30), eps_r ~ U(2, 12), one design seed each, solved by
+    cugmres_solve_batch (operators built on the GPU, 8 worker contexts),
+    GMRES(200) to 1e-10 within --sweep-max-iter steps.  Wall time of the whole
+    batch call; per-system latency = set-up + solve."""
+    import cugmres_b200 as cg
+    from cugmres_b200 import problems as P
+    systems = P.sweep(nsys=args.sweep, seed=0, with_green=False)
+    cg.solve_batch(systems[:4], workers=4, restart=200, max_iter=50, tol=args.tol)  # contexts, autotuner cache
+    t0 = time.perf_counter()
+    xs, infos = cg.solve_batch(systems, workers=8, restart=200, max_iter=args.sweep_max_iter, tol=args.tol)
+    wall = time.perf_counter() - t0
+    lat = np.array([i["seconds"] for i in infos])
+    conv = [i for i in infos if i["status"] == 0]
+    return {"systems": len(infos), "converged": len(conv), "wall_s": wall, "solves_per_s": len(infos) / wall,
+            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
+            "arnoldi_steps": int(sum(i["iterations"] for i in infos)),
+            "matvecs_per_s": float(sum(i["iterations"] + i["cycles"] for i in infos) / wall),
+            "note": f"GMRES(200), tol {args.tol:g}, at most {args.sweep_max_iter} steps per system"}
+
+
 def run_reference(args, rank, world):
     """The reference's CPU GMRES (oracle port: MKL absent) on the host cores."""
     if rank != 0:
@@ -300,7 +324,6 @@ def main():
 
     clocks = Clocks(local)
     clocks.start()
-    s.profile(True)
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
@@ -308,9 +331,14 @@ def main():
     if world > 1:
         dist.barrier()
     ms_total = ms_one * args.steps
+    clk = clocks.stop()
+    # phase breakdown from one more solve with CUDA events between kernel groups (not timed;
+    # events disable the graph replay)
+    s.profile(True)
+    s.solve(b_dev, **kw)
+    torch.cuda.synchronize()
     prof = s.profile_read()
     s.profile(False)
-    clk = clocks.stop()
 
     # end to end through the public API from pinned host memory
     b_host = torch.from_numpy(pr["b"]).pin_memory()
@@ -335,8 +363,17 @@ def main():
     phases = {k: v for k, v in prof.items() if v["ms"] > 0}
     dom = max(phases.items(), key=lambda kv: kv[1]["ms"])
     tot_ms = sum(v["ms"] for v in phases.values())
+    # DRAM traffic per launch of the dominant kernel: ncu (dram__bytes_read.sum + dram__bytes_write.sum)
+    # of one launch at step k = 30 of the 1024^2 FP64 solve, as a ratio to that launch's algorithmic
+    # bytes, applied to this run's mean algorithmic bytes per launch (profiles/dcgs2_passes_1024x1024_k30.md)
+    ncu_ratio = {"dots": (536.909 + 4.744) / 536.871, "axpy": (536.917 + 7.709) / 570.425}
+    launches = max(1, dom[1].get("launches", 0))
+    alg_per_launch = dom[1].get("bytes", 0.0) / launches
+    traffic = ncu_ratio[dom[0]] * alg_per_launch if dom[0] in ncu_ratio and alg_per_launch > 0 else None
     roof = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1]["gbs"], 1), "peak": hbm, "unit": "GB/s",
-            "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind, "traffic": None,
+            "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind,
+            "traffic": round(traffic) if traffic else None, "traffic_unit": "bytes/launch",
+            "algorithmic_bytes_per_launch": round(alg_per_launch),
             "phases": {k: {"share": round(v["ms"] / tot_ms, 4), "gbs": round(v["gbs"], 1),
                            "ms": round(v["ms"], 3)} for k, v in phases.items()}}
     mv = prof.get("matvec", {})
@@ -365,6 +402,8 @@ def main():
         line["side"] = side_measurements(args, stream)
         if not args.no_learned:
             line["side"]["learned"] = learned_side(args, stream)
+    if rank == 0 and world == 1 and args.sweep > 0:
+        line.setdefault("side", {})["sweep"] = sweep_side(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, pr, last["iterations"])
     if rank == 0:

@@ -937,7 +937,13 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     int status = CG_OK;
 
     int prec_cycles = 0, x0_learned = 0;
-    double cycle_start_res = -1.0;  // true residual at the start of the last preconditioned cycle
+    // Preconditioner policy: the first cycle runs preconditioned, the second plain;
+    // afterwards each cycle uses the mode whose last cycle cut the true residual
+    // faster per second (log reduction / wall time); a preconditioned cycle that
+    // does not reduce it at all switches to plain GMRES for the rest of the solve.
+    double rate_prec = -1.0, rate_plain = -1.0;  // < 0: not measured yet
+    bool cycle_open = false, last_prec = false, prec_failed = false;
+    double cycle_t0 = 0.0, cycle_res0 = 0.0;
     if (learned && o.learned_x0 && o.zero_x0) {
         // initial guess x0 = M(b) (FP64 application); kept only if it lowers the residual
         CG_TRY(fno::apply(c->net, s, c->N, 0, bp, c->chi32, (float)c->k0h, xp, nullptr));
@@ -1074,17 +1080,34 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             CG_TRY(enqueue_begin(s));
             continue;
         }
-        if (use_prec && cycle_start_res >= 0.0 && !(hs.true_res < 0.9 * cycle_start_res)) use_prec = false;
+        if (learned && cycle_open) {
+            const double dt = now_s() - cycle_t0;
+            const double red = (cycle_res0 > 0.0 && hs.true_res > 0.0) ? log(cycle_res0 / hs.true_res) : 0.0;
+            const double rate = dt > 0.0 ? red / dt : 0.0;
+            if (last_prec) {
+                rate_prec = rate;
+                if (!(red > 0.0)) prec_failed = true;
+            } else {
+                rate_plain = rate;
+            }
+        }
+        if (learned) {
+            if (prec_failed) use_prec = false;
+            else if (rate_prec < 0.0) use_prec = true;
+            else if (rate_plain < 0.0) use_prec = false;
+            else use_prec = rate_prec > rate_plain;
+        }
         if (hs.status != 0) break;
         if (o.timeout_s > 0.0 && now_s() - t0 > o.timeout_s) {
             status = CG_ERR_TIMEOUT;
             break;
         }
         CG_TRY(prof_mark(c, cp, -1, -1, s));
-        if (use_prec) {
-            cycle_start_res = hs.true_res;
-            prec_cycles++;
-        }
+        if (use_prec) prec_cycles++;
+        cycle_open = true;
+        last_prec = use_prec;
+        cycle_t0 = now_s();
+        cycle_res0 = hs.true_res;
         if (graphs) {
             CG_TRY(launch_cycle_graph());
         } else {

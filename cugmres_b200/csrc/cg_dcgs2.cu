@@ -82,7 +82,7 @@ static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
 // D2_WARPS * cs * 4 doubles (at most 64 KB) whatever the restart length.
 static constexpr int D2T_CHUNK = 256;
 template <typename CV, int U>
-__global__ void __launch_bounds__(D2_THREADS) k_dots2t(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -484,6 +484,97 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
 // --------------------------------------------------------------- axpy2
 // q_k = cu u - sum_j P_j q_j into V[k];  u_{k+1} = cw w + du u - sum_j S_j q_j into V[k+1]
 // (k = st->k - 1: the step kernel has advanced the index).
+// Shared prologue of the axpy passes: P, S coefficients into shared memory
+// and t_k = ([c; delta] - H(0:k, 0:k-1) a) / nu (one warp per row of H).
+template <typename CV>
+__device__ __forceinline__ void axpy2_prologue(const KrylovPtrs &kp, const DevState *st, int k, CV *Pc, CV *Sc) {
+    typedef typename real_of<CV>::type R;
+    for (int j = threadIdx.x; j < k; j += blockDim.x) {
+        const double2 p = kp.P[j], q = kp.S[j];
+        Pc[j] = mk<CV>((R)p.x, (R)p.y);
+        Sc[j] = mk<CV>((R)q.x, (R)q.y);
+    }
+    const int ld = kp.mcap + 1;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const double inu = st->cu;
+    for (int i = blockIdx.x * (AX2_THREADS / 32) + warp; i <= k; i += gridDim.x * (AX2_THREADS / 32)) {
+        double er = 0.0, ei = 0.0;
+        for (int j = (i > 0 ? i - 1 : 0) + lane; j < k; j += 32) {
+            const double2 h = kp.Hm[(size_t)i * ld + j];
+            const double2 a = kp.D1[j];
+            er += h.x * a.x - h.y * a.y;
+            ei += h.x * a.y + h.y * a.x;
+        }
+        er = warp_sum(er);
+        ei = warp_sum(ei);
+        if (lane == 0) {
+            const double2 c = i < k ? kp.D2[i] : st->delta;
+            kp.tv[i] = make_double2((c.x - er) * inu, (c.y - ei) * inu);
+        }
+    }
+    __syncthreads();
+}
+
+// Tile-major axpy pass: each warp owns tiles of 32*U elements and streams the
+// basis vectors over the tile with the next vector's tile in flight while
+// the current one is accumulated into both outputs.
+template <typename CV, int U>
+__global__ void __launch_bounds__(AX2_THREADS, 2) k_axpy2t(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    typedef typename real_of<CV>::type R;
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k - 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    CV *Pc = reinterpret_cast<CV *>(smraw);
+    CV *Sc = Pc + (kp.mcap + 1);
+    axpy2_prologue<CV>(kp, st, k, Pc, Sc);
+    const R cu = (R)st->cu, cw = (R)st->cw;
+    const CV du = mk<CV>((R)st->du.x, (R)st->du.y);
+    CV *u = V + (long long)k * n;
+    CV *w = V + (long long)(k + 1) * n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long TILE = 32LL * U;
+    const long long ntile = (n + TILE - 1) / TILE;
+    const long long nw = (long long)gridDim.x * (AX2_THREADS / 32);
+    for (long long tile = (long long)blockIdx.x * (AX2_THREADS / 32) + warp; tile < ntile; tile += nw) {
+        const long long e0 = tile * TILE + lane;
+        const bool full = tile * TILE + TILE <= n;
+        CV sp[U], ss[U], a[U];
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            sp[t] = czero<CV>();
+            ss[t] = czero<CV>();
+            const long long e = e0 + 32 * t;
+            a[t] = (k > 0 && (full || e < n)) ? __ldcs(V + e) : czero<CV>();
+        }
+        for (int j = 0; j < k; j++) {
+            const CV p = Pc[j], q = Sc[j];
+            CV nx[U];
+            const bool more = j + 1 < k;
+#pragma unroll
+            for (int t = 0; t < U; t++) {
+                const long long e = e0 + 32 * t;
+                nx[t] = (more && (full || e < n)) ? __ldcs(V + (long long)(j + 1) * n + e) : czero<CV>();
+            }
+#pragma unroll
+            for (int t = 0; t < U; t++) {
+                sp[t] = cadd(sp[t], cmul(p, a[t]));
+                ss[t] = cadd(ss[t], cmul(q, a[t]));
+                a[t] = nx[t];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            const long long e = e0 + 32 * t;
+            if (full || e < n) {
+                const CV uu = u[e], ww = w[e];
+                u[e] = csub(cscale(uu, cu), sp[t]);
+                w[e] = csub(cadd(cscale(ww, cw), cmul(du, uu)), ss[t]);
+            }
+        }
+    }
+}
+
 template <typename CV, int JU>
 __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
@@ -493,35 +584,9 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
     extern __shared__ __align__(16) unsigned char smraw[];
     CV *Pc = reinterpret_cast<CV *>(smraw);
     CV *Sc = Pc + (kp.mcap + 1);
-    for (int j = threadIdx.x; j < k; j += blockDim.x) {
-        const double2 p = kp.P[j], q = kp.S[j];
-        Pc[j] = mk<CV>((R)p.x, (R)p.y);
-        Sc[j] = mk<CV>((R)q.x, (R)q.y);
-    }
+    axpy2_prologue<CV>(kp, st, k, Pc, Sc);
     const R cu = (R)st->cu, cw = (R)st->cw;
     const CV du = mk<CV>((R)st->du.x, (R)st->du.y);
-    {
-        // t_k = ([c; delta] - H(0:k, 0:k-1) a) / nu, one warp per row of H
-        const int ld = kp.mcap + 1;
-        const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-        const double inu = st->cu;
-        for (int i = blockIdx.x * (AX2_THREADS / 32) + warp; i <= k; i += gridDim.x * (AX2_THREADS / 32)) {
-            double er = 0.0, ei = 0.0;
-            for (int j = (i > 0 ? i - 1 : 0) + lane; j < k; j += 32) {
-                const double2 h = kp.Hm[(size_t)i * ld + j];
-                const double2 a = kp.D1[j];
-                er += h.x * a.x - h.y * a.y;
-                ei += h.x * a.y + h.y * a.x;
-            }
-            er = warp_sum(er);
-            ei = warp_sum(ei);
-            if (lane == 0) {
-                const double2 c = i < k ? kp.D2[i] : st->delta;
-                kp.tv[i] = make_double2((c.x - er) * inu, (c.y - ei) * inu);
-            }
-        }
-    }
-    __syncthreads();
     CV *u = V + (long long)k * n;
     CV *w = V + (long long)(k + 1) * n;
     const long long stride = (long long)gridDim.x * blockDim.x;
@@ -569,7 +634,7 @@ static int dots2_shape(int) {
     return v >= 0 ? v : 6;
 }
 static int axpy2_shape(int prec_v) {
-    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 3);
+    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 5);
     return v >= 0 ? v : (prec_v == 0 ? 0 : 2);
 }
 
@@ -593,6 +658,8 @@ template <typename CV> struct Axpy2Table {
         switch (v) {
             case 1: return k_axpy2<CV, 2>;
             case 2: return k_axpy2<CV, 8>;
+            case 3: return k_axpy2t<CV, 4>;
+            case 4: return k_axpy2t<CV, 8>;
             default: return k_axpy2<CV, 4>;
         }
     }

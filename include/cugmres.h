@@ -98,9 +98,11 @@ typedef struct {
 /* right preconditioning */
 enum {
     CG_PRECOND_NONE = 0,    /* plain GMRES                                                     */
-    CG_PRECOND_LEARNED = 1  /* flexible GMRES with the attached spectral-convolution network;
-                               a cycle that fails to reduce the true residual switches the
-                               rest of the solve to plain GMRES                                */
+    CG_PRECOND_LEARNED = 1  /* flexible GMRES with the attached spectral-convolution network:
+                               the first cycle runs preconditioned, the second plain, then
+                               each cycle uses the mode that cut the true residual faster
+                               per second; a preconditioned cycle that does not reduce it
+                               switches the rest of the solve to plain GMRES               */
 };
 
 typedef struct {
