@@ -615,14 +615,17 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 }
 
 // ------------------------------------------------------------- launchers
-// Shapes of the two streaming passes: the dot pass's variant (0-4: (J, U) of
-// k_dots2; 5, 6: tile-major k_dots2t with U = 4, 8) and the j-unroll of
-// k_axpy2, per precision.  Measured on B200 at N = 1024, restart 100 (300
-// steps, k = 0..99): FP64 dots 91.6 ms (shape 0), 81.0 (4), 61.4 (5), 54.2 ms
-// (6, 4.9 TB/s); FP32 97.6, 78.8 (1), 58.7 (5), 42.9 ms (6).  Shape 6 is the
-// default for both precisions.  FP64
-// axpy unroll 4, FP32 unroll 8 (36.4 ms vs 43.2 ms).  CUGMRES_DOTS2_SHAPE /
-// CUGMRES_AXPY2_SHAPE override both precisions (diagnostics).
+// Shapes of the two streaming passes.  Dot pass: 0-4 = (J, U) of the
+// group-major k_dots2, 5, 6 = tile-major k_dots2t with U = 4, 8.  Axpy pass:
+// 0-2 = j-unroll 4, 2, 8 of the element-major k_axpy2, 3, 4 = tile-major
+// k_axpy2t with U = 4, 8.  Measured on B200 at N = 1024, restart 100 (300
+// steps, k = 0..99), ms per 300 steps (HBM rate of the algorithmic bytes):
+//   FP64 dots: 91.6 (shape 0), 81.0 (4), 59.4 (5), 54.3 (6, 4.9 TB/s)
+//   FP32 dots: 97.6 (0), 78.8 (1), 50.0 (5), 38.3 (6)
+//   FP64 axpy: 64.4 (0), 45.7 (3), 42.0 (4, 6.5 TB/s)
+//   FP32 axpy: 35.5 (2), 34.6 (3), 24.8 (4)
+// Shapes 6 and 4 are the defaults for both precisions.  CUGMRES_DOTS2_SHAPE /
+// CUGMRES_AXPY2_SHAPE override them (diagnostics).
 static int env_shape(const char *name, int nshapes) {
     const char *e = getenv(name);
     if (!e || !*e) return -1;
@@ -633,9 +636,9 @@ static int dots2_shape(int) {
     static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 7);
     return v >= 0 ? v : 6;
 }
-static int axpy2_shape(int prec_v) {
+static int axpy2_shape(int) {
     static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 5);
-    return v >= 0 ? v : (prec_v == 0 ? 0 : 2);
+    return v >= 0 ? v : 4;
 }
 
 template <typename CV, bool COMP> struct Dots2Table {

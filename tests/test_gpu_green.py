@@ -47,6 +47,11 @@ def test_solve_with_device_operator(cuda_device):
 
 
 def test_batch_with_device_green(cuda_device):
-    systems = P.sweep(nsys=6, seed=4, sides=(96, 128), with_green=False)
-    xs, infos = cg.solve_batch(systems, workers=3, restart=100, max_iter=4000, tol=1e-10)
-    assert all(i["status"] == 0 and i["rel_residual_true"] <= 1e-10 for i in infos)
+    """Device-built operators give the same batch results as host-built blocks."""
+    systems = P.sweep(nsys=6, seed=4, sides=(96, 128), eps_range=(2.0, 4.0))
+    xa, ia = cg.solve_batch(systems, workers=3, restart=100, max_iter=4000, tol=1e-10)
+    xb, ib = cg.solve_batch(systems, workers=3, restart=100, max_iter=4000, tol=1e-10, device_green=True)
+    for a, b, x1, x2 in zip(ia, ib, xa, xb):
+        assert a["status"] == 0 and b["status"] == 0 and b["rel_residual_true"] <= 1e-10
+        assert abs(a["iterations"] - b["iterations"]) <= 1
+        assert np.linalg.norm(x1 - x2) / np.linalg.norm(x1) < 1e-8
