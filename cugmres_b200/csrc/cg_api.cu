@@ -260,7 +260,7 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
         CG_CU(cudaMalloc((void **)&c->kp.y, sizeof(double2) * mc));
         CG_CU(cudaMalloc((void **)&c->kp.hist, sizeof(double) * (ic + 1)));
         const size_t part_cgs2 = 2 * (size_t)dot_blocks(c) * (mc + 1);
-        const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms, mc), dots2_blocks(1, c->sms, mc)) *
+        const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) *
                                   (size_t)dots2_part_ld(mc);
         CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(part_cgs2, part_dcgs2)));
         CG_CU(cudaMalloc((void **)&c->kp.npart, sizeof(double) * np));
@@ -932,8 +932,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     VecSel zk = vk;  // Z_k (input of the flexible Arnoldi matvec)
     zk.base = c->Z;
     const int nrb = row_blocks(c);
-    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(prec, c->sms, c->mcap);
-    const int nax2 = axpy2_blocks(prec, c->sms, c->mcap);
+    const int ndot = dot_blocks(c), nax = axpy_blocks(c, n), ndot2 = dots2_blocks(prec, c->sms, c->mcap, n);
+    const int nax2 = axpy2_blocks(prec, c->sms, c->mcap, n);
     int status = CG_OK;
 
     int prec_cycles = 0, x0_learned = 0;
@@ -977,11 +977,11 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
                 CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, q));
                 CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, nullptr, nullptr, vk1, nullptr, c->st, GATE_STOP, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, i, q));
-                CG_LAUNCH(launch_dots2(prec, c->V, n, kp, ndot2, q));
+                CG_LAUNCH(launch_dots2(prec, c->V, n, kp, ndot2, c->sms, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, i, q));
                 CG_LAUNCH(launch_dcgs2_step(kp, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, i, q));
-                CG_LAUNCH(launch_axpy2(prec, c->V, n, kp, nax2, q));
+                CG_LAUNCH(launch_axpy2(prec, c->V, n, kp, nax2, c->sms, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, i, q));
                 continue;
             }

@@ -81,6 +81,21 @@ static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
 // D2T_CHUNK) vectors (u and w are re-read once per chunk), so shared memory is
 // D2_WARPS * cs * 4 doubles (at most 64 KB) whatever the restart length.
 static constexpr int D2T_CHUNK = 256;
+
+// Sum of four values over the warp with a reduce-scatter butterfly: 6
+// shuffles instead of 4 x 5.  On return lane 8*q holds the total of a_q
+// (q = 0..3); the summation order is fixed (deterministic).
+__device__ __forceinline__ double warp_sum4_scatter(double a0, double a1, double a2, double a3, int lane) {
+    const bool b4 = lane & 16, b3 = lane & 8;
+    const double s0 = b4 ? a0 : a2, s1 = b4 ? a1 : a3;
+    const double k0 = (b4 ? a2 : a0) + __shfl_xor_sync(0xffffffffu, s0, 16);
+    const double k1 = (b4 ? a3 : a1) + __shfl_xor_sync(0xffffffffu, s1, 16);
+    double m = (b3 ? k1 : k0) + __shfl_xor_sync(0xffffffffu, b3 ? k0 : k1, 8);
+    m += __shfl_xor_sync(0xffffffffu, m, 4);
+    m += __shfl_xor_sync(0xffffffffu, m, 2);
+    m += __shfl_xor_sync(0xffffffffu, m, 1);
+    return m;
+}
 template <typename CV, int U>
 __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
@@ -132,14 +147,8 @@ __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__
                         a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
                     }
                 }
-                const double d0 = warp_sum((double)s0), d1 = warp_sum((double)s1);
-                const double d2 = warp_sum((double)s2), d3 = warp_sum((double)s3);
-                if (lane == 0) {
-                    my[4 * j] += d0;
-                    my[4 * j + 1] += d1;
-                    my[4 * j + 2] += d2;
-                    my[4 * j + 3] += d3;
-                }
+                const double d = warp_sum4_scatter((double)s0, (double)s1, (double)s2, (double)s3, lane);
+                if ((lane & 7) == 0) my[4 * j + (lane >> 3)] += d;
             }
         }
         __syncthreads();
@@ -624,21 +633,31 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 //   FP32 dots: 97.6 (0), 78.8 (1), 50.0 (5), 38.3 (6)
 //   FP64 axpy: 64.4 (0), 45.7 (3), 42.0 (4, 6.5 TB/s)
 //   FP32 axpy: 35.5 (2), 34.6 (3), 24.8 (4)
-// Shapes 6 and 4 are the defaults for both precisions.  CUGMRES_DOTS2_SHAPE /
-// CUGMRES_AXPY2_SHAPE override them (diagnostics).
+// Shapes 6 and 4 are the defaults for large grids (tile_major below); smaller
+// grids use FP64 (4, 0) and FP32 (1, 2), which measured 0.86 s against 1.33 s
+// for shapes (6, 4) on the 256 x 256 unrestarted solve (1043 steps).
+// CUGMRES_DOTS2_SHAPE / CUGMRES_AXPY2_SHAPE override them (diagnostics).
 static int env_shape(const char *name, int nshapes) {
     const char *e = getenv(name);
     if (!e || !*e) return -1;
     const int v = atoi(e);
     return (v >= 0 && v < nshapes) ? v : -1;
 }
-static int dots2_shape(int) {
+// The tile-major passes give each warp 32 * 8 elements, so they need at least
+// as many tiles as the GPU holds resident warps (two 8-warp blocks per SM);
+// smaller grids (n < 606,208 on 148 SMs, i.e. N < 779) use the group-major
+// dot pass and the element-major axpy pass, which also spread the basis
+// vectors or single elements over the warps.
+static bool tile_major(long long n, int sms) { return n >= (long long)sms * 2 * (D2_THREADS / 32) * 32 * 8; }
+static int dots2_shape(int prec_v, long long n, int sms) {
     static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 7);
-    return v >= 0 ? v : 6;
+    if (v >= 0) return v;
+    return tile_major(n, sms) ? 6 : (prec_v == 0 ? 4 : 1);
 }
-static int axpy2_shape(int) {
+static int axpy2_shape(int prec_v, long long n, int sms) {
     static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 5);
-    return v >= 0 ? v : 4;
+    if (v >= 0) return v;
+    return tile_major(n, sms) ? 4 : (prec_v == 0 ? 0 : 2);
 }
 
 template <typename CV, bool COMP> struct Dots2Table {
@@ -674,25 +693,22 @@ static size_t dots2_smem(int v, int mcap) {
     const int jc = mcap + 1 < D2T_CHUNK ? mcap + 1 : D2T_CHUNK;
     return (v == 5 || v == 6) ? (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double) : 0;
 }
-static int dots2_shape_for(int prec_v, int mcap) {
-    (void)mcap;
-    return dots2_shape(prec_v);
-}
+
 template <typename CV, bool COMP> static typename Dots2Table<CV, COMP>::K dots2_kernel(int v, size_t smem) {
     typename Dots2Table<CV, COMP>::K kern = Dots2Table<CV, COMP>::get(v);
     if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     return kern;
 }
 
-int dots2_blocks(int prec_v, int sms, int mcap) {
-    const int v = dots2_shape_for(prec_v, mcap);
+int dots2_blocks(int prec_v, int sms, int mcap, long long n) {
+    const int v = dots2_shape(prec_v, n, sms);
     const size_t smem = dots2_smem(v, mcap);
     return prec_v == 0 ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
                        : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
 }
 
-int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s) {
-    const int v = dots2_shape_for(prec_v, kp.mcap);
+int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
+    const int v = dots2_shape(prec_v, n, sms);
     const size_t smem = dots2_smem(v, kp.mcap);
     if (prec_v == 0) dots2_kernel<double2, false>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const double2 *)V, n, kp);
     else dots2_kernel<float2, true>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const float2 *)V, n, kp);
@@ -710,29 +726,31 @@ int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s) {
     return (int)cudaGetLastError();
 }
 
-template <typename CV> static int axpy2_prepare(size_t smem) {
+template <typename CV> static int axpy2_prepare(int v, size_t smem) {
     if (smem > 48 * 1024)
-        return (int)cudaFuncSetAttribute(Axpy2Table<CV>::get(axpy2_shape(sizeof(CV) == sizeof(double2) ? 0 : 1)), cudaFuncAttributeMaxDynamicSharedMemorySize,
+        return (int)cudaFuncSetAttribute(Axpy2Table<CV>::get(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     return 0;
 }
 
-int axpy2_blocks(int prec_v, int sms, int mcap) {
+int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
     const size_t smem = 2 * (size_t)(mcap + 1) * (prec_v == 0 ? sizeof(double2) : sizeof(float2));
+    const int v = axpy2_shape(prec_v, n, sms);
     if (prec_v == 0) {
-        axpy2_prepare<double2>(smem);
-        return waves_grid(Axpy2Table<double2>::get(axpy2_shape(0)), AX2_THREADS, smem, sms);
+        axpy2_prepare<double2>(v, smem);
+        return waves_grid(Axpy2Table<double2>::get(v), AX2_THREADS, smem, sms);
     }
-    axpy2_prepare<float2>(smem);
-    return waves_grid(Axpy2Table<float2>::get(axpy2_shape(1)), AX2_THREADS, smem, sms);
+    axpy2_prepare<float2>(v, smem);
+    return waves_grid(Axpy2Table<float2>::get(v), AX2_THREADS, smem, sms);
 }
 
-int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s) {
+int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
     const size_t smem = 2 * (size_t)(kp.mcap + 1) * (prec_v == 0 ? sizeof(double2) : sizeof(float2));
-    int e = prec_v == 0 ? axpy2_prepare<double2>(smem) : axpy2_prepare<float2>(smem);
+    const int v = axpy2_shape(prec_v, n, sms);
+    int e = prec_v == 0 ? axpy2_prepare<double2>(v, smem) : axpy2_prepare<float2>(v, smem);
     if (e) return e;
-    if (prec_v == 0) Axpy2Table<double2>::get(axpy2_shape(0))<<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
-    else Axpy2Table<float2>::get(axpy2_shape(1))<<<nblk, AX2_THREADS, smem, s>>>((float2 *)V, n, kp);
+    if (prec_v == 0) Axpy2Table<double2>::get(v)<<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
+    else Axpy2Table<float2>::get(v)<<<nblk, AX2_THREADS, smem, s>>>((float2 *)V, n, kp);
     return (int)cudaGetLastError();
 }
 

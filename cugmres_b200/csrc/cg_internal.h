@@ -103,11 +103,11 @@ int launch_axpy(int prec_v, int prec_w, const void *V, long long n, const Krylov
                 double sign, int nj_mode, VecSel w, int want_norm, int ctr, int nblk, int gate, cudaStream_t s);
 int launch_givens(const KrylovPtrs &kp, cudaStream_t s);
 // delayed CGS2 step (cg_dcgs2.cu)
-int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
+int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s);
 int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s);
-int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, cudaStream_t s);
-int dots2_blocks(int prec_v, int sms, int mcap);
-int axpy2_blocks(int prec_v, int sms, int mcap);
+int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s);
+int dots2_blocks(int prec_v, int sms, int mcap, long long n);
+int axpy2_blocks(int prec_v, int sms, int mcap, long long n);
 // partials per block of the two-RHS dot pass
 __host__ __device__ inline int dots2_part_ld(int mcap) { return 2 * (mcap + 1) > 64 ? 2 * (mcap + 1) : 64; }
 int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s);
