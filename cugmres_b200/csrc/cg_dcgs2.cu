@@ -182,6 +182,93 @@ __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__
     }
 }
 
+// Split variant of the dot pass for grids with few tiles and many basis
+// vectors: a block owns a tile of 32*U elements at a time and its warps share
+// the basis (warp w takes q_j with j = w mod D2_WARPS), each warp keeping u and
+// w of the tile in registers.  Every coefficient j has one owning warp, so the
+// block accumulates it in a single shared-memory slot (chunks of cs vectors)
+// without atomics; block partials and the last-block sum as in k_dots2t.
+template <typename CV, int U>
+__global__ void __launch_bounds__(D2_THREADS) k_dots2s(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    typedef typename real_of<CV>::type R;
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int njt = k + 1;
+    const CV *u = V + (long long)k * n;
+    const CV *w = V + (long long)(k + 1) * n;
+    extern __shared__ double sacc[];  // [cs][4]
+    const int cs = kp.mcap + 1 < D2T_CHUNK ? kp.mcap + 1 : D2T_CHUNK;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pld = part_ld(kp);
+    const long long TILE = 32LL * U;
+    const long long ntile = (n + TILE - 1) / TILE;
+    for (int jc = 0; jc < njt; jc += cs) {
+        const int nj = njt - jc < cs ? njt - jc : cs;
+        const CV *Vc = V + (long long)jc * n;
+        for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) sacc[q] = 0.0;
+        __syncthreads();
+        for (long long tile = blockIdx.x; tile < ntile && warp < nj; tile += gridDim.x) {
+            const long long e0 = tile * TILE + lane;
+            const bool full = tile * TILE + TILE <= n;
+            CV uu[U], ww[U], a[U];
+            const CV *v0 = Vc + (long long)warp * n;
+#pragma unroll
+            for (int t = 0; t < U; t++) {
+                const long long e = e0 + 32 * t;
+                const bool ok = full || e < n;
+                uu[t] = ok ? u[e] : mk<CV>(0, 0);
+                ww[t] = ok ? w[e] : mk<CV>(0, 0);
+                a[t] = ok ? __ldcs(v0 + e) : mk<CV>(0, 0);
+            }
+            for (int j = warp; j < nj; j += D2_WARPS) {
+                R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    s0 += a[t].x * uu[t].x + a[t].y * uu[t].y;
+                    s1 += a[t].x * uu[t].y - a[t].y * uu[t].x;
+                    s2 += a[t].x * ww[t].x + a[t].y * ww[t].y;
+                    s3 += a[t].x * ww[t].y - a[t].y * ww[t].x;
+                }
+                if (j + D2_WARPS < nj) {  // this warp's next vector in flight during the reduction
+                    const CV *vn = Vc + (long long)(j + D2_WARPS) * n;
+#pragma unroll
+                    for (int t = 0; t < U; t++) {
+                        const long long e = e0 + 32 * t;
+                        a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
+                    }
+                }
+                const double d = warp_sum4_scatter((double)s0, (double)s1, (double)s2, (double)s3, lane);
+                if ((lane & 7) == 0) sacc[4 * j + (lane >> 3)] += d;
+            }
+        }
+        __syncthreads();
+        for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) kp.part[4 * ((size_t)blockIdx.x * pld + jc) + q] = sacc[q];
+        __syncthreads();
+    }
+    if (last_block2(&st->counter[3])) {
+        const int nparts = (int)gridDim.x;
+        for (int j = warp; j < njt; j += D2_WARPS) {
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            for (int b = lane; b < nparts; b += 32) {
+                const double *p = kp.part + 4 * ((size_t)b * pld + j);
+                s0 += __ldcg(p);
+                s1 += __ldcg(p + 1);
+                s2 += __ldcg(p + 2);
+                s3 += __ldcg(p + 3);
+            }
+            s0 = warp_sum(s0);
+            s1 = warp_sum(s1);
+            s2 = warp_sum(s2);
+            s3 = warp_sum(s3);
+            if (lane == 0) {
+                kp.D1[j] = make_double2(s0, s1);
+                kp.D2[j] = make_double2(s2, s3);
+            }
+        }
+    }
+}
+
 template <typename CV, bool COMP, int D2_J, int U>
 __global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     DevState *st = kp.st;
@@ -584,6 +671,82 @@ __global__ void __launch_bounds__(AX2_THREADS, 2) k_axpy2t(CV *__restrict__ V, l
     }
 }
 
+// Split variant of the axpy pass for grids with few tiles and many basis
+// vectors: a block owns a tile of 32*U elements at a time, its warps take the
+// basis vectors j = w mod warps and keep partial sums of both outputs in
+// registers; the partials meet in shared memory and are summed over the warps
+// in a fixed order by the threads that finish the tile's elements.
+// Shared memory: P, S coefficients (2 (mcap+1) elements) + 2 * warps * 32U elements.
+template <typename CV, int U>
+__global__ void __launch_bounds__(AX2_THREADS) k_axpy2s(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    typedef typename real_of<CV>::type R;
+    constexpr int W = AX2_THREADS / 32;
+    constexpr int TILE = 32 * U;
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k - 1;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    CV *Pc = reinterpret_cast<CV *>(smraw);
+    CV *Sc = Pc + (kp.mcap + 1);
+    CV *red = Sc + (kp.mcap + 1);  // [W][2][TILE]
+    axpy2_prologue<CV>(kp, st, k, Pc, Sc);
+    const R cu = (R)st->cu, cw = (R)st->cw;
+    const CV du = mk<CV>((R)st->du.x, (R)st->du.y);
+    CV *u = V + (long long)k * n;
+    CV *w = V + (long long)(k + 1) * n;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long ntile = (n + TILE - 1) / TILE;
+    for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+        const long long e0 = tile * TILE + lane;
+        const bool full = tile * TILE + TILE <= n;
+        CV sp[U], ss[U], a[U];
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            sp[t] = czero<CV>();
+            ss[t] = czero<CV>();
+            const long long e = e0 + 32 * t;
+            a[t] = (warp < k && (full || e < n)) ? __ldcs(V + (long long)warp * n + e) : czero<CV>();
+        }
+        for (int j = warp; j < k; j += W) {
+            const CV p = Pc[j], q = Sc[j];
+            CV nx[U];
+            const bool more = j + W < k;
+#pragma unroll
+            for (int t = 0; t < U; t++) {
+                const long long e = e0 + 32 * t;
+                nx[t] = (more && (full || e < n)) ? __ldcs(V + (long long)(j + W) * n + e) : czero<CV>();
+            }
+#pragma unroll
+            for (int t = 0; t < U; t++) {
+                sp[t] = cadd(sp[t], cmul(p, a[t]));
+                ss[t] = cadd(ss[t], cmul(q, a[t]));
+                a[t] = nx[t];
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < U; t++) {
+            red[(warp * 2) * TILE + lane + 32 * t] = sp[t];
+            red[(warp * 2 + 1) * TILE + lane + 32 * t] = ss[t];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < TILE; i += blockDim.x) {
+            const long long e = tile * TILE + i;
+            if (e < n) {
+                CV s1 = czero<CV>(), s2 = czero<CV>();
+#pragma unroll
+                for (int wq = 0; wq < W; wq++) {
+                    s1 = cadd(s1, red[(wq * 2) * TILE + i]);
+                    s2 = cadd(s2, red[(wq * 2 + 1) * TILE + i]);
+                }
+                const CV uu = u[e], ww = w[e];
+                u[e] = csub(cscale(uu, cu), s1);
+                w[e] = csub(cadd(cscale(ww, cw), cmul(du, uu)), s2);
+            }
+        }
+        __syncthreads();
+    }
+}
+
 template <typename CV, int JU>
 __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
@@ -650,14 +813,18 @@ static int env_shape(const char *name, int nshapes) {
 // vectors or single elements over the warps.
 static bool tile_major(long long n, int sms) { return n >= (long long)sms * 2 * (D2_THREADS / 32) * 32 * 8; }
 static int dots2_shape(int prec_v, long long n, int sms) {
-    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 7);
+    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 9);
     if (v >= 0) return v;
-    return tile_major(n, sms) ? 6 : (prec_v == 0 ? 4 : 1);
+    if (tile_major(n, sms)) return 6;
+    return (n + 255) / 256 >= sms ? 7 : 8;  // split, 8 or 2 elements per lane
+    (void)prec_v;
 }
 static int axpy2_shape(int prec_v, long long n, int sms) {
-    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 5);
+    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 7);
     if (v >= 0) return v;
-    return tile_major(n, sms) ? 4 : (prec_v == 0 ? 0 : 2);
+    if (tile_major(n, sms)) return 4;
+    return (n + 127) / 128 >= sms ? 5 : 6;  // split, 4 or 2 elements per lane
+    (void)prec_v;
 }
 
 template <typename CV, bool COMP> struct Dots2Table {
@@ -670,6 +837,8 @@ template <typename CV, bool COMP> struct Dots2Table {
             case 4: return k_dots2<CV, COMP, 2, 4>;
             case 5: return k_dots2t<CV, 4>;
             case 6: return k_dots2t<CV, 8>;
+            case 7: return k_dots2s<CV, 8>;
+            case 8: return k_dots2s<CV, 2>;
             default: return k_dots2<CV, COMP, 4, 2>;
         }
     }
@@ -682,16 +851,20 @@ template <typename CV> struct Axpy2Table {
             case 2: return k_axpy2<CV, 8>;
             case 3: return k_axpy2t<CV, 4>;
             case 4: return k_axpy2t<CV, 8>;
+            case 5: return k_axpy2s<CV, 4>;
+            case 6: return k_axpy2s<CV, 2>;
             default: return k_axpy2<CV, 4>;
         }
     }
 };
 
-// Shape actually used: the tile-major shapes need D2_WARPS * (mcap+1) * 32 bytes
-// of shared memory and fall back to shape 0 above 96 KB (restart > 383).
+// Dynamic shared memory of the dot-pass shapes: per-warp coefficient slots
+// (tile-major) or one slot per coefficient (split), for chunks of cs vectors.
 static size_t dots2_smem(int v, int mcap) {
     const int jc = mcap + 1 < D2T_CHUNK ? mcap + 1 : D2T_CHUNK;
-    return (v == 5 || v == 6) ? (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double) : 0;
+    if (v == 5 || v == 6) return (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double);
+    if (v == 7 || v == 8) return (size_t)jc * 4 * sizeof(double);
+    return 0;
 }
 
 template <typename CV, bool COMP> static typename Dots2Table<CV, COMP>::K dots2_kernel(int v, size_t smem) {
@@ -733,9 +906,18 @@ template <typename CV> static int axpy2_prepare(int v, size_t smem) {
     return 0;
 }
 
+// Dynamic shared memory of the axpy-pass shapes: P, S coefficients, plus the
+// per-warp partial sums of the split shapes.
+static size_t axpy2_smem(int v, int prec_v, int mcap) {
+    const size_t e = prec_v == 0 ? sizeof(double2) : sizeof(float2);
+    size_t b = 2 * (size_t)(mcap + 1) * e;
+    if (v == 5 || v == 6) b += 2 * (size_t)(AX2_THREADS / 32) * 32 * (v == 5 ? 4 : 2) * e;
+    return b;
+}
+
 int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
-    const size_t smem = 2 * (size_t)(mcap + 1) * (prec_v == 0 ? sizeof(double2) : sizeof(float2));
     const int v = axpy2_shape(prec_v, n, sms);
+    const size_t smem = axpy2_smem(v, prec_v, mcap);
     if (prec_v == 0) {
         axpy2_prepare<double2>(v, smem);
         return waves_grid(Axpy2Table<double2>::get(v), AX2_THREADS, smem, sms);
@@ -745,8 +927,8 @@ int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
 }
 
 int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
-    const size_t smem = 2 * (size_t)(kp.mcap + 1) * (prec_v == 0 ? sizeof(double2) : sizeof(float2));
     const int v = axpy2_shape(prec_v, n, sms);
+    const size_t smem = axpy2_smem(v, prec_v, kp.mcap);
     int e = prec_v == 0 ? axpy2_prepare<double2>(v, smem) : axpy2_prepare<float2>(v, smem);
     if (e) return e;
     if (prec_v == 0) Axpy2Table<double2>::get(v)<<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
