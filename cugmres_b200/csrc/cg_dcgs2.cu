@@ -788,17 +788,20 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 
 // ------------------------------------------------------------- launchers
 // Shapes of the two streaming passes.  Dot pass: 0-4 = (J, U) of the
-// group-major k_dots2, 5, 6 = tile-major k_dots2t with U = 4, 8.  Axpy pass:
-// 0-2 = j-unroll 4, 2, 8 of the element-major k_axpy2, 3, 4 = tile-major
-// k_axpy2t with U = 4, 8.  Measured on B200 at N = 1024, restart 100 (300
-// steps, k = 0..99), ms per 300 steps (HBM rate of the algorithmic bytes):
-//   FP64 dots: 91.6 (shape 0), 81.0 (4), 59.4 (5), 54.3 (6, 4.9 TB/s)
-//   FP32 dots: 97.6 (0), 78.8 (1), 50.0 (5), 38.3 (6)
-//   FP64 axpy: 64.4 (0), 45.7 (3), 42.0 (4, 6.5 TB/s)
-//   FP32 axpy: 35.5 (2), 34.6 (3), 24.8 (4)
-// Shapes 6 and 4 are the defaults for large grids (tile_major below); smaller
-// grids use FP64 (4, 0) and FP32 (1, 2), which measured 0.86 s against 1.33 s
-// for shapes (6, 4) on the 256 x 256 unrestarted solve (1043 steps).
+// group-major k_dots2, 5, 6 = tile-major k_dots2t with U = 4, 8, 7, 8 = split
+// k_dots2s with U = 8, 2.  Axpy pass: 0-2 = j-unroll 4, 2, 8 of the
+// element-major k_axpy2, 3, 4 = tile-major k_axpy2t with U = 4, 8, 5, 6 =
+// split k_axpy2s with U = 4, 2.  Measured on B200:
+//   N = 1024, restart 100 (300 steps, k = 0..99), ms per 300 steps:
+//     FP64 dots 91.6 (shape 0), 81.0 (4), 59.4 (5), 54.3 (6, 4.9 TB/s)
+//     FP32 dots 97.6 (0), 78.8 (1), 50.0 (5), 38.3 (6)
+//     FP64 axpy 64.4 (0), 45.7 (3), 42.0 (4, 6.5 TB/s); FP32 axpy 35.5 (2), 24.8 (4)
+//   whole solves, (dots, axpy) shapes (4, 0) / (7, 5) / (8, 6):
+//     256 x 256 unrestarted FP64 (1043 steps) 0.862 / 0.614 / 1.045 s
+//     256 x 256 unrestarted mixed 1.754 / 0.912 / 2.120 s
+//     96 x 96 GMRES(200) FP64 (180 steps) 30.6 / 18.9 / 27.9 ms
+//     512 x 512 GMRES(200) FP64 (1000 steps) 0.381 / 0.254 / 0.327 s
+// Defaults: (6, 4) on grids with tile_major(n), (7, 5) below.
 // CUGMRES_DOTS2_SHAPE / CUGMRES_AXPY2_SHAPE override them (diagnostics).
 static int env_shape(const char *name, int nshapes) {
     const char *e = getenv(name);
@@ -808,23 +811,18 @@ static int env_shape(const char *name, int nshapes) {
 }
 // The tile-major passes give each warp 32 * 8 elements, so they need at least
 // as many tiles as the GPU holds resident warps (two 8-warp blocks per SM);
-// smaller grids (n < 606,208 on 148 SMs, i.e. N < 779) use the group-major
-// dot pass and the element-major axpy pass, which also spread the basis
-// vectors or single elements over the warps.
+// smaller grids (n < 606,208 on 148 SMs, i.e. N < 779) use the split passes,
+// whose warps share the basis vectors of one tile.
 static bool tile_major(long long n, int sms) { return n >= (long long)sms * 2 * (D2_THREADS / 32) * 32 * 8; }
-static int dots2_shape(int prec_v, long long n, int sms) {
+static int dots2_shape(int, long long n, int sms) {
     static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 9);
     if (v >= 0) return v;
-    if (tile_major(n, sms)) return 6;
-    return (n + 255) / 256 >= sms ? 7 : 8;  // split, 8 or 2 elements per lane
-    (void)prec_v;
+    return tile_major(n, sms) ? 6 : 7;
 }
-static int axpy2_shape(int prec_v, long long n, int sms) {
+static int axpy2_shape(int, long long n, int sms) {
     static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 7);
     if (v >= 0) return v;
-    if (tile_major(n, sms)) return 4;
-    return (n + 127) / 128 >= sms ? 5 : 6;  // split, 4 or 2 elements per lane
-    (void)prec_v;
+    return tile_major(n, sms) ? 4 : 5;
 }
 
 template <typename CV, bool COMP> struct Dots2Table {
