@@ -809,11 +809,13 @@ static int env_shape(const char *name, int nshapes) {
     const int v = atoi(e);
     return (v >= 0 && v < nshapes) ? v : -1;
 }
-// The tile-major passes give each warp 32 * 8 elements, so they need at least
-// as many tiles as the GPU holds resident warps (two 8-warp blocks per SM);
-// smaller grids (n < 606,208 on 148 SMs, i.e. N < 779) use the split passes,
-// whose warps share the basis vectors of one tile.
-static bool tile_major(long long n, int sms) { return n >= (long long)sms * 2 * (D2_THREADS / 32) * 32 * 8; }
+// The tile-major passes give each warp 32 * 8 elements, so they need about as
+// many tiles as the GPU holds resident warps (two 8-warp blocks per SM; from
+// 3/4 of that on: n >= 454,656 on 148 SMs, N >= 675); smaller grids use the
+// split passes, whose warps share the basis vectors of one tile.  Measured
+// ms per step at restart 100, tile / split: 512^2 0.179 / 0.153, 768^2
+// 0.303 / 0.321, 1024^2 0.442 / 0.465.
+static bool tile_major(long long n, int sms) { return 4 * n >= 3LL * sms * 2 * (D2_THREADS / 32) * 32 * 8; }
 static int dots2_shape(int, long long n, int sms) {
     static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 9);
     if (v >= 0) return v;
@@ -871,11 +873,25 @@ template <typename CV, bool COMP> static typename Dots2Table<CV, COMP>::K dots2_
     return kern;
 }
 
+// Blocks with any work: a tile of 32*U elements per warp (tile-major) or per
+// block (split); more blocks would only add partial sums to reduce.
+static long long work_blocks(bool split, int U, long long n) {
+    const long long tiles = (n + 32LL * U - 1) / (32LL * U);
+    const long long b = split ? tiles : (tiles + D2_WARPS - 1) / D2_WARPS;
+    return b < 1 ? 1 : b;
+}
+
 int dots2_blocks(int prec_v, int sms, int mcap, long long n) {
     const int v = dots2_shape(prec_v, n, sms);
     const size_t smem = dots2_smem(v, mcap);
-    return prec_v == 0 ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
-                       : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
+    int g = prec_v == 0 ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
+                        : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
+    if (v >= 5 && v <= 8) {
+        const int U = (v == 5) ? 4 : (v == 8 ? 2 : 8);
+        const long long cap = work_blocks(v >= 7, U, n);
+        if (cap < g) g = (int)cap;
+    }
+    return g;
 }
 
 int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
@@ -916,12 +932,20 @@ static size_t axpy2_smem(int v, int prec_v, int mcap) {
 int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
     const int v = axpy2_shape(prec_v, n, sms);
     const size_t smem = axpy2_smem(v, prec_v, mcap);
+    int g;
     if (prec_v == 0) {
         axpy2_prepare<double2>(v, smem);
-        return waves_grid(Axpy2Table<double2>::get(v), AX2_THREADS, smem, sms);
+        g = waves_grid(Axpy2Table<double2>::get(v), AX2_THREADS, smem, sms);
+    } else {
+        axpy2_prepare<float2>(v, smem);
+        g = waves_grid(Axpy2Table<float2>::get(v), AX2_THREADS, smem, sms);
     }
-    axpy2_prepare<float2>(v, smem);
-    return waves_grid(Axpy2Table<float2>::get(v), AX2_THREADS, smem, sms);
+    if (v >= 3 && v <= 6) {
+        const int U = (v == 3 || v == 5) ? 4 : (v == 4 ? 8 : 2);
+        const long long cap = work_blocks(v >= 5, U, n);
+        if (cap < g) g = (int)cap;
+    }
+    return g;
 }
 
 int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
