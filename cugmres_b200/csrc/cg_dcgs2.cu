@@ -163,6 +163,7 @@ __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__
         const int nparts = (int)gridDim.x;
         for (int j = warp; j < njt; j += D2_WARPS) {
             double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll 4
             for (int b = lane; b < nparts; b += 32) {
                 const double *p = kp.part + 4 * ((size_t)b * pld + j);
                 s0 += __ldcg(p);
@@ -183,13 +184,11 @@ __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__
 }
 
 // Split variant of the dot pass for grids with few tiles and many basis
-// vectors.  Work items are (tile of 32*U elements, range of basis vectors):
-// the launch has ntile * nsplit blocks (nsplit = gridDim.x / ntile), block b
-// starts with item b, and its warps share the item's range (warp w takes
-// j = lo + w, lo + w + 8, ...), each keeping u and w of the tile in
-// registers.  Every (tile, j) is computed by exactly one warp, which writes
-// its four sums straight into row `tile` of the partials (no shared memory,
-// no barriers); the last block sums the ntile rows in a fixed order.
+// vectors: a block owns a tile of 32*U elements at a time and its warps share
+// the basis (warp w takes q_j with j = w mod D2_WARPS), each warp keeping u and
+// w of the tile in registers.  Every coefficient j has one owning warp, so the
+// block accumulates it in a single shared-memory slot (chunks of cs vectors)
+// without atomics; block partials and the last-block sum as in k_dots2t.
 template <typename CV, int U>
 __global__ void __launch_bounds__(D2_THREADS) k_dots2s(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
@@ -199,54 +198,60 @@ __global__ void __launch_bounds__(D2_THREADS) k_dots2s(const CV *__restrict__ V,
     const int njt = k + 1;
     const CV *u = V + (long long)k * n;
     const CV *w = V + (long long)(k + 1) * n;
+    extern __shared__ double sacc[];  // [cs][4]
+    const int cs = kp.mcap + 1 < D2T_CHUNK ? kp.mcap + 1 : D2T_CHUNK;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pld = part_ld(kp);
     const long long TILE = 32LL * U;
     const long long ntile = (n + TILE - 1) / TILE;
-    const int nsplit = gridDim.x >= ntile ? (int)(gridDim.x / ntile) : 1;
-    const long long nitems = ntile * nsplit;
-    for (long long item = blockIdx.x; item < nitems; item += gridDim.x) {
-        const long long tile = item / nsplit;
-        const int sidx = (int)(item % nsplit);
-        const int lo = (int)((long long)njt * sidx / nsplit), hi = (int)((long long)njt * (sidx + 1) / nsplit);
-        if (lo + warp >= hi) continue;
-        const long long e0 = tile * TILE + lane;
-        const bool full = tile * TILE + TILE <= n;
-        CV uu[U], ww[U], a[U];
-        const CV *v0 = V + (long long)(lo + warp) * n;
-#pragma unroll
-        for (int t = 0; t < U; t++) {
-            const long long e = e0 + 32 * t;
-            const bool ok = full || e < n;
-            uu[t] = ok ? u[e] : mk<CV>(0, 0);
-            ww[t] = ok ? w[e] : mk<CV>(0, 0);
-            a[t] = ok ? __ldcs(v0 + e) : mk<CV>(0, 0);
-        }
-        for (int j = lo + warp; j < hi; j += D2_WARPS) {
-            R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int jc = 0; jc < njt; jc += cs) {
+        const int nj = njt - jc < cs ? njt - jc : cs;
+        const CV *Vc = V + (long long)jc * n;
+        for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) sacc[q] = 0.0;
+        __syncthreads();
+        for (long long tile = blockIdx.x; tile < ntile && warp < nj; tile += gridDim.x) {
+            const long long e0 = tile * TILE + lane;
+            const bool full = tile * TILE + TILE <= n;
+            CV uu[U], ww[U], a[U];
+            const CV *v0 = Vc + (long long)warp * n;
 #pragma unroll
             for (int t = 0; t < U; t++) {
-                s0 += a[t].x * uu[t].x + a[t].y * uu[t].y;
-                s1 += a[t].x * uu[t].y - a[t].y * uu[t].x;
-                s2 += a[t].x * ww[t].x + a[t].y * ww[t].y;
-                s3 += a[t].x * ww[t].y - a[t].y * ww[t].x;
+                const long long e = e0 + 32 * t;
+                const bool ok = full || e < n;
+                uu[t] = ok ? u[e] : mk<CV>(0, 0);
+                ww[t] = ok ? w[e] : mk<CV>(0, 0);
+                a[t] = ok ? __ldcs(v0 + e) : mk<CV>(0, 0);
             }
-            if (j + D2_WARPS < hi) {  // this warp's next vector in flight during the reduction
-                const CV *vn = V + (long long)(j + D2_WARPS) * n;
+            for (int j = warp; j < nj; j += D2_WARPS) {
+                R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
                 for (int t = 0; t < U; t++) {
-                    const long long e = e0 + 32 * t;
-                    a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
+                    s0 += a[t].x * uu[t].x + a[t].y * uu[t].y;
+                    s1 += a[t].x * uu[t].y - a[t].y * uu[t].x;
+                    s2 += a[t].x * ww[t].x + a[t].y * ww[t].y;
+                    s3 += a[t].x * ww[t].y - a[t].y * ww[t].x;
                 }
+                if (j + D2_WARPS < nj) {  // this warp's next vector in flight during the reduction
+                    const CV *vn = Vc + (long long)(j + D2_WARPS) * n;
+#pragma unroll
+                    for (int t = 0; t < U; t++) {
+                        const long long e = e0 + 32 * t;
+                        a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
+                    }
+                }
+                const double d = warp_sum4_scatter((double)s0, (double)s1, (double)s2, (double)s3, lane);
+                if ((lane & 7) == 0) sacc[4 * j + (lane >> 3)] += d;
             }
-            const double d = warp_sum4_scatter((double)s0, (double)s1, (double)s2, (double)s3, lane);
-            if ((lane & 7) == 0) kp.part[4 * ((size_t)tile * pld + j) + (lane >> 3)] = d;
         }
+        __syncthreads();
+        for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) kp.part[4 * ((size_t)blockIdx.x * pld + jc) + q] = sacc[q];
+        __syncthreads();
     }
     if (last_block2(&st->counter[3])) {
-        const int nparts = (int)(ntile < gridDim.x ? ntile : gridDim.x);
+        const int nparts = (int)gridDim.x;
         for (int j = warp; j < njt; j += D2_WARPS) {
             double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll 4
             for (int b = lane; b < nparts; b += 32) {
                 const double *p = kp.part + 4 * ((size_t)b * pld + j);
                 s0 += __ldcg(p);
@@ -788,14 +793,14 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 // ------------------------------------------------------------- launchers
 // Shapes of the two streaming passes.  Dot pass: 0-4 = (J, U) of the
 // group-major k_dots2, 5, 6 = tile-major k_dots2t with U = 4, 8, 7, 8 = split
-// k_dots2s with U = 8, 2.  Axpy pass: 0-2 = j-unroll 4, 2, 8 of the
+// k_dots2s with U = 8, 4.  Axpy pass: 0-2 = j-unroll 4, 2, 8 of the
 // element-major k_axpy2, 3, 4 = tile-major k_axpy2t with U = 4, 8, 5, 6 =
 // split k_axpy2s with U = 4, 2.  Measured on B200:
 //   N = 1024, restart 100 (300 steps, k = 0..99), ms per 300 steps:
 //     FP64 dots 91.6 (shape 0), 81.0 (4), 59.4 (5), 54.3 (6, 4.9 TB/s)
 //     FP32 dots 97.6 (0), 78.8 (1), 50.0 (5), 38.3 (6)
 //     FP64 axpy 64.4 (0), 45.7 (3), 42.0 (4, 6.5 TB/s); FP32 axpy 35.5 (2), 24.8 (4)
-//   whole solves, (dots, axpy) shapes (4, 0) / (7, 5) / (8, 6):
+//   whole solves, (dots, axpy) shapes (4, 0) / (7, 5) / (split dots and axpy with U = 2):
 //     256 x 256 unrestarted FP64 (1043 steps) 0.862 / 0.614 / 1.045 s
 //     256 x 256 unrestarted mixed 1.754 / 0.912 / 2.120 s
 //     96 x 96 GMRES(200) FP64 (180 steps) 30.6 / 18.9 / 27.9 ms
@@ -837,7 +842,7 @@ template <typename CV, bool COMP> struct Dots2Table {
             case 5: return k_dots2t<CV, 4>;
             case 6: return k_dots2t<CV, 8>;
             case 7: return k_dots2s<CV, 8>;
-            case 8: return k_dots2s<CV, 2>;
+            case 8: return k_dots2s<CV, 4>;
             default: return k_dots2<CV, COMP, 4, 2>;
         }
     }
@@ -857,11 +862,12 @@ template <typename CV> struct Axpy2Table {
     }
 };
 
-// Dynamic shared memory of the dot-pass shapes: per-warp coefficient slots of
-// the tile-major shapes, for chunks of cs vectors.
+// Dynamic shared memory of the dot-pass shapes: per-warp coefficient slots
+// (tile-major) or one slot per coefficient (split), for chunks of cs vectors.
 static size_t dots2_smem(int v, int mcap) {
     const int jc = mcap + 1 < D2T_CHUNK ? mcap + 1 : D2T_CHUNK;
     if (v == 5 || v == 6) return (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double);
+    if (v == 7 || v == 8) return (size_t)jc * 4 * sizeof(double);
     return 0;
 }
 
@@ -884,14 +890,10 @@ int dots2_blocks(int prec_v, int sms, int mcap, long long n) {
     const size_t smem = dots2_smem(v, mcap);
     int g = prec_v == 0 ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
                         : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
-    if (v == 5 || v == 6) {  // tile-major: at most one block per 8 tiles
-        const long long cap = work_blocks(false, v == 5 ? 4 : 8, n);
+    if (v >= 5 && v <= 8) {
+        const int U = (v == 5 || v == 8) ? 4 : 8;
+        const long long cap = work_blocks(v >= 7, U, n);
         if (cap < g) g = (int)cap;
-    } else if (v == 7 || v == 8) {  // split: ntile * nsplit blocks, about four waves
-        const long long ntile = work_blocks(true, v == 7 ? 8 : 2, n);
-        long long nsplit = (4LL * g + ntile - 1) / ntile;
-        nsplit = nsplit < 1 ? 1 : (nsplit > 16 ? 16 : nsplit);
-        g = (int)(ntile * nsplit);
     }
     return g;
 }
