@@ -228,6 +228,8 @@ void free_krylov(cg_ctx *c) {
     dfree_t(c->kp.tv);
     dfree_t(c->kp.P);
     dfree_t(c->kp.S);
+    dfree_t(c->kp.gpart);
+    dfree_t(c->kp.tickets);
     dfree(c->Z);
     c->zcap_bytes = 0;
     c->mcap = 0;
@@ -263,6 +265,10 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
         const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) *
                                   (size_t)dots2_part_ld(mc);
         CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(part_cgs2, part_dcgs2)));
+        const size_t ngroups = ((size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) + 15) / 16;
+        CG_CU(cudaMalloc((void **)&c->kp.gpart, sizeof(double) * 4 * ngroups * (size_t)dots2_part_ld(mc)));
+        CG_CU(cudaMalloc((void **)&c->kp.tickets, sizeof(unsigned int) * ngroups));
+        CG_CU(cudaMemset(c->kp.tickets, 0, sizeof(unsigned int) * ngroups));
         CG_CU(cudaMalloc((void **)&c->kp.npart, sizeof(double) * np));
         CG_CU(cudaMalloc((void **)&c->kp.Hm, sizeof(double2) * (size_t)(mc + 1) * (mc + 1)));
         CG_CU(cudaMalloc((void **)&c->kp.D1, sizeof(double2) * (mc + 2)));

@@ -82,6 +82,47 @@ static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
 // D2_WARPS * cs * 4 doubles (at most 64 KB) whatever the restart length.
 static constexpr int D2T_CHUNK = 256;
 
+// Arrival counter over `count` blocks; the last to arrive resets it and
+// sees true (with the other blocks' writes visible).
+static __device__ __forceinline__ bool last_of(unsigned int *ticket, unsigned int count) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int t = atomicAdd(ticket, 1u);
+        is_last = (t == count - 1);
+        if (is_last) *ticket = 0u;
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// Two-level fixed-order sum of the per-block partial rows part[b][0 .. 4 njt)
+// into D1, D2: the last block of each group of 16 blocks sums its group's
+// rows into gpart[g], the last group sums the group rows.  Replaces one block
+// reading every row, which dominated the pass on grids of hundreds of blocks.
+constexpr int RGROUP = 16;
+static __device__ void dots2_finish(const KrylovPtrs &kp, DevState *st, int njt, int pld) {
+    const int nb = gridDim.x, ng = (nb + RGROUP - 1) / RGROUP;
+    const int g = blockIdx.x / RGROUP;
+    const int gsz = nb - g * RGROUP < RGROUP ? nb - g * RGROUP : RGROUP;
+    if (!last_of(&kp.tickets[g], (unsigned int)gsz)) return;
+    for (int q = threadIdx.x; q < 4 * njt; q += blockDim.x) {
+        double s = 0.0;
+        for (int b = g * RGROUP; b < g * RGROUP + gsz; b++) s += __ldcg(kp.part + 4 * (size_t)b * pld + q);
+        kp.gpart[4 * (size_t)g * pld + q] = s;
+    }
+    if (!last_of(&st->counter[3], (unsigned int)ng)) return;
+    for (int q = threadIdx.x; q < 4 * njt; q += blockDim.x) {
+        double s = 0.0;
+        for (int gg = 0; gg < ng; gg++) s += __ldcg(kp.gpart + 4 * (size_t)gg * pld + q);
+        double2 *dst = (q & 3) < 2 ? kp.D1 : kp.D2;
+        reinterpret_cast<double *>(dst + (q >> 2))[q & 1] = s;
+    }
+}
+
+
 // Sum of four values over the warp with a reduce-scatter butterfly: 6
 // shuffles instead of 4 x 5.  On return lane 8*q holds the total of a_q
 // (q = 0..3); the summation order is fixed (deterministic).
@@ -159,28 +200,7 @@ __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__
         }
         __syncthreads();
     }
-    if (last_block2(&st->counter[3])) {
-        const int nparts = (int)gridDim.x;
-        for (int j = warp; j < njt; j += D2_WARPS) {
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll 4
-            for (int b = lane; b < nparts; b += 32) {
-                const double *p = kp.part + 4 * ((size_t)b * pld + j);
-                s0 += __ldcg(p);
-                s1 += __ldcg(p + 1);
-                s2 += __ldcg(p + 2);
-                s3 += __ldcg(p + 3);
-            }
-            s0 = warp_sum(s0);
-            s1 = warp_sum(s1);
-            s2 = warp_sum(s2);
-            s3 = warp_sum(s3);
-            if (lane == 0) {
-                kp.D1[j] = make_double2(s0, s1);
-                kp.D2[j] = make_double2(s2, s3);
-            }
-        }
-    }
+    dots2_finish(kp, st, njt, pld);
 }
 
 // Split variant of the dot pass for grids with few tiles and many basis
@@ -247,28 +267,7 @@ __global__ void __launch_bounds__(D2_THREADS) k_dots2s(const CV *__restrict__ V,
         for (int q = threadIdx.x; q < nj * 4; q += blockDim.x) kp.part[4 * ((size_t)blockIdx.x * pld + jc) + q] = sacc[q];
         __syncthreads();
     }
-    if (last_block2(&st->counter[3])) {
-        const int nparts = (int)gridDim.x;
-        for (int j = warp; j < njt; j += D2_WARPS) {
-            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll 4
-            for (int b = lane; b < nparts; b += 32) {
-                const double *p = kp.part + 4 * ((size_t)b * pld + j);
-                s0 += __ldcg(p);
-                s1 += __ldcg(p + 1);
-                s2 += __ldcg(p + 2);
-                s3 += __ldcg(p + 3);
-            }
-            s0 = warp_sum(s0);
-            s1 = warp_sum(s1);
-            s2 = warp_sum(s2);
-            s3 = warp_sum(s3);
-            if (lane == 0) {
-                kp.D1[j] = make_double2(s0, s1);
-                kp.D2[j] = make_double2(s2, s3);
-            }
-        }
-    }
+    dots2_finish(kp, st, njt, pld);
 }
 
 template <typename CV, bool COMP, int D2_J, int U>

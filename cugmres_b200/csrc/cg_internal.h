@@ -58,6 +58,8 @@ struct KrylovPtrs {
     double2 *tv;     // [m+2] first-pass coefficients of A q_{k-1}
     double2 *P;      // [m+1] axpy coefficients for q_k
     double2 *S;      // [m+1] axpy coefficients for u_{k+1}
+    double *gpart;   // [ceil(nblk_dots2 / 16) * 4 * part_ld] group sums of the dot partials
+    unsigned int *tickets;  // [ceil(nblk_dots2 / 16)] arrival counters of those groups (reset by the last)
     int mcap;        // allocated restart capacity (leading dimension of Rm / part)
 };
 
