@@ -524,6 +524,55 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
         const double2 da = cmul(delta, a);
         kp.S[i] = make_double2((c.x - da.x * inu) * inu, (c.y - da.y * inu) * inu);
     }
+    // Rotations 0..k-2 applied to col[0..k-1]: the carried entry follows the
+    // affine recurrence carry_{j+1} = -s_j carry_j + c_j col[j+1], so the chain
+    // is a prefix scan of affine maps.  Each thread folds a segment of the
+    // rotations, the block scans the segment maps (Hillis-Steele, log2 of the
+    // thread count rounds), then each thread replays its segment from its
+    // incoming carry and writes the rotated entries of column k-1 into Rm.
+    __shared__ double scan_a[STEP_THREADS];
+    __shared__ double2 scan_b[STEP_THREADS];
+    __shared__ double2 carry_last;
+    const bool ref = st->rotation == 1;
+    if (k >= 1) {
+        const int nr = k - 1;
+        const int seg = (nr + STEP_THREADS - 1) / STEP_THREADS;
+        const int j0 = tid * seg < nr ? tid * seg : nr;
+        const int j1 = j0 + seg < nr ? j0 + seg : nr;
+        double a = 1.0;
+        double2 b = make_double2(0.0, 0.0);
+        for (int j = j0; j < j1; j++) {
+            const double sj = sns[j];
+            a = -sj * a;
+            b = cadd(cscale(b, -sj), cmul(css[j], col[j + 1]));
+        }
+        scan_a[tid] = a;
+        scan_b[tid] = b;
+        __syncthreads();
+        for (int off = 1; off < STEP_THREADS; off <<= 1) {
+            const double a2 = scan_a[tid];
+            const double2 b2 = scan_b[tid];
+            const double a1 = tid >= off ? scan_a[tid - off] : 1.0;
+            const double2 b1 = tid >= off ? scan_b[tid - off] : make_double2(0.0, 0.0);
+            __syncthreads();
+            if (tid >= off) {  // the earlier map (a1, b1), then this one (a2, b2)
+                scan_a[tid] = a2 * a1;
+                scan_b[tid] = cadd(cscale(b1, a2), b2);
+            }
+            __syncthreads();
+        }
+        double2 carry = col[0];
+        if (tid > 0) carry = cadd(cscale(col[0], scan_a[tid - 1]), scan_b[tid - 1]);
+        for (int j = j0; j < j1; j++) {
+            const double2 nx = col[j + 1];
+            const double2 c = css[j];
+            const double sj = sns[j];
+            kp.Rm[(size_t)(k - 1) * ld + j] = cadd(cmul(ref ? c : cconj(c), carry), cscale(nx, sj));
+            carry = csub(cmul(c, nx), cscale(carry, sj));
+        }
+        if (nr == 0 ? tid == 0 : (j0 < j1 && j1 == nr)) carry_last = carry;
+        __syncthreads();
+    }
     if (tid == 0) {
         if (brk) st->brk = 1;
         st->cu = inu;
@@ -534,16 +583,8 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
         if (k == 0) {
             kp.g[0] = make_double2(nu, 0.0);
         } else {
-            // Givens: rotations 0..k-2 on col[0..k-1], new rotation from (col[k-1], nu)
-            const bool ref = st->rotation == 1;
-            double2 carry = col[0];
-            for (int j = 0; j < k - 1; j++) {
-                const double2 nx = col[j + 1];
-                const double2 c = css[j];
-                const double s = sns[j];
-                col[j] = cadd(cmul(ref ? c : cconj(c), carry), cscale(nx, s));
-                carry = csub(cmul(c, nx), cscale(carry, s));
-            }
+            // new rotation from (rotated col[k-1], nu)
+            const double2 carry = carry_last;
             const double rho = hypot(hypot(carry.x, carry.y), nu);
             double2 c;
             double s;
@@ -555,7 +596,7 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
                 s = nu / rho;
             }
             const double2 cc = ref ? c : cconj(c);
-            col[k - 1] = cadd(cmul(cc, carry), make_double2(s * nu, 0.0));
+            kp.Rm[(size_t)(k - 1) * ld + (k - 1)] = cadd(cmul(cc, carry), make_double2(s * nu, 0.0));
             kp.cs[k - 1] = c;
             kp.sn[k - 1] = s;
             const double2 gk = kp.g[k - 1];
@@ -575,9 +616,6 @@ __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
         st->k = k + 1;
         st->stop = stop;
     }
-    __syncthreads();
-    if (k >= 1)
-        for (int i = tid; i < k; i += STEP_THREADS) kp.Rm[(size_t)(k - 1) * ld + i] = col[i];
 }
 
 // --------------------------------------------------------------- axpy2
