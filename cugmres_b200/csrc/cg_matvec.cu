@@ -24,7 +24,7 @@
 //
 // Launch shapes (points per thread, threads per block, resident blocks per SM
 // requested from the compiler) are template parameters; the MvShape variants
-// 0..3 are instantiated for L >= 256 and the autotuner in cg_api.cu picks one
+// 0..4 are instantiated for L >= 128 and the autotuner in cg_api.cu picks one
 // per (precision, L); smaller L always use variant 0.
 #include "cg_fft.cuh"
 #include "cg_internal.h"
@@ -49,7 +49,8 @@ typedef MvShape<16, 256, 256, 512, 1> MvV0;  // 16 points, wide blocks
 typedef MvShape<16, 256, 256, 512, 2> MvV1;  // 16 points, two blocks per SM (<= 128 registers)
 typedef MvShape<8, 256, 512, 512, 1> MvV2;   // 8 points, twice the threads per column
 typedef MvShape<8, 256, 256, 256, 2> MvV3;   // 8 points, two blocks per SM
-constexpr int MV_VARIANTS = 4;
+typedef MvShape<8, 64, 64, 64, 4> MvV4;      // 8 points, small blocks (many blocks on small grids)
+constexpr int MV_VARIANTS = 5;
 
 template <int L, typename SH> struct RowCfg {
     typedef Plan<L, SH::E> P;
@@ -329,17 +330,17 @@ template <typename SH, int L> struct Passes {
 };
 
 // Calls F<Passes<SH, L>>::run(args...) for the shape selected by `variant`
-// (L >= 256) or variant 0 (smaller L).
+// (L >= 128) or variant 0 (smaller L).
 template <template <typename> class F, typename... A> static int dispatch(int variant, int L, A... args) {
     switch (L) {
         case 16: return F<Passes<MvV0, 16>>::run(args...);
         case 32: return F<Passes<MvV0, 32>>::run(args...);
         case 64: return F<Passes<MvV0, 64>>::run(args...);
-        case 128: return F<Passes<MvV0, 128>>::run(args...);
         default: break;
     }
 #define CG_V_CASES(SH)                                            \
     switch (L) {                                                  \
+        case 128: return F<Passes<SH, 128>>::run(args...);        \
         case 256: return F<Passes<SH, 256>>::run(args...);        \
         case 512: return F<Passes<SH, 512>>::run(args...);        \
         case 1024: return F<Passes<SH, 1024>>::run(args...);      \
@@ -352,6 +353,7 @@ template <template <typename> class F, typename... A> static int dispatch(int va
         case 1: CG_V_CASES(MvV1)
         case 2: CG_V_CASES(MvV2)
         case 3: CG_V_CASES(MvV3)
+        case 4: CG_V_CASES(MvV4)
         default: return -1;
     }
 #undef CG_V_CASES
@@ -382,7 +384,7 @@ int fft_supported(int L) {
     return L == 16 || L == 32 || L == 64 || L == 128 || L == 256 || L == 512 || L == 1024 || L == 2048 || L == 4096;
 }
 
-int matvec_variants(int L) { return L >= 256 ? MV_VARIANTS : 1; }
+int matvec_variants(int L) { return L >= 128 ? MV_VARIANTS : 1; }
 
 int rows_per_block(int variant, int L) { return dispatch<RpcF>(variant, L); }
 

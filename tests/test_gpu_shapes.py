@@ -16,7 +16,7 @@ sys.path.insert(0, sys.argv[1])
 import cugmres_b200 as cg
 from cugmres_b200 import problems as P
 from oracle import oracle as O
-for N in (128, 300, 512):
+for N in (64, 128, 300, 512):
     pr = P.helmholtz(N, 4.0, seed=N)
     s = cg.Solver(0).set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
     x = np.random.default_rng(N).standard_normal((N, N)) + 1j
@@ -30,7 +30,7 @@ for N in (128, 300, 512):
 """
 
 
-@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "tuned"])
+@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "4", "tuned"])
 def test_matvec_shape_parity(cuda_device, shape, tmp_path):
     env = dict(os.environ)
     env["CUGMRES_TUNE_CACHE"] = str(tmp_path / "tune.txt")
