@@ -28,6 +28,7 @@
 
 #include "../../include/cugmres.h"
 #include "cg_common.cuh"
+#include "cg_fft.cuh"
 #include "cg_fno.h"
 #include "cg_internal.h"
 
@@ -155,7 +156,7 @@ __global__ void k_quarter(const double2 *__restrict__ full, double2 *__restrict_
     const int Lq = L / 2 + 1;
     const long long tot = (long long)Lq * Lq;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (long long)gridDim.x * blockDim.x) {
-        const int r = (int)(e / Lq), c = (int)(e % Lq);
+        const int c = (int)(e / Lq), r = (int)(e % Lq);  // column-major quarter
         const double2 v = full[(size_t)r * L + c];
         q64[e] = make_double2(v.x * scale, v.y * scale);
         q32[e] = make_float2((float)(v.x * scale), (float)(v.y * scale));
@@ -298,6 +299,7 @@ MatvecArgs margs(const cg_ctx *c, int prec, int transpose = 0) {
     a.cdiag = prec == 0 ? (const void *)c->c64 : (const void *)c->c32;
     a.tw = prec == 0 ? (const void *)c->tw64 : (const void *)c->tw32;
     a.T = c->T;
+    a.sms = c->sms;
     return a;
 }
 
@@ -316,9 +318,10 @@ int row_blocks(const cg_ctx *c) {
 }
 
 // ------------------------------------------------------------- autotuner
-// Times each launch shape of each matvec pass on the context's operator with
-// CUDA events and keeps the fastest.  Choices are cached per process and in a
-// text file (one line "device|L|precision fwd cols inv") under
+// Picks the launch shape of each matvec pass on the context's operator by
+// coordinate descent over (forward, columns, inverse), timing whole matvecs
+// with CUDA events, each after an L2 flush.  Choices are cached per process
+// and in a text file (one line "device|L|precision|version fwd cols inv") under
 // $CUGMRES_TUNE_CACHE, else $XDG_CACHE_HOME/cugmres_b200/autotune.txt, else
 // ~/.cache/cugmres_b200/autotune.txt.  CUGMRES_AUTOTUNE=0 disables tuning;
 // CUGMRES_MATVEC_SHAPE=v forces shape v.
@@ -382,7 +385,9 @@ int autotune(cg_ctx *c, int prec) {
         for (int p = 0; p < 3; p++) c->var[prec][p] = v;
         return CG_OK;
     }
-    std::string key = std::string(c->devname) + "|" + std::to_string(c->L) + "|" + std::to_string(prec);
+    // the key carries the tuner's version so that choices made by an older
+    // tuner or for older kernels are not reused
+    std::string key = std::string(c->devname) + "|" + std::to_string(c->L) + "|" + std::to_string(prec) + "|t2";
     for (char &ch : key)
         if (ch == ' ') ch = '_';
     {
@@ -398,39 +403,67 @@ int autotune(cg_ctx *c, int prec) {
     cudaStream_t s = c->stream;
     CG_CU(cudaMemsetAsync(c->xbuf, 0, sizeof(double2) * n, s));
     CG_CU(cudaMemsetAsync(c->T, 0, sizeof(double2) * (size_t)c->N * c->L, s));
+    // In a solve the dot and axpy passes stream the Krylov basis through L2
+    // between two matvecs, so each timed matvec starts after a write of twice
+    // the L2 size (skipped if that buffer cannot be had).
+    int l2 = 0;
+    cudaDeviceGetAttribute(&l2, cudaDevAttrL2CacheSize, c->device);
+    const size_t flush_bytes = (size_t)std::max(l2, 1 << 20) * 2;
+    void *flush = nullptr;
+    if (cudaMalloc(&flush, flush_bytes) != cudaSuccess) {
+        flush = nullptr;
+        cudaGetLastError();
+    }
     cudaEvent_t e0, e1;
     CG_CU(cudaEventCreate(&e0));
     CG_CU(cudaEventCreate(&e1));
-    std::array<int, 3> best = {0, 0, 0};
     int status = CG_OK;
-    for (int pass = 0; pass < 3 && status == CG_OK; pass++) {
-        float best_ms = 1e30f;
-        for (int v = 0; v < nv && status == CG_OK; v++) {
-            MatvecArgs a = margs(c, prec);
-            a.vfwd = a.vcols = a.vinv = v;
-            auto launch = [&]() -> int {
-                if (pass == 0) return launch_rows_forward(prec, a, fixed_vec(c->xbuf), nullptr, nullptr, GATE_NONE, s);
-                if (pass == 1) return launch_cols_convolve(prec, a, nullptr, GATE_NONE, s);
-                return launch_rows_inverse(prec, 0, prec, a, fixed_vec(c->xbuf), nullptr, nullptr, fixed_vec(c->rbuf),
-                                           nullptr, nullptr, GATE_NONE, s);
-            };
-            for (int w = 0; w < 2 && status == CG_OK; w++)
-                if (launch() != 0) status = CG_ERR_CUDA;
+    // time of the whole three-pass matvec (sum over timed repetitions)
+    auto time_shapes = [&](const std::array<int, 3> &v) -> float {
+        MatvecArgs a = margs(c, prec);
+        a.vfwd = v[0];
+        a.vcols = v[1];
+        a.vinv = v[2];
+        float tot = 0.f;
+        constexpr int WARM = 2, REPS = 6;
+        for (int r = 0; r < WARM + REPS && status == CG_OK; r++) {
+            if (flush && cudaMemsetAsync(flush, r & 0xff, flush_bytes, s) != cudaSuccess) status = CG_ERR_CUDA;
             cudaEventRecord(e0, s);
-            for (int r = 0; r < 5 && status == CG_OK; r++)
-                if (launch() != 0) status = CG_ERR_CUDA;
+            if (launch_rows_forward(prec, a, fixed_vec(c->xbuf), nullptr, nullptr, GATE_NONE, s) != 0 ||
+                launch_cols_convolve(prec, a, nullptr, GATE_NONE, s) != 0 ||
+                launch_rows_inverse(prec, 0, prec, a, fixed_vec(c->xbuf), nullptr, nullptr, fixed_vec(c->rbuf), nullptr,
+                                    nullptr, GATE_NONE, s) != 0)
+                status = CG_ERR_CUDA;
             cudaEventRecord(e1, s);
             if (cudaEventSynchronize(e1) != cudaSuccess) status = CG_ERR_CUDA;
             float ms = 0.f;
             cudaEventElapsedTime(&ms, e0, e1);
-            if (ms < best_ms) {
-                best_ms = ms;
-                best[pass] = v;
-            }
+            if (r >= WARM) tot += ms;
         }
+        return tot;
+    };
+    // coordinate descent over the three passes, starting from shape 0
+    std::array<int, 3> best = {0, 0, 0};
+    float best_ms = time_shapes(best);
+    for (int sweep = 0; sweep < 2 && status == CG_OK; sweep++) {
+        bool changed = false;
+        for (int pass = 0; pass < 3 && status == CG_OK; pass++)
+            for (int v = 0; v < nv && status == CG_OK; v++) {
+                if (v == best[pass]) continue;
+                std::array<int, 3> cand = best;
+                cand[pass] = v;
+                const float ms = time_shapes(cand);
+                if (ms < 0.99f * best_ms) {
+                    best_ms = ms;
+                    best = cand;
+                    changed = true;
+                }
+            }
+        if (!changed) break;
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (flush) cudaFree(flush);
     if (status != CG_OK) return status;
     for (int p = 0; p < 3; p++) c->var[prec][p] = best[p];
     std::lock_guard<std::mutex> lock(g_tune_mu);
@@ -702,27 +735,29 @@ int cugmres_set_operator(cg_ctx *c, int N, const cg_c128 *g_block, const double 
         CG_CU(cudaMalloc((void **)&c->c64, sizeof(double) * n));
         CG_CU(cudaMalloc((void **)&c->c32, sizeof(float) * n));
         CG_CU(cudaMalloc((void **)&c->chi32, sizeof(float) * n));
-        CG_CU(cudaMalloc((void **)&c->tw64, sizeof(double2) * 2 * L));
-        CG_CU(cudaMalloc((void **)&c->tw32, sizeof(float2) * 2 * L));
+        CG_CU(cudaMalloc((void **)&c->tw64, sizeof(double2) * 4 * L));
+        CG_CU(cudaMalloc((void **)&c->tw32, sizeof(float2) * 4 * L));
         CG_CU(cudaMalloc(&c->T, sizeof(double2) * (size_t)N * L));
         CG_CU(cudaMalloc((void **)&c->bbuf, sizeof(double2) * n));
         CG_CU(cudaMalloc((void **)&c->xbuf, sizeof(double2) * n));
         CG_CU(cudaMalloc((void **)&c->rbuf, sizeof(double2) * n));
     }
-    // twiddles exp(-2 pi i m / L) and their conjugates, in double
-    std::vector<double2> tw(2 * L);
-    std::vector<float2> twf(2 * L);
+    // per-stage twiddle tables (cg_fft.cuh layout) of the 16- and 8-point
+    // plans, forward exp(-2 pi i m / L) and inverse, computed in double
+    std::vector<double2> tw(4 * L);
+    std::vector<float2> twf(4 * L);
     const double pi = 3.14159265358979323846;
-    for (int m = 0; m < L; m++) {
-        const double a = 2.0 * pi * (double)m / (double)L;
-        const double cr = cos(a), si = sin(a);
-        tw[m] = make_double2(cr, -si);
-        tw[L + m] = make_double2(cr, si);
-        twf[m] = make_float2((float)cr, (float)-si);
-        twf[L + m] = make_float2((float)cr, (float)si);
+    for (int t = 0; t < 4; t++) {
+        const double sg = (t & 1) ? 1.0 : -1.0;
+        for (int i = 0; i < L; i++) {
+            const int m = twiddle_exponent(L, t < 2 ? 16 : 8, i);
+            const double a = 2.0 * pi * (double)(m < 0 ? 0 : m) / (double)L;
+            tw[(size_t)t * L + i] = m < 0 ? make_double2(0.0, 0.0) : make_double2(cos(a), sg * sin(a));
+        }
     }
-    CG_CU(cudaMemcpyAsync(c->tw64, tw.data(), sizeof(double2) * 2 * L, cudaMemcpyHostToDevice, c->stream));
-    CG_CU(cudaMemcpyAsync(c->tw32, twf.data(), sizeof(float2) * 2 * L, cudaMemcpyHostToDevice, c->stream));
+    for (size_t i = 0; i < tw.size(); i++) twf[i] = make_float2((float)tw[i].x, (float)tw[i].y);
+    CG_CU(cudaMemcpyAsync(c->tw64, tw.data(), sizeof(double2) * 4 * L, cudaMemcpyHostToDevice, c->stream));
+    CG_CU(cudaMemcpyAsync(c->tw32, twf.data(), sizeof(float2) * 4 * L, cudaMemcpyHostToDevice, c->stream));
     double2 *g_tmp = nullptr;
     double *chi_tmp = nullptr;
     const double2 *gp = (const double2 *)g_block;

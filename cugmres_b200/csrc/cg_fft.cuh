@@ -9,8 +9,13 @@
 // where each thread owns E = 16 (or 8) points:
 //
 //   stage s with radix R and span Ns reads  a[j + r L/R]          (r < R)
-//   multiplies by the twiddle  w_L^{(j mod Ns) r L/(Ns R)},
+//   multiplies by the twiddle  w_{Ns R}^{(j mod Ns) r} = w_L^{(j mod Ns) r L/(Ns R)},
 //   does an R-point DFT and writes b[(j/Ns) Ns R + (j mod Ns) + q Ns] (q < R).
+//
+// Twiddles come from per-stage tables (see Plan::twoff): stage s >= 1 keeps
+// w_{Ns R}^{k r} for k < Ns, 1 <= r < R at twoff(s) + (r-1) Ns + k, so the
+// threads of a warp (consecutive k) read consecutive entries instead of
+// entries k r L/(Ns R) apart in one length-L table.
 //
 // Thread t of a transform owns butterflies j = t + b*TPR (TPR = L/E threads).
 // The first stage (span 1, no twiddles) reads and the last stage (span L/R)
@@ -175,12 +180,45 @@ template <int L, int E0 = 16> struct Plan {
     // padded shared-memory index (one pad element every 16)
     static __device__ __forceinline__ int pad(int i) { return i + (i >> 4); }
     static constexpr int SMEM_ELEMS = L + L / 16;
+    // offset of stage s's twiddles (s >= 1); the tables of all stages take
+    // sum_s (R_s - 1) Ns_s = L - R_0 < L entries
+    __host__ __device__ static constexpr int twoff(int s) {
+        return s <= 1 ? 0 : twoff(s - 1) + (radix(s - 1) - 1) * span(s - 1);
+    }
 };
 
-// Twiddle lookup: the caller passes the forward table exp(-2 pi i m / L) or,
-// for inverse transforms, the conjugated table; m < L.
-template <bool INV, typename C> __device__ __forceinline__ C twiddle(const C *__restrict__ tw, int m) {
-    return __ldg(tw + m);
+// Twiddle tables of one precision, 4 L entries: [E0 = 16 forward | E0 = 16
+// inverse | E0 = 8 forward | E0 = 8 inverse], each in the per-stage layout of
+// Plan<L, E0> (forward exp(-2 pi i m / L), inverse the conjugates).
+template <int L, int E0, bool INV, typename C> __device__ __forceinline__ const C *tw_table(const C *tw) {
+    return tw + (E0 == 16 ? 0 : 2 * L) + (INV ? L : 0);
+}
+
+// Exponent m of entry i of the per-stage table of a length-L transform with
+// E0 points per thread (the entry is exp(-/+ 2 pi i m / L)), or -1 for the
+// unused entries i >= L - R_0.  Mirrors Plan at run time, for the host and
+// for device-side table builders.
+__host__ __device__ inline int twiddle_exponent(int L, int E0, int i) {
+    const int E = L >= E0 ? E0 : L;
+    int lg = 0, lge = 0;
+    while ((1 << lg) < L) lg++;
+    while ((1 << lge) < E) lge++;
+    const int nfull = lg / lge, rem = 1 << (lg - nfull * lge);
+    const int nst = nfull + (rem > 1 ? 1 : 0);
+    int ns = 1, off = 0;
+    for (int st = 0; st < nst; st++) {
+        const int R = st < nfull ? E : rem;
+        if (st > 0) {
+            const int size = (R - 1) * ns;
+            if (i < off + size) {
+                const int r = (i - off) / ns + 1, k = (i - off) % ns;
+                return k * r * (L / (ns * R));
+            }
+            off += size;
+        }
+        ns *= R;
+    }
+    return -1;
 }
 
 // One Stockham stage S of a length-L transform (compile-time radix and span).
@@ -213,11 +251,11 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
             for (int b = 0; b < NB; b++) {
                 const int j = t + b * TPR;
                 const int k = j % Ns;
-                constexpr int step = L / (Ns * R);
+                const C *__restrict__ ts = tw + P::twoff(S) + k;
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     C v = sm[P::pad(j + r * (L / R)) * SMS];
-                    if (r > 0) v = cmul(v, twiddle<INV>(tw, k * r * step));
+                    if (r > 0) v = cmul(v, __ldg(ts + (r - 1) * Ns));
                     tmp[b * R + r] = v;
                 }
             }
@@ -250,11 +288,12 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
 // keeps the column kernels' accesses on distinct banks).
 // HALF_IN: inputs L/2 .. L-1 are zero (first stage uses dft_half_input).
 // Every thread of the block must call this the same number of times
-// (it contains __syncthreads()).
+// (it contains __syncthreads()).  tw is the base of the 4 L-entry table set
+// (tw_table picks the plan's and direction's table).
 template <int L, int E0, bool INV, bool HALF_IN, int SMS = 1, typename C>
 __device__ __forceinline__ void fft_run(C (&reg)[Plan<L, E0>::E], C *sm, const C *__restrict__ tw, int t) {
     C tmp[Plan<L, E0>::E];
-    Stage<L, E0, INV, HALF_IN, 0, SMS>::run(reg, tmp, sm, tw, t);
+    Stage<L, E0, INV, HALF_IN, 0, SMS>::run(reg, tmp, sm, tw_table<L, E0, INV>(tw), t);
 }
 
 }  // namespace cg

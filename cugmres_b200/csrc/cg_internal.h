@@ -72,6 +72,7 @@ struct MatvecArgs {
     const void *tw;     // L twiddles (C)
     void *T;            // N x L intermediate (C)
     int transpose = 0;  // 1: A^T x = x - diag(c) G x (contrast applied after the convolution)
+    int sms = 148;      // multiprocessors of the device (grid of the persistent column pass)
 };
 
 // Reference to a basis vector selected by the device-side Arnoldi index:

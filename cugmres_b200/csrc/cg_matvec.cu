@@ -17,14 +17,16 @@
 //                            r = b - x + conv (residual), with ||y||^2 partials.
 // The spectrum is even in both axes for the reference's kernel and for the
 // GFIEM kernel (G depends on |d1|, |d2|), so only its quarter
-// (L/2+1) x (L/2+1) is stored and read; the 1/L^2 normalisation is folded into it.
-// Twiddle tables hold 2L entries: exp(-2 pi i m/L) then its conjugate, so the
-// inverse transform reads different addresses from the forward one (otherwise
-// the compiler keeps the forward twiddles live across the column convolution).
+// (L/2+1) x (L/2+1) is stored and read, column-major (Gq[qc][qr]) so that the
+// column pass reads it along its columns; the 1/L^2 normalisation is folded into it.
+// Twiddle tables (cg_fft.cuh) hold 4L entries: per-stage forward and inverse
+// tables of the 16- and 8-point plans.  The inverse transform reads different
+// addresses from the forward one (otherwise the compiler keeps the forward
+// twiddles live across the column convolution).
 //
 // Launch shapes (points per thread, threads per block, resident blocks per SM
-// requested from the compiler) are template parameters; the MvShape variants
-// 0..4 are instantiated for L >= 128 and the autotuner in cg_api.cu picks one
+// requested from the compiler, pipelined column pass) are template parameters;
+// the MvShape variants 0..6 are instantiated for L >= 128 and the autotuner in cg_api.cu picks one
 // per (precision, L); smaller L always use variant 0.
 #include "cg_fft.cuh"
 #include "cg_internal.h"
@@ -41,16 +43,19 @@ static __device__ __forceinline__ long long sel_index(const DevState *st, int ko
 
 // E: points per thread; ROWT: target threads per row block; COLT64 / COLT32:
 // target threads per column block in FP64 / FP32; MINB: resident blocks per SM
-// requested from the compiler (bounds the registers per thread).
-template <int E_, int ROWT_, int COLT64_, int COLT32_, int MINB_> struct MvShape {
-    static constexpr int E = E_, ROWT = ROWT_, COLT64 = COLT64_, COLT32 = COLT32_, MINB = MINB_;
+// requested from the compiler (bounds the registers per thread); PIPE: the
+// column pass is the persistent, double-buffered k_cols_convolve_pipe.
+template <int E_, int ROWT_, int COLT64_, int COLT32_, int MINB_, int PIPE_ = 0> struct MvShape {
+    static constexpr int E = E_, ROWT = ROWT_, COLT64 = COLT64_, COLT32 = COLT32_, MINB = MINB_, PIPE = PIPE_;
 };
-typedef MvShape<16, 256, 256, 512, 1> MvV0;  // 16 points, wide blocks
-typedef MvShape<16, 256, 256, 512, 2> MvV1;  // 16 points, two blocks per SM (<= 128 registers)
-typedef MvShape<8, 256, 512, 512, 1> MvV2;   // 8 points, twice the threads per column
-typedef MvShape<8, 256, 256, 256, 2> MvV3;   // 8 points, two blocks per SM
-typedef MvShape<8, 64, 64, 64, 4> MvV4;      // 8 points, small blocks (many blocks on small grids)
-constexpr int MV_VARIANTS = 5;
+typedef MvShape<16, 256, 256, 512, 1> MvV0;     // 16 points, wide blocks
+typedef MvShape<16, 256, 256, 512, 2> MvV1;     // 16 points, two blocks per SM (<= 128 registers)
+typedef MvShape<8, 256, 512, 512, 1> MvV2;      // 8 points, twice the threads per column
+typedef MvShape<8, 256, 256, 256, 2> MvV3;      // 8 points, two blocks per SM
+typedef MvShape<8, 64, 64, 64, 4> MvV4;         // 8 points, small blocks (many blocks on small grids)
+typedef MvShape<16, 256, 256, 512, 1, 1> MvV5;  // V0 with the pipelined column pass
+typedef MvShape<8, 256, 512, 512, 1, 1> MvV6;   // V2 with the pipelined column pass
+constexpr int MV_VARIANTS = 7;
 
 template <int L, typename SH> struct RowCfg {
     typedef Plan<L, SH::E> P;
@@ -139,14 +144,110 @@ k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict
     for (int p = 0; p < E; p++) {
         const int k1 = t + p * TPR;
         const int qr = k1 <= L / 2 ? k1 : L - k1;
-        reg[p] = cmul(reg[p], __ldg(gq + (size_t)qr * Lq + qc));
+        reg[p] = cmul(reg[p], __ldg(gq + (size_t)qc * Lq + qr));
     }
-    fft_run<L, SH::E, true, false, CPB>(reg, sm, tw + L, t);
+    fft_run<L, SH::E, true, false, CPB>(reg, sm, tw, t);
 #pragma unroll
     for (int p = 0; p < E / 2; p++) {
         const int k = t + p * TPR;
         if (k < N) T[(size_t)k * L + col] = reg[p];
     }
+}
+
+// Pass 2, persistent and double-buffered: one block per SM walks the column
+// tiles v = blockIdx.x, blockIdx.x + gridDim.x, ...; while it transforms tile
+// v, cp.async copies tile v + gridDim.x (rows 0..N-1 of its CPB columns) and
+// that tile's CPB quarter-spectrum columns into the other half of a shared
+// staging buffer, so the loads of T and of the spectrum leave the critical
+// path.  Same arithmetic, in the same order, as k_cols_convolve.
+static __device__ __forceinline__ uint32_t cg_smem_u32(const void *p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+template <typename C> static __device__ __forceinline__ void cp_async_elem(C *dst, const C *src) {
+    if constexpr (sizeof(C) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(cg_smem_u32(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(cg_smem_u32(dst)), "l"(src) : "memory");
+}
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int NPEND> static __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(NPEND) : "memory");
+}
+
+template <int L, typename SH, int ESZ> struct PipeCfg {
+    typedef ColCfg<L, SH, ESZ> Q;
+    static constexpr int LQ = L / 2 + 1;
+    static constexpr int TD = (L / 2) * Q::CPB;       // staged tile: rows < L/2 (N <= L/2)
+    static constexpr int GD = ((LQ * Q::CPB + 1) / 2) * 2;  // staged spectrum columns (even count: 16-byte slots)
+    static constexpr int SLOT = TD + GD;
+    static constexpr int SMEM_ELEMS = Q::SMEM_ELEMS + 2 * SLOT;
+};
+
+template <typename C, int L, typename SH>
+__global__ void __launch_bounds__(ColCfg<L, SH, sizeof(C)>::THREADS, 1)
+k_cols_convolve_pipe(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict__ tw, int N, const DevState *st,
+                     int gate) {
+    typedef Plan<L, SH::E> P;
+    typedef ColCfg<L, SH, sizeof(C)> Q;
+    typedef PipeCfg<L, SH, sizeof(C)> G;
+    constexpr int E = P::E, TPR = P::TPR, CPB = Q::CPB, THREADS = Q::THREADS, LQ = G::LQ;
+    if (gated(st, gate)) return;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    C *sx = reinterpret_cast<C *>(smraw);  // FFT exchange, Q::SMEM_ELEMS
+    C *buf = sx + Q::SMEM_ELEMS;           // two staging slots
+    const int cl = threadIdx.x % CPB, t = threadIdx.x / CPB;
+    C *sm = sx + cl;
+    const int ntiles = L / CPB;
+    // mirrored tile order, as in k_cols_convolve: neighbouring v share spectrum columns
+    auto tile_of = [ntiles](int v) { return (v & 1) ? (ntiles - 1 - (v >> 1)) : (v >> 1); };
+    auto issue = [&](int v, int slot) {
+        C *td = buf + slot * G::SLOT;
+        C *gd = td + G::TD;
+        const int col0 = tile_of(v) * CPB;
+        for (int e = threadIdx.x; e < N * CPB; e += THREADS)
+            cp_async_elem(td + e, T + (size_t)(e / CPB) * L + col0 + (e % CPB));
+        for (int e = threadIdx.x; e < LQ * CPB; e += THREADS) {
+            const int c = e / LQ, qr = e % LQ;
+            const int col = col0 + c;
+            const int qc = col <= L / 2 ? col : L - col;
+            cp_async_elem(gd + e, gq + (size_t)qc * LQ + qr);
+        }
+        cp_async_commit();
+    };
+    int v = blockIdx.x;
+    if (v < ntiles) issue(v, 0);
+    for (int it = 0; v < ntiles; it++, v += gridDim.x) {
+        const int slot = it & 1;
+        if (v + (int)gridDim.x < ntiles) issue(v + gridDim.x, slot ^ 1);
+        else cp_async_commit();  // empty group: the wait below always leaves one group pending
+        cp_async_wait<1>();
+        __syncthreads();
+        const C *td = buf + slot * G::SLOT;
+        const C *gd = td + G::TD;
+        const int col = tile_of(v) * CPB + cl;
+        C reg[E];
+#pragma unroll
+        for (int p = 0; p < E; p++) {
+            const int k = t + p * TPR;
+            reg[p] = czero<C>();
+            if (p < E / 2 && k < N) reg[p] = td[k * CPB + cl];
+        }
+        fft_run<L, SH::E, false, true, CPB>(reg, sm, tw, t);
+#pragma unroll
+        for (int p = 0; p < E; p++) {
+            const int k1 = t + p * TPR;
+            const int qr = k1 <= L / 2 ? k1 : L - k1;
+            reg[p] = cmul(reg[p], gd[cl * LQ + qr]);
+        }
+        fft_run<L, SH::E, true, false, CPB>(reg, sm, tw, t);
+#pragma unroll
+        for (int p = 0; p < E / 2; p++) {
+            const int k = t + p * TPR;
+            if (k < N) T[(size_t)k * L + col] = reg[p];
+        }
+        __syncthreads();  // this slot is refilled by the next iteration's issue
+    }
+    cp_async_wait<0>();
 }
 
 // ---------------------------------------------------------------- pass 3
@@ -176,7 +277,7 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
 #pragma unroll
         for (int p = 0; p < E; p++) reg[p] = czero<C>();
     }
-    fft_run<L, SH::E, true, false>(reg, sm, tw + L, t);
+    fft_run<L, SH::E, true, false>(reg, sm, tw, t);
     const long long kx = sel_index(st, xs.koff);
     const long long ky = sel_index(st, ys.koff);
     const C *x = reinterpret_cast<const C *>(xs.base) + kx * xs.stride;
@@ -266,7 +367,13 @@ template <typename K> static int set_smem(K kern, size_t bytes) {
 }
 
 // The three passes for one launch shape SH and one embedding size L.
-template <typename SH, int L> struct Passes {
+// The row passes do not depend on PIPE: shapes that differ only in it share
+// one row-pass instantiation.
+template <typename SH> using RowShape = MvShape<SH::E, SH::ROWT, SH::COLT64, SH::COLT32, SH::MINB, 0>;
+
+template <typename SH0, int L> struct Passes {
+    typedef RowShape<SH0> SH;  // row passes
+    typedef SH0 CS;            // column pass
     static int fwd(int prec, const MatvecArgs &a, VecSel x, const double *xs, const DevState *st, int gate,
                    cudaStream_t s) {
         typedef RowCfg<L, SH> Q;
@@ -290,13 +397,24 @@ template <typename SH, int L> struct Passes {
     }
 
     template <typename C> static int cols_t(const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
-        typedef ColCfg<L, SH, sizeof(C)> Q;
-        const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
-        auto kern = k_cols_convolve<C, L, SH>;
-        int e = set_smem(kern, smem);
-        if (e) return e;
-        kern<<<L / Q::CPB, Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate);
-        return (int)cudaGetLastError();
+        typedef ColCfg<L, CS, sizeof(C)> Q;
+        if constexpr (CS::PIPE) {
+            const size_t smem = (size_t)PipeCfg<L, CS, sizeof(C)>::SMEM_ELEMS * sizeof(C);
+            auto kern = k_cols_convolve_pipe<C, L, CS>;
+            int e = set_smem(kern, smem);
+            if (e) return e;
+            const int ntiles = L / Q::CPB;
+            const int grid = ntiles < a.sms ? ntiles : a.sms;
+            kern<<<grid, Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate);
+            return (int)cudaGetLastError();
+        } else {
+            const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
+            auto kern = k_cols_convolve<C, L, CS>;
+            int e = set_smem(kern, smem);
+            if (e) return e;
+            kern<<<L / Q::CPB, Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate);
+            return (int)cudaGetLastError();
+        }
     }
     static int cols(int prec, const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
         return prec == 0 ? cols_t<double2>(a, st, gate, s) : cols_t<float2>(a, st, gate, s);
@@ -354,6 +472,8 @@ template <template <typename> class F, typename... A> static int dispatch(int va
         case 2: CG_V_CASES(MvV2)
         case 3: CG_V_CASES(MvV3)
         case 4: CG_V_CASES(MvV4)
+        case 5: CG_V_CASES(MvV5)
+        case 6: CG_V_CASES(MvV6)
         default: return -1;
     }
 #undef CG_V_CASES

@@ -8,7 +8,7 @@
 // Green's block, the contrast and x without any allocation: every
 // intermediate buffer lives in the file-scope device array g_noalloc_scratch
 // below, whose size fixes the largest grid it accepts (N <= 256, so
-// L <= 512).  Every GPU that loads the library keeps this array (about 7.6 MB)
+// L <= 512).  Every GPU that loads the library keeps this array (about 7.9 MB)
 // until the process exits.
 //
 // Properties a caller must know:
@@ -26,6 +26,7 @@
 
 #include "../../include/cugmres.h"
 #include "cg_common.cuh"
+#include "cg_fft.cuh"
 #include "cg_internal.h"
 
 namespace {
@@ -38,7 +39,7 @@ constexpr size_t NA_OFF_QUARTER = na_align(NA_OFF_FULL + (size_t)NA_MAX_L * NA_M
 constexpr size_t NA_OFF_T = na_align(NA_OFF_QUARTER + (size_t)(NA_MAX_L / 2 + 1) * (NA_MAX_L / 2 + 1) * sizeof(double2));
 constexpr size_t NA_OFF_C = na_align(NA_OFF_T + (size_t)NA_MAX_N * NA_MAX_L * sizeof(double2));
 constexpr size_t NA_OFF_TW = na_align(NA_OFF_C + (size_t)NA_MAX_N * NA_MAX_N * sizeof(double));
-constexpr size_t NA_BYTES = na_align(NA_OFF_TW + (size_t)2 * NA_MAX_L * sizeof(double2));
+constexpr size_t NA_BYTES = na_align(NA_OFF_TW + (size_t)4 * NA_MAX_L * sizeof(double2));
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[NA_BYTES];
 
@@ -72,13 +73,15 @@ bool na_on_device(const void *p) {
     return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
 }
 
-// twiddles exp(-2 pi i m/L) then their conjugates
+// the four per-stage twiddle tables of cg_fft.cuh (16- and 8-point plans,
+// forward and inverse), 4 L entries
 __global__ void k_na_twiddles(double2 *tw, int L) {
-    for (int m = blockIdx.x * blockDim.x + threadIdx.x; m < L; m += gridDim.x * blockDim.x) {
-        double s, c;
-        sincospi(2.0 * (double)m / (double)L, &s, &c);
-        tw[m] = make_double2(c, -s);
-        tw[L + m] = make_double2(c, s);
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < 4 * L; e += gridDim.x * blockDim.x) {
+        const int t = e / L, i = e % L;
+        const int m = cg::twiddle_exponent(L, t < 2 ? 16 : 8, i);
+        double s = 0.0, c = 0.0;
+        if (m >= 0) sincospi(2.0 * (double)m / (double)L, &s, &c);
+        tw[e] = make_double2(c, (t & 1) ? s : -s);
     }
 }
 
@@ -99,7 +102,7 @@ __global__ void k_na_prepare(const double2 *__restrict__ full, double2 *__restri
     const int Lq = L / 2 + 1;
     const double inv = 1.0 / ((double)L * (double)L);
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < Lq * Lq; e += gridDim.x * blockDim.x) {
-        const double2 v = full[(e / Lq) * L + (e % Lq)];
+        const double2 v = full[(e % Lq) * L + (e / Lq)];  // column-major quarter
         quarter[e] = make_double2(v.x * inv, v.y * inv);
     }
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < n; e += gridDim.x * blockDim.x) c[e] = chi[e] * scale;
@@ -126,7 +129,7 @@ extern "C" int cugmres_matvec_noalloc(int N, const cg_c128 *g_block, const doubl
     double *c = (double *)(base + NA_OFF_C);
     double2 *tw = (double2 *)(base + NA_OFF_TW);
 
-    k_na_twiddles<<<(L + 255) / 256, 256, 0, s>>>(tw, L);
+    k_na_twiddles<<<(4 * L + 255) / 256, 256, 0, s>>>(tw, L);
     k_na_embed<<<(L * L + 255) / 256, 256, 0, s>>>((const double2 *)g_block, full, N, L);
     if (cudaGetLastError() != cudaSuccess) return CG_ERR_CUDA;
     if (cg::launch_fft2d_full_fp64(L, full, tw, s) != 0) return CG_ERR_CUDA;

@@ -150,7 +150,7 @@ int cugmres_set_operator_circulant(cg_ctx *ctx, int N, const cg_c64 *g_prep, con
 int cugmres_grid_size(const cg_ctx *ctx, int *N, int *L);
 /* Launch shapes the autotuner chose for the three matvec passes (row forward,
  * column convolution, row inverse) of `precision`; shapes[3] receives indices
- * 0..4 (0 for embeddings L < 128).  Tuning runs in cugmres_set_operator and is
+ * 0..6 (0 for embeddings L < 128).  Tuning runs in cugmres_set_operator and is
  * cached per device in $CUGMRES_TUNE_CACHE (default
  * ~/.cache/cugmres_b200/autotune.txt); CUGMRES_AUTOTUNE=0 keeps shape 0. */
 int cugmres_matvec_shapes(const cg_ctx *ctx, int precision, int *shapes);
@@ -237,7 +237,7 @@ int cugmres_fast_gmres(const cg_c64 *g_prep, const unsigned char *mask, cg_c64 *
  * No counterpart in the reference (its matvec allocates through cuFFT plans and
  * the solver cudaMallocs per call).  It builds the spectrum from g_block and
  * applies A = I - G diag(chi_scale * chi) to x, using only a fixed scratch
- * array compiled into the library (about 7.6 MB per GPU, held until exit).
+ * array compiled into the library (about 7.9 MB per GPU, held until exit).
  *   - N <= CUGMRES_NOALLOC_MAX_N, otherwise CG_ERR_INVALID (use cugmres_matvec);
  *   - g_block (N x N), chi (N x N), x and y must be device memory of the current
  *     device, otherwise CG_ERR_INVALID;
