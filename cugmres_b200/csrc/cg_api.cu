@@ -65,6 +65,10 @@ struct cg_ctx {
     cudaEvent_t ev = nullptr;
     // launch shapes of the three matvec passes per precision (autotuned)
     int var[2][3] = {{0, 0, 0}, {0, 0, 0}};
+    // the GPU is shared with other contexts' solves (batched sweeps): the
+    // autotuner leaves out the persistent column pass, which would hold every
+    // SM's shared memory while the other streams' kernels wait
+    bool shared_gpu = false;
     char devname[256] = {0};
     // per-phase timing
     bool prof = false;
@@ -80,6 +84,12 @@ struct cg_ctx {
     void *Z = nullptr;  // preconditioned basis z_j = M(v_j), restart + 1 vectors
     size_t zcap_bytes = 0;
 };
+
+namespace cg {
+void ctx_set_shared_gpu(cg_ctx *c, bool on) {
+    if (c) c->shared_gpu = on;
+}
+}  // namespace cg
 
 namespace {
 
@@ -387,7 +397,8 @@ int autotune(cg_ctx *c, int prec) {
     }
     // the key carries the tuner's version so that choices made by an older
     // tuner or for older kernels are not reused
-    std::string key = std::string(c->devname) + "|" + std::to_string(c->L) + "|" + std::to_string(prec) + "|t2";
+    std::string key = std::string(c->devname) + "|" + std::to_string(c->L) + "|" + std::to_string(prec) + "|t2" +
+                      (c->shared_gpu ? "s" : "");
     for (char &ch : key)
         if (ch == ' ') ch = '_';
     {
@@ -449,7 +460,7 @@ int autotune(cg_ctx *c, int prec) {
         bool changed = false;
         for (int pass = 0; pass < 3 && status == CG_OK; pass++)
             for (int v = 0; v < nv && status == CG_OK; v++) {
-                if (v == best[pass]) continue;
+                if (v == best[pass] || (c->shared_gpu && matvec_variant_persistent(v))) continue;
                 std::array<int, 3> cand = best;
                 cand[pass] = v;
                 const float ms = time_shapes(cand);

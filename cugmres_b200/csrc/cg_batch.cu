@@ -9,7 +9,10 @@
 // fill the GPU next to the large ones and each context reuses its buffers for
 // consecutive systems of the same size.  The operator set-up, the autotuned
 // launch shapes (cached per device and embedding size) and the solve are the
-// single-system paths; results are per system.
+// single-system paths; results are per system.  With more than one worker the
+// contexts are marked as sharing the GPU, so their autotuner leaves out the
+// persistent column pass (one block of ~200 KB shared memory on every SM,
+// which would make the other workers' kernels wait).
 #include <algorithm>
 #include <atomic>
 #include <thread>
@@ -17,6 +20,7 @@
 #include <vector>
 
 #include "../../include/cugmres.h"
+#include "cg_internal.h"
 
 namespace {
 
@@ -48,6 +52,7 @@ extern "C" int cugmres_solve_batch(int device, int nsys, const cg_system *sys, c
             fatal = st;
             return;
         }
+        if (nw > 1) cg::ctx_set_shared_gpu(ctx, true);
         for (;;) {
             const int q = next.fetch_add(1);
             if (q >= nsys) break;

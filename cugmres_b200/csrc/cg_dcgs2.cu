@@ -830,10 +830,11 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 // ------------------------------------------------------------- launchers
 // Shapes of the two streaming passes.  Dot pass: 0-4 = (J, U) of the
 // group-major k_dots2, 5, 6 = tile-major k_dots2t with U = 4, 8, 7, 8 = split
-// k_dots2s with U = 8, 4, 9 = tile-major with U = 16 for FP32 (8 for FP64).
+// k_dots2s with U = 8, 4, 9 = tile-major with U = 16 for FP32 (8 for FP64),
+// 10 = tile-major with U = 14 for FP32 (7 for FP64).
 // Axpy pass: 0-2 = j-unroll 4, 2, 8 of the element-major k_axpy2, 3, 4 =
 // tile-major k_axpy2t with U = 4, 8, 5, 6 = split k_axpy2s with U = 4, 2,
-// 7 = tile-major with U = 16 for FP32 (8 for FP64).  Measured on B200:
+// 7, 8 = tile-major with U = 16, 14 for FP32 (8, 7 for FP64).  Measured on B200:
 //   N = 1024, restart 100 (300 steps, k = 0..99), ms per 300 steps:
 //     FP64 dots 91.6 (shape 0), 81.0 (4), 59.4 (5), 54.3 (6, 4.9 TB/s)
 //     FP32 dots 97.6 (0), 78.8 (1), 50.0 (5), 38.3 (6)
@@ -843,8 +844,8 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 //     256 x 256 unrestarted mixed 1.754 / 0.912 / 2.120 s
 //     96 x 96 GMRES(200) FP64 (180 steps) 30.6 / 18.9 / 27.9 ms
 //     512 x 512 GMRES(200) FP64 (1000 steps) 0.381 / 0.254 / 0.327 s
-// Defaults: (6, 4) on grids with tile_major(n) ((9, 4) for FP32 where 16-point
-// tiles fill the GPU), (7, 5) below.
+// Defaults: tile-major on grids with tile_major(n), widths by balanced(),
+// split (7, 5) below.
 // CUGMRES_DOTS2_SHAPE / CUGMRES_AXPY2_SHAPE override them (diagnostics).
 static int env_shape(const char *name, int nshapes) {
     const char *e = getenv(name);
@@ -858,23 +859,36 @@ static int env_shape(const char *name, int nshapes) {
 // split passes, whose warps share the basis vectors of one tile.  Measured
 // ms per step at restart 100, tile / split: 512^2 0.179 / 0.153, 768^2
 // 0.303 / 0.321, 1024^2 0.442 / 0.465.
-// FP32 vectors: on grids with enough 16-point tiles for the same rule, the dot
-// pass takes 16 points per lane (shape 9), the bytes of an FP64 tile per warp
-// reduction; measured at 1024^2 mixed GMRES(100): dots 97.8 -> 86.3 ms per
-// 1000 steps (4.5 -> 5.1 TB/s).  The 16-point FP32 axpy spills and is slower.
-static bool tile_major(long long n, int sms, int U = 8) {
-    return 4 * n >= 3LL * sms * 2 * (D2_THREADS / 32) * 32 * U;
+static bool tile_major(long long n, int sms) { return 4 * n >= 3LL * sms * 2 * (D2_THREADS / 32) * 32 * 8; }
+// Tile width of the tile-major passes: of two instantiated widths U (points
+// per lane), the one whose busiest warp streams fewer elements, i.e. the
+// smaller ceil(tiles / resident warps) * U, ties to the first.  The resident
+// warps are two 8-warp blocks per SM.  At n = 2^20 on 148 SMs, U = 8 gives
+// 4096 tiles over 2368 warps (the second round 73 % full) and U = 7 gives
+// 4682 (99 %); measured at 1024^2, ms per 1000 steps: FP64 dots 150.7 (U = 8)
+// -> 142.2 (U = 7), FP64 axpy 140.1 -> 138.0, FP32 dots 97.8 (U = 8) -> 86.8
+// (U = 16) -> 83.5 (U = 14), FP32 axpy 82.2 (U = 8) -> 78.4 (U = 14); at
+// 2048^2 FP32 dots 34.3 (U = 16) -> 32.3 (U = 14), FP32 axpy 32.0 (U = 8)
+// against 32.7 (U = 14, a tie by the rule).
+static int balanced(long long n, int sms, int va, int Ua, int vb, int Ub) {
+    const long long nw = 2LL * sms * (D2_THREADS / 32);
+    auto cost = [&](int U) {
+        const long long tiles = (n + 32LL * U - 1) / (32LL * U);
+        return (tiles + nw - 1) / nw * U;
+    };
+    return cost(Ub) < cost(Ua) ? vb : va;
 }
 static int dots2_shape(int prec_v, long long n, int sms) {
-    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 10);
+    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 11);
     if (v >= 0) return v;
     if (!tile_major(n, sms)) return 7;
-    return (prec_v != 0 && tile_major(n, sms, 16)) ? 9 : 6;
+    return prec_v == 0 ? balanced(n, sms, 6, 8, 10, 7) : balanced(n, sms, 9, 16, 10, 14);
 }
-static int axpy2_shape(int, long long n, int sms) {
-    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 8);
+static int axpy2_shape(int prec_v, long long n, int sms) {
+    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 9);
     if (v >= 0) return v;
-    return tile_major(n, sms) ? 4 : 5;
+    if (!tile_major(n, sms)) return 5;
+    return prec_v == 0 ? balanced(n, sms, 4, 8, 8, 7) : balanced(n, sms, 4, 8, 8, 14);
 }
 
 template <typename CV, bool COMP> struct Dots2Table {
@@ -892,6 +906,9 @@ template <typename CV, bool COMP> struct Dots2Table {
             case 9:  // 16 points per lane: the FP64 tile's bytes for FP32 vectors
                 if constexpr (sizeof(CV) == 8) return k_dots2t<CV, 16>;
                 else return k_dots2t<CV, 8>;
+            case 10:  // 7 (FP64) / 14 (FP32) points per lane
+                if constexpr (sizeof(CV) == 8) return k_dots2t<CV, 14>;
+                else return k_dots2t<CV, 7>;
             default: return k_dots2<CV, COMP, 4, 2>;
         }
     }
@@ -909,6 +926,9 @@ template <typename CV> struct Axpy2Table {
             case 7:  // 16 points per lane for FP32 vectors
                 if constexpr (sizeof(CV) == 8) return k_axpy2t<CV, 16>;
                 else return k_axpy2t<CV, 8>;
+            case 8:  // 7 (FP64) / 14 (FP32) points per lane
+                if constexpr (sizeof(CV) == 8) return k_axpy2t<CV, 14>;
+                else return k_axpy2t<CV, 7>;
             default: return k_axpy2<CV, 4>;
         }
     }
@@ -918,7 +938,7 @@ template <typename CV> struct Axpy2Table {
 // (tile-major) or one slot per coefficient (split), for chunks of cs vectors.
 static size_t dots2_smem(int v, int mcap) {
     const int jc = mcap + 1 < D2T_CHUNK ? mcap + 1 : D2T_CHUNK;
-    if (v == 5 || v == 6 || v == 9) return (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double);
+    if (v == 5 || v == 6 || v == 9 || v == 10) return (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double);
     if (v == 7 || v == 8) return (size_t)jc * 4 * sizeof(double);
     return 0;
 }
@@ -942,8 +962,8 @@ int dots2_blocks(int prec_v, int sms, int mcap, long long n) {
     const size_t smem = dots2_smem(v, mcap);
     int g = prec_v == 0 ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
                         : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
-    if (v >= 5 && v <= 9) {
-        const int U = (v == 5 || v == 8) ? 4 : (v == 9 && prec_v != 0) ? 16 : 8;
+    if (v >= 5 && v <= 10) {
+        const int U = (v == 5 || v == 8) ? 4 : v == 10 ? (prec_v != 0 ? 14 : 7) : (v == 9 && prec_v != 0) ? 16 : 8;
         const long long cap = work_blocks(v == 7 || v == 8, U, n);
         if (cap < g) g = (int)cap;
     }
@@ -996,8 +1016,9 @@ int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
         axpy2_prepare<float2>(v, smem);
         g = waves_grid(Axpy2Table<float2>::get(v), AX2_THREADS, smem, sms);
     }
-    if (v >= 3 && v <= 7) {
-        const int U = (v == 3 || v == 5) ? 4 : v == 4 ? 8 : v == 6 ? 2 : (prec_v != 0 ? 16 : 8);
+    if (v >= 3 && v <= 8) {
+        const int U = (v == 3 || v == 5) ? 4 : v == 4 ? 8 : v == 6 ? 2 : v == 8 ? (prec_v != 0 ? 14 : 7)
+                                                                                 : (prec_v != 0 ? 16 : 8);
         const long long cap = work_blocks(v == 5 || v == 6, U, n);
         if (cap < g) g = (int)cap;
     }

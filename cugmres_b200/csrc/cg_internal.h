@@ -6,6 +6,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+struct cg_ctx;  // solver context (cg_api.cu)
+
 namespace cg {
 
 // Solver state kept in device memory so that no host synchronisation is
@@ -93,6 +95,12 @@ int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, V
 int rows_per_block(int variant, int L);
 int fft_supported(int L);
 int matvec_variants(int L);
+// 1 if launch shape v runs the column pass as a persistent kernel (one block
+// of about 200 KB shared memory on every SM)
+int matvec_variant_persistent(int v);
+// marks a context whose GPU is shared with other contexts' solves (set by the
+// batch solver before its first operator)
+void ctx_set_shared_gpu(cg_ctx *c, bool on);
 
 // full (unpruned) forward 2D transform of an L x L FP64 array, used to build the spectrum
 int launch_fft2d_full_fp64(int L, double2 *a, const double2 *tw, cudaStream_t s);

@@ -506,6 +506,8 @@ int fft_supported(int L) {
 
 int matvec_variants(int L) { return L >= 128 ? MV_VARIANTS : 1; }
 
+int matvec_variant_persistent(int v) { return v == 5 || v == 6; }
+
 int rows_per_block(int variant, int L) { return dispatch<RpcF>(variant, L); }
 
 int launch_rows_forward(int prec, const MatvecArgs &a, VecSel x, const double *xs, const DevState *st, int gate,
