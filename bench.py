@@ -374,7 +374,7 @@ def main():
     # DRAM traffic per launch of the dominant kernel: ncu (dram__bytes_read.sum + dram__bytes_write.sum)
     # of one launch at step k = 30 of the 1024^2 FP64 solve, as a ratio to that launch's algorithmic
     # bytes, applied to this run's mean algorithmic bytes per launch (profiles/dcgs2_passes_1024x1024_k30.md)
-    ncu_ratio = {"dots": (536.909 + 4.744) / 536.871, "axpy": (536.917 + 7.709) / 570.425}
+    ncu_ratio = {"dots": (536.904 + 4.625) / 536.871, "axpy": (536.961 + 8.369) / 570.425}
     launches = max(1, dom[1].get("launches", 0))
     alg_per_launch = dom[1].get("bytes", 0.0) / launches
     traffic = ncu_ratio[dom[0]] * alg_per_launch if dom[0] in ncu_ratio and alg_per_launch > 0 else None
