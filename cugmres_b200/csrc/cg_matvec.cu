@@ -26,7 +26,7 @@
 //
 // Launch shapes (points per thread, threads per block, resident blocks per SM
 // requested from the compiler, pipelined column pass) are template parameters;
-// the MvShape variants 0..6 are instantiated for L >= 128 and the autotuner in cg_api.cu picks one
+// the MvShape variants 0..7 are instantiated for L >= 128 and the autotuner in cg_api.cu picks one
 // per (precision, L); smaller L always use variant 0.
 #include "cg_fft.cuh"
 #include "cg_internal.h"
@@ -55,7 +55,14 @@ typedef MvShape<8, 256, 256, 256, 2> MvV3;      // 8 points, two blocks per SM
 typedef MvShape<8, 64, 64, 64, 4> MvV4;         // 8 points, small blocks (many blocks on small grids)
 typedef MvShape<16, 256, 256, 512, 1, 1> MvV5;  // V0 with the pipelined column pass
 typedef MvShape<8, 256, 512, 512, 1, 1> MvV6;   // V2 with the pipelined column pass
-constexpr int MV_VARIANTS = 7;
+// 16 points, smaller column blocks, two per SM (each block's barriers hold
+// only its own warps, so one block's shared-memory exchanges can overlap the
+// other's butterflies).  Measured at L = 2048 (ncu): FP32 column pass 30.3 us
+// against 32.6 us for V0 (two columns per 256-thread block); FP64 60.6 us
+// against 53.4 us (one column per 128-thread block: its loads use 16 of each
+// 32-byte sector of T).
+typedef MvShape<16, 256, 128, 256, 2> MvV7;
+constexpr int MV_VARIANTS = 8;
 
 template <int L, typename SH> struct RowCfg {
     typedef Plan<L, SH::E> P;
@@ -367,9 +374,9 @@ template <typename K> static int set_smem(K kern, size_t bytes) {
 }
 
 // The three passes for one launch shape SH and one embedding size L.
-// The row passes do not depend on PIPE: shapes that differ only in it share
-// one row-pass instantiation.
-template <typename SH> using RowShape = MvShape<SH::E, SH::ROWT, SH::COLT64, SH::COLT32, SH::MINB, 0>;
+// The row passes do not depend on the column fields (COLT64, COLT32, PIPE):
+// shapes that differ only in them share one row-pass instantiation.
+template <typename SH> using RowShape = MvShape<SH::E, SH::ROWT, 0, 0, SH::MINB, 0>;
 
 template <typename SH0, int L> struct Passes {
     typedef RowShape<SH0> SH;  // row passes
@@ -474,6 +481,7 @@ template <template <typename> class F, typename... A> static int dispatch(int va
         case 4: CG_V_CASES(MvV4)
         case 5: CG_V_CASES(MvV5)
         case 6: CG_V_CASES(MvV6)
+        case 7: CG_V_CASES(MvV7)
         default: return -1;
     }
 #undef CG_V_CASES
