@@ -49,6 +49,43 @@ template <typename K> static int waves_grid(K kern, int threads, size_t smem, in
     return per_sm * sms;
 }
 
+// Two FP32 complex values (re0, im0, re1, im1) moved by one 16-byte access:
+// the load unit of the FP32 tile-major passes on vectors of even length, so
+// that they issue as few load instructions per byte as the FP64 passes.
+template <> struct real_of<float4> { typedef float type; };
+template <typename CV> struct scalar_of { typedef CV type; };  // complex scalar of a load unit
+template <> struct scalar_of<float4> { typedef float2 type; };
+template <> __host__ __device__ __forceinline__ float4 czero<float4>() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+__device__ __forceinline__ float4 cadd(float4 a, float4 b) {
+    return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w);
+}
+__device__ __forceinline__ float4 csub(float4 a, float4 b) {
+    return make_float4(a.x - b.x, a.y - b.y, a.z - b.z, a.w - b.w);
+}
+__device__ __forceinline__ float4 cscale(float4 a, float s) { return make_float4(a.x * s, a.y * s, a.z * s, a.w * s); }
+__device__ __forceinline__ float4 cmul(float2 p, float4 a) {
+    return make_float4(p.x * a.x - p.y * a.y, p.x * a.y + p.y * a.x, p.x * a.z - p.y * a.w, p.x * a.w + p.y * a.z);
+}
+// s0 + i s1 += conj(a) u, s2 + i s3 += conj(a) w over the complex values of a load unit
+__device__ __forceinline__ void dacc(double2 a, double2 u, double2 w, double &s0, double &s1, double &s2, double &s3) {
+    s0 += a.x * u.x + a.y * u.y;
+    s1 += a.x * u.y - a.y * u.x;
+    s2 += a.x * w.x + a.y * w.y;
+    s3 += a.x * w.y - a.y * w.x;
+}
+__device__ __forceinline__ void dacc(float2 a, float2 u, float2 w, float &s0, float &s1, float &s2, float &s3) {
+    s0 += a.x * u.x + a.y * u.y;
+    s1 += a.x * u.y - a.y * u.x;
+    s2 += a.x * w.x + a.y * w.y;
+    s3 += a.x * w.y - a.y * w.x;
+}
+__device__ __forceinline__ void dacc(float4 a, float4 u, float4 w, float &s0, float &s1, float &s2, float &s3) {
+    s0 += (a.x * u.x + a.y * u.y) + (a.z * u.z + a.w * u.w);
+    s1 += (a.x * u.y - a.y * u.x) + (a.z * u.w - a.w * u.z);
+    s2 += (a.x * w.x + a.y * w.y) + (a.z * w.z + a.w * w.w);
+    s3 += (a.x * w.y - a.y * w.x) + (a.z * w.w - a.w * w.z);
+}
+
 static __device__ __forceinline__ int part_ld(const KrylovPtrs &kp) { return dots2_part_ld(kp.mcap); }
 
 static __device__ __forceinline__ bool last_block2(unsigned int *ticket) {
@@ -167,25 +204,20 @@ __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__
             for (int t = 0; t < U; t++) {
                 const long long e = e0 + 32 * t;
                 const bool ok = full || e < n;
-                uu[t] = ok ? u[e] : mk<CV>(0, 0);
-                ww[t] = ok ? w[e] : mk<CV>(0, 0);
-                a[t] = ok ? __ldcs(Vc + e) : mk<CV>(0, 0);
+                uu[t] = ok ? u[e] : czero<CV>();
+                ww[t] = ok ? w[e] : czero<CV>();
+                a[t] = ok ? __ldcs(Vc + e) : czero<CV>();
             }
             for (int j = 0; j < nj; j++) {
                 R s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
-                for (int t = 0; t < U; t++) {
-                    s0 += a[t].x * uu[t].x + a[t].y * uu[t].y;
-                    s1 += a[t].x * uu[t].y - a[t].y * uu[t].x;
-                    s2 += a[t].x * ww[t].x + a[t].y * ww[t].y;
-                    s3 += a[t].x * ww[t].y - a[t].y * ww[t].x;
-                }
+                for (int t = 0; t < U; t++) dacc(a[t], uu[t], ww[t], s0, s1, s2, s3);
                 if (j + 1 < nj) {  // next vector's tile in flight during the reduction
                     const CV *vn = Vc + (long long)(j + 1) * n;
 #pragma unroll
                     for (int t = 0; t < U; t++) {
                         const long long e = e0 + 32 * t;
-                        a[t] = (full || e < n) ? __ldcs(vn + e) : mk<CV>(0, 0);
+                        a[t] = (full || e < n) ? __ldcs(vn + e) : czero<CV>();
                     }
                 }
                 const double d = warp_sum4_scatter((double)s0, (double)s1, (double)s2, (double)s3, lane);
@@ -658,15 +690,16 @@ __device__ __forceinline__ void axpy2_prologue(const KrylovPtrs &kp, const DevSt
 template <typename CV, int U>
 __global__ void __launch_bounds__(AX2_THREADS, 2) k_axpy2t(CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
+    typedef typename scalar_of<CV>::type CS;
     DevState *st = kp.st;
     if (st->stop) return;
     const int k = st->k - 1;
     extern __shared__ __align__(16) unsigned char smraw[];
-    CV *Pc = reinterpret_cast<CV *>(smraw);
-    CV *Sc = Pc + (kp.mcap + 1);
-    axpy2_prologue<CV>(kp, st, k, Pc, Sc);
+    CS *Pc = reinterpret_cast<CS *>(smraw);
+    CS *Sc = Pc + (kp.mcap + 1);
+    axpy2_prologue<CS>(kp, st, k, Pc, Sc);
     const R cu = (R)st->cu, cw = (R)st->cw;
-    const CV du = mk<CV>((R)st->du.x, (R)st->du.y);
+    const CS du = mk<CS>((R)st->du.x, (R)st->du.y);
     CV *u = V + (long long)k * n;
     CV *w = V + (long long)(k + 1) * n;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -685,7 +718,7 @@ __global__ void __launch_bounds__(AX2_THREADS, 2) k_axpy2t(CV *__restrict__ V, l
             a[t] = (k > 0 && (full || e < n)) ? __ldcs(V + e) : czero<CV>();
         }
         for (int j = 0; j < k; j++) {
-            const CV p = Pc[j], q = Sc[j];
+            const CS p = Pc[j], q = Sc[j];
             CV nx[U];
             const bool more = j + 1 < k;
 #pragma unroll
@@ -831,10 +864,13 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long 
 // Shapes of the two streaming passes.  Dot pass: 0-4 = (J, U) of the
 // group-major k_dots2, 5, 6 = tile-major k_dots2t with U = 4, 8, 7, 8 = split
 // k_dots2s with U = 8, 4, 9 = tile-major with U = 16 for FP32 (8 for FP64),
-// 10 = tile-major with U = 14 for FP32 (7 for FP64).
+// 10 = tile-major with U = 14 for FP32 (7 for FP64), 11, 12 = FP32 tile-major
+// on 16-byte pairs (float4 loads) with 16, 14 points per lane (even n; FP64: 6, 10).
 // Axpy pass: 0-2 = j-unroll 4, 2, 8 of the element-major k_axpy2, 3, 4 =
 // tile-major k_axpy2t with U = 4, 8, 5, 6 = split k_axpy2s with U = 4, 2,
-// 7, 8 = tile-major with U = 16, 14 for FP32 (8, 7 for FP64).  Measured on B200:
+// 7, 8 = tile-major with U = 16, 14 for FP32 (8, 7 for FP64), 9, 10 = FP32
+// tile-major on 16-byte pairs with 8, 14 points per lane (even n; FP64: 4, 8).
+// Measured on B200:
 //   N = 1024, restart 100 (300 steps, k = 0..99), ms per 300 steps:
 //     FP64 dots 91.6 (shape 0), 81.0 (4), 59.4 (5), 54.3 (6, 4.9 TB/s)
 //     FP32 dots 97.6 (0), 78.8 (1), 50.0 (5), 38.3 (6)
@@ -879,16 +915,18 @@ static int balanced(long long n, int sms, int va, int Ua, int vb, int Ub) {
     return cost(Ub) < cost(Ua) ? vb : va;
 }
 static int dots2_shape(int prec_v, long long n, int sms) {
-    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 11);
+    static const int v = env_shape("CUGMRES_DOTS2_SHAPE", 13);
     if (v >= 0) return v;
     if (!tile_major(n, sms)) return 7;
-    return prec_v == 0 ? balanced(n, sms, 6, 8, 10, 7) : balanced(n, sms, 9, 16, 10, 14);
+    if (prec_v == 0) return balanced(n, sms, 6, 8, 10, 7);
+    return n % 2 == 0 ? balanced(n, sms, 11, 16, 12, 14) : balanced(n, sms, 9, 16, 10, 14);
 }
 static int axpy2_shape(int prec_v, long long n, int sms) {
-    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 9);
+    static const int v = env_shape("CUGMRES_AXPY2_SHAPE", 11);
     if (v >= 0) return v;
     if (!tile_major(n, sms)) return 5;
-    return prec_v == 0 ? balanced(n, sms, 4, 8, 8, 7) : balanced(n, sms, 4, 8, 8, 14);
+    if (prec_v == 0) return balanced(n, sms, 4, 8, 8, 7);
+    return n % 2 == 0 ? balanced(n, sms, 9, 8, 10, 14) : balanced(n, sms, 4, 8, 8, 14);
 }
 
 template <typename CV, bool COMP> struct Dots2Table {
@@ -907,6 +945,14 @@ template <typename CV, bool COMP> struct Dots2Table {
                 if constexpr (sizeof(CV) == 8) return k_dots2t<CV, 16>;
                 else return k_dots2t<CV, 8>;
             case 10:  // 7 (FP64) / 14 (FP32) points per lane
+                if constexpr (sizeof(CV) == 8) return k_dots2t<CV, 14>;
+                else return k_dots2t<CV, 7>;
+            // 11, 12: FP32 on even lengths runs k_dots2t<float4, 8 / 7> (dots2_vec_kernel);
+            // the same widths in complex values otherwise
+            case 11:
+                if constexpr (sizeof(CV) == 8) return k_dots2t<CV, 16>;
+                else return k_dots2t<CV, 8>;
+            case 12:
                 if constexpr (sizeof(CV) == 8) return k_dots2t<CV, 14>;
                 else return k_dots2t<CV, 7>;
             default: return k_dots2<CV, COMP, 4, 2>;
@@ -929,6 +975,12 @@ template <typename CV> struct Axpy2Table {
             case 8:  // 7 (FP64) / 14 (FP32) points per lane
                 if constexpr (sizeof(CV) == 8) return k_axpy2t<CV, 14>;
                 else return k_axpy2t<CV, 7>;
+            // 9, 10: FP32 on even lengths runs k_axpy2t<float4, 4 / 7> (axpy2_vec_kernel);
+            // the same widths in complex values otherwise
+            case 9: return k_axpy2t<CV, 8>;
+            case 10:
+                if constexpr (sizeof(CV) == 8) return k_axpy2t<CV, 14>;
+                else return k_axpy2t<CV, 7>;
             default: return k_axpy2<CV, 4>;
         }
     }
@@ -938,9 +990,25 @@ template <typename CV> struct Axpy2Table {
 // (tile-major) or one slot per coefficient (split), for chunks of cs vectors.
 static size_t dots2_smem(int v, int mcap) {
     const int jc = mcap + 1 < D2T_CHUNK ? mcap + 1 : D2T_CHUNK;
-    if (v == 5 || v == 6 || v == 9 || v == 10) return (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double);
+    if (v == 5 || v == 6 || (v >= 9 && v <= 12)) return (size_t)D2_WARPS * (size_t)jc * 4 * sizeof(double);
     if (v == 7 || v == 8) return (size_t)jc * 4 * sizeof(double);
     return 0;
+}
+
+// FP32 tile-major shapes on 16-byte pairs of complex values (even n only)
+static bool dots2_vec(int prec_v, long long n, int v) { return prec_v != 0 && n % 2 == 0 && (v == 11 || v == 12); }
+static bool axpy2_vec(int prec_v, long long n, int v) { return prec_v != 0 && n % 2 == 0 && (v == 9 || v == 10); }
+typedef void (*DotsVecK)(const float4 *, long long, KrylovPtrs);
+typedef void (*AxpyVecK)(float4 *, long long, KrylovPtrs);
+static DotsVecK dots2_vec_kernel(int v, size_t smem) {
+    DotsVecK kern = v == 11 ? k_dots2t<float4, 8> : k_dots2t<float4, 7>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return kern;
+}
+static AxpyVecK axpy2_vec_kernel(int v, size_t smem) {
+    AxpyVecK kern = v == 9 ? k_axpy2t<float4, 4> : k_axpy2t<float4, 7>;
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    return kern;
 }
 
 template <typename CV, bool COMP> static typename Dots2Table<CV, COMP>::K dots2_kernel(int v, size_t smem) {
@@ -960,10 +1028,14 @@ static long long work_blocks(bool split, int U, long long n) {
 int dots2_blocks(int prec_v, int sms, int mcap, long long n) {
     const int v = dots2_shape(prec_v, n, sms);
     const size_t smem = dots2_smem(v, mcap);
-    int g = prec_v == 0 ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
-                        : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
-    if (v >= 5 && v <= 10) {
-        const int U = (v == 5 || v == 8) ? 4 : v == 10 ? (prec_v != 0 ? 14 : 7) : (v == 9 && prec_v != 0) ? 16 : 8;
+    int g = dots2_vec(prec_v, n, v) ? waves_grid(dots2_vec_kernel(v, smem), D2_THREADS, smem, sms)
+            : prec_v == 0           ? waves_grid(dots2_kernel<double2, false>(v, smem), D2_THREADS, smem, sms)
+                                    : waves_grid(dots2_kernel<float2, true>(v, smem), D2_THREADS, smem, sms);
+    if (v >= 5 && v <= 12) {
+        // points per lane, in complex values
+        const int U = (v == 5 || v == 8) ? 4
+                      : (v == 10 || v == 12) ? (prec_v != 0 ? 14 : 7)
+                      : ((v == 9 || v == 11) && prec_v != 0) ? 16 : 8;
         const long long cap = work_blocks(v == 7 || v == 8, U, n);
         if (cap < g) g = (int)cap;
     }
@@ -973,7 +1045,8 @@ int dots2_blocks(int prec_v, int sms, int mcap, long long n) {
 int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
     const int v = dots2_shape(prec_v, n, sms);
     const size_t smem = dots2_smem(v, kp.mcap);
-    if (prec_v == 0) dots2_kernel<double2, false>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const double2 *)V, n, kp);
+    if (dots2_vec(prec_v, n, v)) dots2_vec_kernel(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const float4 *)V, n / 2, kp);
+    else if (prec_v == 0) dots2_kernel<double2, false>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const double2 *)V, n, kp);
     else dots2_kernel<float2, true>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const float2 *)V, n, kp);
     return (int)cudaGetLastError();
 }
@@ -1009,16 +1082,22 @@ int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
     const int v = axpy2_shape(prec_v, n, sms);
     const size_t smem = axpy2_smem(v, prec_v, mcap);
     int g;
-    if (prec_v == 0) {
+    if (axpy2_vec(prec_v, n, v)) {
+        g = waves_grid(axpy2_vec_kernel(v, smem), AX2_THREADS, smem, sms);
+    } else if (prec_v == 0) {
         axpy2_prepare<double2>(v, smem);
         g = waves_grid(Axpy2Table<double2>::get(v), AX2_THREADS, smem, sms);
     } else {
         axpy2_prepare<float2>(v, smem);
         g = waves_grid(Axpy2Table<float2>::get(v), AX2_THREADS, smem, sms);
     }
-    if (v >= 3 && v <= 8) {
-        const int U = (v == 3 || v == 5) ? 4 : v == 4 ? 8 : v == 6 ? 2 : v == 8 ? (prec_v != 0 ? 14 : 7)
-                                                                                 : (prec_v != 0 ? 16 : 8);
+    if (v >= 3 && v <= 10) {
+        // points per lane, in complex values
+        const int U = (v == 3 || v == 5) ? 4
+                      : (v == 4 || v == 9) ? 8
+                      : v == 6 ? 2
+                      : (v == 8 || v == 10) ? (prec_v != 0 ? 14 : 7)
+                                            : (prec_v != 0 ? 16 : 8);
         const long long cap = work_blocks(v == 5 || v == 6, U, n);
         if (cap < g) g = (int)cap;
     }
@@ -1028,6 +1107,10 @@ int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
 int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
     const int v = axpy2_shape(prec_v, n, sms);
     const size_t smem = axpy2_smem(v, prec_v, kp.mcap);
+    if (axpy2_vec(prec_v, n, v)) {
+        axpy2_vec_kernel(v, smem)<<<nblk, AX2_THREADS, smem, s>>>((float4 *)V, n / 2, kp);
+        return (int)cudaGetLastError();
+    }
     int e = prec_v == 0 ? axpy2_prepare<double2>(v, smem) : axpy2_prepare<float2>(v, smem);
     if (e) return e;
     if (prec_v == 0) Axpy2Table<double2>::get(v)<<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);

@@ -1,8 +1,10 @@
 """Every launch shape of the two DCGS2 streaming passes (dot pass and axpy
 pass, selected with CUGMRES_DOTS2_SHAPE / CUGMRES_AXPY2_SHAPE) gives the same
 solve as the default shapes: group-major, tile-major (8, 7, 16 and 14 points
-per lane) and split kernels, on grids whose size is not a multiple of any
-tile (n = 96^2 and 150^2), in FP64 and mixed precision."""
+per lane; FP32 also on 16-byte pairs of complex values) and split kernels, on
+grids whose size is not a multiple of any tile (n = 96^2, 97^2 (odd: the
+FP32 pair shapes fall back to single values) and 150^2), in FP64 and mixed
+precision."""
 import os
 import subprocess
 import sys
@@ -20,7 +22,7 @@ sys.path.insert(0, sys.argv[1])
 import cugmres_b200 as cg
 from cugmres_b200 import problems as P
 out = {}
-for N, eps in ((96, 2.0), (150, 2.0)):
+for N, eps in ((96, 2.0), (97, 2.0), (150, 2.0)):
     pr = P.helmholtz(N, eps, seed=N)
     s = cg.Solver(0).set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
     for prec in ("fp64", "mixed"):
@@ -33,8 +35,8 @@ for N, eps in ((96, 2.0), (150, 2.0)):
 np.savez(sys.argv[2], **out)
 """
 
-DOTS = [str(v) for v in range(11)]
-AXPY = [str(v) for v in range(9)]
+DOTS = [str(v) for v in range(13)]
+AXPY = [str(v) for v in range(11)]
 
 
 def _run(tmp_path, name, env_extra):
@@ -54,7 +56,7 @@ def default_run(tmp_path_factory, cuda_device):
 
 
 def _compare(got, ref):
-    for N in (96, 150):
+    for N in (96, 97, 150):
         for prec in ("fp64", "mixed"):
             assert got[f"res_{N}_{prec}"] <= 1e-10
             assert abs(int(got[f"it_{N}_{prec}"]) - int(ref[f"it_{N}_{prec}"])) <= 1, (N, prec)
