@@ -965,8 +965,10 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     h.inner_tol = prec == 1 ? o.inner_tol : 0.0;
     // the flexible variant stores z_j explicitly, so it uses the CGS2 path (the delayed
     // reorthogonalisation would need A M(.) to be linear)
+    // (flexible GMRES: preconditioned cycles CGS2, plain cycles the requested scheme)
     h.ortho = (o.ortho == CG_ORTHO_CGS2 || learned) ? 1 : 0;
-    const bool delayed = h.ortho == 0;
+    const bool want_delayed = o.ortho == CG_ORTHO_DCGS2;
+    bool delayed = h.ortho == 0;  // scheme of the cycle being enqueued
     *c->st_host = h;
     CG_CU(cudaMemcpyAsync(c->st, c->st_host, sizeof(DevState), cudaMemcpyHostToDevice, s));
     CG_LAUNCH(launch_norm2(0, bp, n, c->kp.npart, &c->st->counter[2], &c->st->nb, axpy_blocks(c, n), s));
@@ -993,6 +995,12 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     // afterwards each cycle uses the mode whose last cycle cut the true residual
     // faster per second (log reduction / wall time); a preconditioned cycle that
     // does not reduce it at all switches to plain GMRES for the rest of the solve.
+    // Preconditioned cycles, and the plain probe, last at most LEARNED_CYCLE_STEPS
+    // steps: each preconditioned cycle refreshes the measured rate, so a choice
+    // that the first (easiest) cycle biased towards the network costs at most
+    // that many expensive steps, and a long restart or an unrestarted solve does
+    // not spend its budget on the network before the modes are compared.
+    constexpr int LEARNED_CYCLE_STEPS = 40;
     double rate_prec = -1.0, rate_plain = -1.0;  // < 0: not measured yet
     bool cycle_open = false, last_prec = false, prec_failed = false;
     double cycle_t0 = 0.0, cycle_res0 = 0.0;
@@ -1067,10 +1075,12 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     };
     // Graph replay of [cycle + next residual/decisions] when nothing in it
     // changes between cycles (not while profiling, not with the network).
-    const bool graphs = !c->prof && !learned && graphs_enabled();
+    // (flexible GMRES: plain cycles after the probe only)
+    const bool graphs = !c->prof && graphs_enabled();
     unsigned char key[256];
-    memset(key, 0, sizeof(key));
-    {
+    // key of the cycle about to be replayed (the scheme can change between cycles)
+    auto make_key = [&]() {
+        memset(key, 0, sizeof(key));
         struct K {
             int prec, delayed, m, transpose, ndot, nax, ndot2, nax2, nrb, mcap, var[2][3];
             long long n;
@@ -1083,8 +1093,9 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         kk.V = c->V, kk.x = xp, kk.b = bp, kk.st = c->st, kk.scale = kp.scale, kk.part = kp.part;
         static_assert(sizeof(K) <= sizeof(key), "graph key");
         memcpy(key, &kk, sizeof(kk));
-    }
+    };
     auto launch_cycle_graph = [&]() -> int {
+        make_key();
         if (!c->gexec || memcmp(c->gkey, key, sizeof(key)) != 0) {
             free_graph(c);
             if (!c->cap_stream) CG_CU(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
@@ -1160,10 +1171,17 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         last_prec = use_prec;
         cycle_t0 = now_s();
         cycle_res0 = hs.true_res;
-        if (graphs) {
+        if (learned) {
+            const bool d = want_delayed && !use_prec;
+            if (d != delayed) CG_LAUNCH(launch_set_ortho(kp, d ? 0 : 1, s));
+            delayed = d;
+        }
+        if (graphs && !use_prec && !(learned && rate_plain < 0.0)) {
             CG_TRY(launch_cycle_graph());
         } else {
-            CG_TRY(enqueue_cycle(std::min(m, o.max_iter - hs.it) + (delayed ? 1 : 0), s));
+            int len = std::min(m, o.max_iter - hs.it);
+            if (learned && (use_prec || rate_plain < 0.0)) len = std::min(len, LEARNED_CYCLE_STEPS);
+            CG_TRY(enqueue_cycle(len + (delayed ? 1 : 0), s));
             CG_TRY(prof_mark(c, cp, -1, -1, s));
             CG_TRY(enqueue_begin(s));
         }

@@ -123,6 +123,8 @@ int axpy2_blocks(int prec_v, int sms, int mcap, long long n);
 __host__ __device__ inline int dots2_part_ld(int mcap) { return 2 * (mcap + 1) > 64 ? 2 * (mcap + 1) : 64; }
 int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s);
 int launch_cycle_begin(const KrylovPtrs &kp, int nparts, cudaStream_t s);
+// ortho 0: delayed CGS2, 1: CGS2, for the cycle k_cycle_begin has just set up
+int launch_set_ortho(const KrylovPtrs &kp, int ortho, cudaStream_t s);
 int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
                  cudaStream_t s);
 int launch_convert(int from_prec, int to_prec, const void *src, void *dst, long long n, cudaStream_t s);

@@ -435,6 +435,21 @@ int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s) {
     return (int)cudaGetLastError();
 }
 
+// Switches the orthogonalisation mode of the cycle that k_cycle_begin has just
+// set up (flexible GMRES alternates preconditioned CGS2 cycles with plain
+// delayed-CGS2 cycles): the only mode-specific part of a cycle's start is the
+// lazy normalisation of V_0 that CGS2 keeps in scale[0].
+__global__ void k_set_ortho(KrylovPtrs kp, int ortho) {
+    DevState *st = kp.st;
+    st->ortho = ortho;
+    if (!st->stop) kp.scale[0] = ortho == 1 ? 1.0 / st->beta0 : 1.0;
+}
+
+int launch_set_ortho(const KrylovPtrs &kp, int ortho, cudaStream_t s) {
+    k_set_ortho<<<1, 1, 0, s>>>(kp, ortho);
+    return (int)cudaGetLastError();
+}
+
 int launch_cycle_begin(const KrylovPtrs &kp, int nparts, cudaStream_t s) {
     k_cycle_begin<<<1, 32, 0, s>>>(kp, nparts);
     return (int)cudaGetLastError();

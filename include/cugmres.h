@@ -86,7 +86,11 @@ typedef struct {
                              tol is an absolute threshold on ||b - A x0|| only                 */
     double timeout_s;   /* <= 0: none; otherwise the solve returns CG_ERR_TIMEOUT after this    */
     int ortho;          /* CG_ORTHO_*                                                          */
-    int preconditioner; /* CG_PRECOND_*; CG_PRECOND_LEARNED needs cugmres_set_preconditioner  */
+    int preconditioner; /* CG_PRECOND_*; CG_PRECOND_LEARNED needs cugmres_set_preconditioner;
+                           flexible GMRES: a preconditioned and a plain probe cycle, then every
+                           cycle in the mode that last reduced the true residual faster per
+                           second (plain for good once a preconditioned cycle fails to reduce
+                           it); preconditioned cycles last at most 40 steps                 */
     int learned_x0;     /* 1: with a preconditioner attached and zero_x0, start from x0 = M(b)
                            (kept only if ||b - A x0|| < ||b||, otherwise x0 = 0)             */
     int transpose;      /* 1: solve A^T x = b, A^T = I - diag(c) G (the adjoint system of the
