@@ -1,4 +1,6 @@
-"""Every matvec launch shape the autotuner may pick gives the same operator."""
+"""Every matvec launch shape the autotuner may pick gives the same operator
+(A in FP64 and FP32, and the transposed operator A^T), for embeddings L = 128
+to 4096."""
 import os
 import subprocess
 import sys
@@ -25,8 +27,11 @@ for N in (64, 128, 300, 512, 1100):
     e64 = np.abs(y - yo).max() / np.abs(yo).max()
     y32 = s.matvec(x.astype(np.complex64), precision="fp32")
     e32 = np.abs(y32 - yo).max() / np.abs(yo).max()
-    print(N, s.matvec_shapes("fp64"), s.matvec_shapes("fp32"), e64, e32)
-    assert e64 < 1e-13 and e32 < 2e-6, (e64, e32)
+    yt = s.matvec(x, transpose=True)  # A^T: the contrast moves to the inverse row pass
+    yto = O.matvec_transpose(O.spectrum(pr["g_block"], s.L), pr["chi"] * pr["chi_scale"], x)
+    et = np.abs(yt - yto).max() / np.abs(yto).max()
+    print(N, s.matvec_shapes("fp64"), s.matvec_shapes("fp32"), e64, e32, et)
+    assert e64 < 1e-13 and e32 < 2e-6 and et < 1e-13, (e64, e32, et)
 """
 
 
