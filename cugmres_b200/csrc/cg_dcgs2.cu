@@ -900,7 +900,7 @@ static bool tile_major(long long n, int sms) { return 4 * n >= 3LL * sms * 2 * (
 // per lane), the one whose busiest warp streams fewer elements, i.e. the
 // smaller ceil(tiles / resident warps) * U, ties to the first.  The resident
 // warps are two 8-warp blocks per SM.  At n = 2^20 on 148 SMs, U = 8 gives
-// 4096 tiles over 2368 warps (the second round 73 % full) and U = 7 gives
+// 4096 tiles over 2368 warps (the second wave 73 % full) and U = 7 gives
 // 4682 (99 %); measured at 1024^2, ms per 1000 steps: FP64 dots 150.7 (U = 8)
 // -> 142.2 (U = 7), FP64 axpy 140.1 -> 138.0, FP32 dots 97.8 (U = 8) -> 86.8
 // (U = 16) -> 83.5 (U = 14), FP32 axpy 82.2 (U = 8) -> 78.4 (U = 14); at
