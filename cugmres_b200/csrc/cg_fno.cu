@@ -165,12 +165,23 @@ __global__ void k_norm_fin(const double *part, int nbx, int B, long long hw, flo
     }
 }
 
+// Channel-major copy of cell e's 32 channels: vT[line][c][w], line = e / W,
+// w = e % W (the operand layout of the tensor-core column DFT).  The lanes of
+// a warp hold consecutive cells, so each store of a channel is coalesced.
+__device__ __forceinline__ void st_channel_major(__nv_bfloat16 *vT, long long e, int W, const float (&v)[32]) {
+    const long long line = e / W;
+    const int w = (int)(e - line * W);
+    __nv_bfloat16 *d = vT + line * (long long)C * W + w;
+#pragma unroll
+    for (int c = 0; c < C; c++) d[(long long)c * W] = __float2bfloat16(v[c]);
+}
+
 // --------------------------------------------------------------------- lift
 template <typename RT>
 __global__ void __launch_bounds__(256)
 k_lift(const RT *__restrict__ r, const float *__restrict__ chi, const float *__restrict__ k0h,
        const float *__restrict__ inv_s, long long hw, long long cells, const float *__restrict__ prm,
-       __nv_bfloat16 *__restrict__ v0, const int *gate) {
+       __nv_bfloat16 *__restrict__ v0, __nv_bfloat16 *__restrict__ vT, int W, const int *gate) {
     if (gated(gate)) return;
     __shared__ float P[C * NIN + C];
     for (int i = threadIdx.x; i < C * NIN + C; i += blockDim.x) P[i] = prm[OFF_P + i];
@@ -186,6 +197,7 @@ k_lift(const RT *__restrict__ r, const float *__restrict__ chi, const float *__r
         for (int c = 0; c < C; c++)
             v[c] = P[C * NIN + c] + P[c * NIN] * f0 + P[c * NIN + 1] * f1 + P[c * NIN + 2] * f2 + P[c * NIN + 3] * f3;
         st_bf16x32(v0 + e * C, v);
+        if (vT) st_channel_major(vT, e, W, v);
     }
 }
 
@@ -438,6 +450,8 @@ struct EpiLayer {
     const float *spec;
     __nv_bfloat16 *z;
     __nv_bfloat16 *vout;
+    __nv_bfloat16 *vT;  // nullable: channel-major copy of vout for the tensor-core column DFT
+    int W;
     int act;
     __device__ __forceinline__ void row(long long r, const float (&a)[32], int) {
         float zz[32];
@@ -456,9 +470,70 @@ struct EpiLayer {
             for (int q = 0; q < 32; q++) zz[q] = gelu(zz[q]);
         }
         st_bf16x32(vout + r * C, zz);
+        if (vT) st_channel_major(vT, r, W, zz);
     }
     __device__ __forceinline__ void done(long long) {}
 };
+
+// Column DFT on the tensor cores for W = 1024 = 32 x 32 (w = 32 w1 + w2): the
+// GEMM's A operand is the channel-major activation vT read as rows
+// rho = (line C + c) 32 + w1 of the 32 values w2, and B holds the twiddles
+// cos / -sin(2 pi w2 k / 1024) of the 16 column modes k (rows 2k, 2k + 1; BF16
+// hi and lo parts in two launches, the second adding to the first).  Row rho's
+// accumulator is sum_w2 v e^{-2 pi i w2 k / 1024}; the epilogue multiplies it by
+// e^{-2 pi i w1 k / 32} and sums over w1, which are the 32 lanes of the warp
+// (reduce-scatter: lane j ends with value j = 2k + part), into X[line][k][c].
+// Every lane of a warp must take part: M is a multiple of 128 (W = 1024).
+struct EpiDftW {
+    float *X;            // float2 [lines][M2][C] seen as floats
+    const float2 *tw32;  // (cos, sin)(2 pi m / 32)
+    int add;
+    __device__ __forceinline__ void row(long long rho, const float (&a)[32], int) {
+        const int lane = (int)(rho & 31);
+        float v[32];
+#pragma unroll
+        for (int k = 0; k < M2; k++) {
+            const float2 e = __ldg(tw32 + ((lane * k) & 31));
+            const float re = a[2 * k], im = a[2 * k + 1];
+            v[2 * k] = re * e.x + im * e.y;  // (re + i im) (e.x - i e.y)
+            v[2 * k + 1] = im * e.x - re * e.y;
+        }
+#pragma unroll
+        for (int sh = 16; sh >= 1; sh >>= 1) {
+            const bool up = (lane & sh) != 0;
+#pragma unroll
+            for (int i = 0; i < sh; i++) {
+                const float send = up ? v[i] : v[i + sh];
+                const float keep = up ? v[i + sh] : v[i];
+                v[i] = keep + __shfl_xor_sync(0xffffffffu, send, sh);
+            }
+        }
+        const long long line = rho >> 10;
+        const int c = (int)((rho >> 5) & 31);
+        float *dst = X + ((line * M2 + (lane >> 1)) * C + c) * 2 + (lane & 1);
+        *dst = add ? *dst + v[0] : v[0];
+    }
+    __device__ __forceinline__ void done(long long) {}
+};
+
+// B operand (hi rows 0..31, lo rows 32..63) and the 32 outer twiddles of EpiDftW.
+__global__ void k_tc_dft_twiddles(__nv_bfloat16 *twb, float2 *tw32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 1024) {
+        const int n = i >> 5, w2 = i & 31, k = n >> 1;
+        double sn, cs;
+        sincospi(2.0 * (double)(w2 * k) / 1024.0, &sn, &cs);
+        const float v = (n & 1) ? (float)-sn : (float)cs;
+        const __nv_bfloat16 hi = __float2bfloat16(v);
+        twb[i] = hi;
+        twb[1024 + i] = __float2bfloat16(v - __bfloat162float(hi));
+    }
+    if (i < 32) {
+        double sn, cs;
+        sincospi(2.0 * (double)i / 32.0, &sn, &cs);
+        tw32[i] = make_float2((float)cs, (float)sn);
+    }
+}
 
 // Projection, forward (N = 128 hidden): zq = acc + bq1, q = GELU(zq),
 // o = Q2 q + bq2; inference writes z = r + s (o0 + i o1).
@@ -870,6 +945,10 @@ struct cg_fno {
     cg_c64 *r_in = nullptr, *x_in = nullptr, *z_out = nullptr;
     CUtensorMap mapA[LAYERS + 1], mapDZ[2], mapDZQ;
     long long map_cells = -1;
+    // tensor-core column DFT (W = 1024): channel-major activations, B operand, outer twiddles
+    __nv_bfloat16 *vT = nullptr, *twb = nullptr;
+    float2 *tw32 = nullptr;
+    CUtensorMap mapVT, mapTwHi, mapTwLo;
     // twiddles of the current grid
     int tw_H = 0, tw_W = 0;
     float2 *twh = nullptr, *tww = nullptr;
@@ -936,6 +1015,7 @@ int ensure_ws(cg_fno *f, int B, int H, int W) {
     std::vector<std::pair<void **, size_t>> plan;
     auto add = [&](void **ptr, size_t bytes) { plan.push_back({ptr, bytes}); };
     for (int l = 0; l <= LAYERS; l++) add((void **)&f->act[l], (size_t)nc * C * 2);
+    add((void **)&f->vT, (size_t)nc * C * 2);
     for (int l = 0; l < LAYERS - 1; l++) add((void **)&f->zpre[l], (size_t)nc * C * 2);
     add((void **)&f->zq, (size_t)nc * HID * 2);
     add((void **)&f->dz[0], (size_t)nc * C * 2);
@@ -993,6 +1073,7 @@ int ensure_maps(cg_fno *f, long long cells) {
     for (int q = 0; q < 2; q++)
         if (make_map(&f->mapDZ[q], f->dz[q], cells, C, umma::TILE_M)) return CG_ERR_CUDA;
     if (make_map(&f->mapDZQ, f->dzq, cells, HID, umma::TILE_M)) return CG_ERR_CUDA;
+    if (make_map(&f->mapVT, f->vT, cells, C, umma::TILE_M)) return CG_ERR_CUDA;  // rows (line, c, w1) x 32 w2
     f->map_cells = cells;
     return CG_OK;
 }
@@ -1016,11 +1097,38 @@ int ensure_twiddles(cg_fno *f, int H, int W) {
     return CG_OK;
 }
 
+// The column DFT runs on the tensor cores for W = 1024 (CUGMRES_FNO_TC_DFT=0: never).
+bool tc_dft(const cg_fno *f, int W) {
+    static const bool on = [] {
+        const char *e = getenv("CUGMRES_FNO_TC_DFT");
+        return !(e && e[0] == '0');
+    }();
+    return on && W == 1024 && f->twb != nullptr;
+}
+
+int ensure_tc_dft(cg_fno *f) {
+    if (f->twb) return CG_OK;
+    FN_CU(cudaMalloc((void **)&f->twb, sizeof(__nv_bfloat16) * 2048));
+    FN_CU(cudaMalloc((void **)&f->tw32, sizeof(float2) * 32));
+    k_tc_dft_twiddles<<<4, 256, 0, f->stream>>>(f->twb, f->tw32);
+    FN_CU(cudaGetLastError());
+    if (make_map(&f->mapTwHi, f->twb, C, C, C) || make_map(&f->mapTwLo, f->twb + 1024, C, C, C)) {
+        cudaFree(f->twb);
+        cudaFree(f->tw32);
+        f->twb = nullptr;
+        f->tw32 = nullptr;
+        return CG_ERR_CUDA;
+    }
+    FN_CU(cudaStreamSynchronize(f->stream));
+    return CG_OK;
+}
+
 int prepare_grid(cg_fno *f, int B, int H, int W) {
     if (H < 2 * M1 || W < 2 * M2 || H > 4096 || W > 1024) return CG_ERR_INVALID;
     FN_TRY(ensure_ws(f, B, H, W));
     FN_TRY(ensure_maps(f, (long long)B * H * W));
     FN_TRY(ensure_twiddles(f, H, W));
+    if (W == 1024) FN_TRY(ensure_tc_dft(f));
     return CG_OK;
 }
 
@@ -1037,11 +1145,22 @@ int set_smem_attrs(int W, int H) {
 }
 
 // Spectral branch S_l(in) into f->spec (FP32 [cells][C]); saves X2 when X2save.
+// tc: the column DFT runs on the tensor cores from f->vT, the channel-major copy of `in`.
 int spectral_fwd(cg_fno *f, const __nv_bfloat16 *in, int B, int H, int W, int layer, float2 *X2save, const int *gate,
-                 cudaStream_t s) {
+                 cudaStream_t s, bool tc) {
     const long long lines = (long long)B * H;
     const int HC = (H + HCH - 1) / HCH;
-    k_dft_w_fwd<<<(unsigned)lines, 512, dft_w_fwd_smem(W), s>>>(in, W, f->tww, f->X1, 1.f, 1.f, gate);
+    if (tc) {
+        EpiDftW e;
+        e.X = reinterpret_cast<float *>(f->X1);
+        e.tw32 = f->tw32;
+        e.add = 0;
+        FN_K(gemm<32, 1, 6>(f->sms, f->mapVT, f->mapTwHi, lines * W, e, f->err, gate, s));
+        e.add = 1;
+        FN_K(gemm<32, 1, 6>(f->sms, f->mapVT, f->mapTwLo, lines * W, e, f->err, gate, s));
+    } else {
+        k_dft_w_fwd<<<(unsigned)lines, 512, dft_w_fwd_smem(W), s>>>(in, W, f->tww, f->X1, 1.f, 1.f, gate);
+    }
     k_dft_h_fwd<<<dim3(B * HC, NJ / 128), 128, H * 8, s>>>(f->X1, H, HC, f->twh, f->Hp, gate);
     k_mix_fwd<<<K1N * M2, 256, 0, s>>>(f->Hp, B, HC, f->p, layer, X2save, f->Y2, gate);
     k_dft_h_inv<<<dim3(B * HC, NJ / 128), 128, H * 8, s>>>(f->Y2, H, HC, f->twh, f->X1, gate);
@@ -1061,10 +1180,12 @@ int forward(cg_fno *f, cudaStream_t s, int B, int H, int W, const RT *r, const f
     k_norm_part<RT><<<dim3(nbx, B), RED_THREADS, 0, s>>>(r, train ? x : nullptr, hw, nbx, f->npart, gate);
     k_norm_fin<<<(B + 63) / 64, 64, 0, s>>>(f->npart, nbx, B, hw, f->s, f->inv_s, train ? f->wts : nullptr, gate);
     const int lb = (int)std::min<long long>((cells + 255) / 256, 8LL * f->sms);
-    k_lift<RT><<<lb, 256, 0, s>>>(r, chi, f->k0h, f->inv_s, hw, cells, f->p, f->act[0], gate);
+    const bool tc = tc_dft(f, W);
+    k_lift<RT><<<lb, 256, 0, s>>>(r, chi, f->k0h, f->inv_s, hw, cells, f->p, f->act[0], tc ? f->vT : nullptr, W,
+                                  gate);
     FN_K(cudaGetLastError());
     for (int l = 0; l < LAYERS; l++) {
-        FN_K(spectral_fwd(f, f->act[l], B, H, W, l, train ? f->X2s[l] : nullptr, gate, s));
+        FN_K(spectral_fwd(f, f->act[l], B, H, W, l, train ? f->X2s[l] : nullptr, gate, s, tc));
         if (l == LAYERS - 1 && !f->local_last) {
             k_spec_bias<<<lb, 256, 0, s>>>(f->spec, f->p + off_b(l), f->act[l + 1], cells, gate);
             FN_K(cudaGetLastError());
@@ -1075,6 +1196,8 @@ int forward(cg_fno *f, cudaStream_t s, int B, int H, int W, const RT *r, const f
         e.spec = f->spec;
         e.z = (train && l < LAYERS - 1) ? f->zpre[l] : nullptr;
         e.vout = f->act[l + 1];
+        e.vT = (tc && l + 1 < LAYERS) ? f->vT : nullptr;  // the next layer's column DFT reads it
+        e.W = W;
         e.act = l < LAYERS - 1 ? 1 : 0;
         FN_K(gemm<32, 1, 6>(f->sms, f->mapA[l], f->mapW[l], cells, e, f->err, gate, s));
     }
@@ -1292,6 +1415,8 @@ extern "C" void cugmres_fno_destroy(cg_fno *f) {
     cudaFree(f->m);
     cudaFree(f->v);
     cudaFree(f->wb);
+    cudaFree(f->twb);
+    cudaFree(f->tw32);
     cudaFree(f->err);
     cudaFree(f->ws);
     cudaFree(f->twh);

@@ -73,8 +73,10 @@ def test_fno_params_roundtrip(net):
     assert np.array_equal(net.get_params(), p)
 
 
-@pytest.mark.parametrize("B,H,W", [(2, 32, 48), (1, 64, 64), (3, 40, 96)])
+@pytest.mark.parametrize("B,H,W", [(2, 32, 48), (1, 64, 64), (3, 40, 96), (1, 32, 1024), (2, 40, 1024)])
 def test_fno_forward_matches_oracle(net, B, H, W):
+    """W = 1024 takes the tensor-core column DFT (two-level split, BF16 hi/lo
+    twiddles), the other widths the CUDA-core one."""
     p = _params(1)
     net.set_params(p)
     chi, k0h, r, _ = _inputs(B, H, W, 7)
