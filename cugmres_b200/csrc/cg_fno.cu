@@ -516,7 +516,47 @@ struct EpiDftW {
     __device__ __forceinline__ void done(long long) {}
 };
 
-// B operand (hi rows 0..31, lo rows 32..63) and the 32 outer twiddles of EpiDftW.
+// Inverse column DFT on the tensor cores for W = 1024: rows
+// rho = (line 32 + w1) 32 + c of Z (k_zinv: Z[2k] + i Z[2k+1] =
+// sc(k) Y[line][k][c] e^{+2 pi i w1 k / 32}, BF16) times B[w2][n] = cos / -sin
+// of 2 pi w2 k / 1024 give out[line][32 w1 + w2][c] = sum_k Re(Z_k e^{+2 pi i w2 k / 1024})
+// for the 32 w2 of the row; the lanes of a warp are the 32 channels, so each
+// output column is one coalesced store.
+struct EpiDftWInv {
+    float *out;  // FP32 [cells][C]
+    __device__ __forceinline__ void row(long long rho, const float (&a)[32], int) {
+        const int c = (int)(rho & 31), w1 = (int)((rho >> 5) & 31);
+        const long long line = rho >> 10;
+        float *dst = out + (line * 1024 + 32 * w1) * C + c;
+#pragma unroll
+        for (int w2 = 0; w2 < 32; w2++) dst[w2 * C] = a[w2];
+    }
+    __device__ __forceinline__ void done(long long) {}
+};
+
+__global__ void __launch_bounds__(256)
+k_zinv(const float2 *__restrict__ Y, long long lines, float s0, float s1, const float2 *__restrict__ tw32,
+       __nv_bfloat16 *__restrict__ Z, const int *gate) {
+    if (gated(gate)) return;
+    for (long long rho = (long long)blockIdx.x * blockDim.x + threadIdx.x; rho < lines * 1024;
+         rho += (long long)gridDim.x * blockDim.x) {
+        const int c = (int)(rho & 31), w1 = (int)((rho >> 5) & 31);
+        const long long line = rho >> 10;
+        float z[32];
+#pragma unroll
+        for (int k = 0; k < M2; k++) {
+            const float2 y = Y[(line * M2 + k) * C + c];
+            const float sc = k == 0 ? s0 : s1;
+            const float2 e = __ldg(tw32 + ((w1 * k) & 31));  // e^{+2 pi i w1 k / 32}
+            z[2 * k] = sc * (y.x * e.x - y.y * e.y);
+            z[2 * k + 1] = sc * (y.x * e.y + y.y * e.x);
+        }
+        st_bf16x32(Z + rho * 32, z);
+    }
+}
+
+// B operands (forward hi rows 0..31, forward lo rows 32..63; inverse rows
+// 64..95: B[w2][n], the forward's transpose, BF16) and the 32 outer twiddles.
 __global__ void k_tc_dft_twiddles(__nv_bfloat16 *twb, float2 *tw32) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < 1024) {
@@ -527,6 +567,7 @@ __global__ void k_tc_dft_twiddles(__nv_bfloat16 *twb, float2 *tw32) {
         const __nv_bfloat16 hi = __float2bfloat16(v);
         twb[i] = hi;
         twb[1024 + i] = __float2bfloat16(v - __bfloat162float(hi));
+        twb[2048 + w2 * 32 + n] = hi;
     }
     if (i < 32) {
         double sn, cs;
@@ -948,7 +989,7 @@ struct cg_fno {
     // tensor-core column DFT (W = 1024): channel-major activations, B operand, outer twiddles
     __nv_bfloat16 *vT = nullptr, *twb = nullptr;
     float2 *tw32 = nullptr;
-    CUtensorMap mapVT, mapTwHi, mapTwLo;
+    CUtensorMap mapVT, mapTwHi, mapTwLo, mapTwInv;
     // twiddles of the current grid
     int tw_H = 0, tw_W = 0;
     float2 *twh = nullptr, *tww = nullptr;
@@ -1108,11 +1149,12 @@ bool tc_dft(const cg_fno *f, int W) {
 
 int ensure_tc_dft(cg_fno *f) {
     if (f->twb) return CG_OK;
-    FN_CU(cudaMalloc((void **)&f->twb, sizeof(__nv_bfloat16) * 2048));
+    FN_CU(cudaMalloc((void **)&f->twb, sizeof(__nv_bfloat16) * 3072));
     FN_CU(cudaMalloc((void **)&f->tw32, sizeof(float2) * 32));
     k_tc_dft_twiddles<<<4, 256, 0, f->stream>>>(f->twb, f->tw32);
     FN_CU(cudaGetLastError());
-    if (make_map(&f->mapTwHi, f->twb, C, C, C) || make_map(&f->mapTwLo, f->twb + 1024, C, C, C)) {
+    if (make_map(&f->mapTwHi, f->twb, C, C, C) || make_map(&f->mapTwLo, f->twb + 1024, C, C, C) ||
+        make_map(&f->mapTwInv, f->twb + 2048, C, C, C)) {
         cudaFree(f->twb);
         cudaFree(f->tw32);
         f->twb = nullptr;
@@ -1165,7 +1207,17 @@ int spectral_fwd(cg_fno *f, const __nv_bfloat16 *in, int B, int H, int W, int la
     k_mix_fwd<<<K1N * M2, 256, 0, s>>>(f->Hp, B, HC, f->p, layer, X2save, f->Y2, gate);
     k_dft_h_inv<<<dim3(B * HC, NJ / 128), 128, H * 8, s>>>(f->Y2, H, HC, f->twh, f->X1, gate);
     const float inv = 1.f / ((float)H * (float)W);
-    k_dft_w_inv<<<(unsigned)lines, 256, dft_w_inv_smem(W), s>>>(f->X1, W, f->tww, f->spec, inv, 2.f * inv, gate);
+    if (tc) {
+        // Z reuses the channel-major buffer (its column DFT has run) and its map
+        const int zb = (int)std::min<long long>((lines * 1024 + 255) / 256, 8LL * f->sms);
+        k_zinv<<<zb, 256, 0, s>>>(f->X1, lines, inv, 2.f * inv, f->tw32, f->vT, gate);
+        FN_K(cudaGetLastError());
+        EpiDftWInv e;
+        e.out = f->spec;
+        FN_K(gemm<32, 1, 6>(f->sms, f->mapVT, f->mapTwInv, lines * W, e, f->err, gate, s));
+    } else {
+        k_dft_w_inv<<<(unsigned)lines, 256, dft_w_inv_smem(W), s>>>(f->X1, W, f->tww, f->spec, inv, 2.f * inv, gate);
+    }
     return (int)cudaGetLastError();
 }
 
