@@ -21,6 +21,20 @@ time vs the measured HBM copy bandwidth in MEASURED_PEAKS.json), e2e (the same
 solve through the public API from pinned host buffers, H2D/D2H inside the
 timed region), the CPU oracle timed on a bounded sample (rank 0, N = 1), clocks
 sampled with nvidia-smi during the timed region.
+
+--impl reference: the reference's CPU GMRES (the oracle's C restatement of
+FFT_GMRES_with_MKL generalised to restarts; MKL is absent) on every host
+thread, rank 0 only.  It loads nothing of this library: the system is built by
+oracle/problems.py with the oracle's own Green's block.  Each timed step is
+one whole restart cycle (restart Arnoldi steps, the true residual and the
+update); the value scales the mean cycle time by the cycles of the same
+budget-capped solve (max_iter / restart).  Warm-up steps run a 5-step sample.
+
+--profile-case: a fixed launch sequence for profiler captures (no timing, no
+JSON): three FP64 and three FP32 matvecs of the 1024^2 system, then one solve of
+exactly --case-steps Arnoldi steps (tolerance 1e-14, so it never stops early):
+per step [k_rows_forward, k_cols_convolve, k_rows_inverse, k_dots2, k_dcgs2_step,
+k_axpy2]; `ncu -k regex:k_dots2 -s 30 -c 1` then picks the dot pass of step 30.
 """
 import argparse
 import json
@@ -52,7 +66,8 @@ def parse():
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--inner-tol", type=float, default=1e-5)
-    ap.add_argument("--cpu-sample-steps", type=int, default=6)
+    ap.add_argument("--profile-case", action="store_true", help="fixed launch sequence for profiler captures")
+    ap.add_argument("--case-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and 256^2 side measurements")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner side measurement")
@@ -137,27 +152,65 @@ def workload(args):
             "l2": "inputs larger than L2 (basis of restart+1 vectors of N^2 complex)"}
 
 
-def cpu_baseline(args, pr, iters_needed):
-    """Oracle (plain-C restatement of the reference's CPU GMRES) on a bounded
-    sample: `cpu-sample-steps` Arnoldi steps of the same system with every host
-    thread, scaled to one solve by the GPU's iteration count."""
+def oracle_system(args):
+    """The benchmark system built by the oracle alone (no libcugmres load)."""
     from oracle import oracle as O
+    from oracle import problems as OP
     O.build()
-    threads = os.cpu_count() or 1
-    O.set_threads(threads)
-    L = 16
-    while L < 2 * args.N - 1:
-        L *= 2
-    gh = O.spectrum(pr["g_block"], L)
+    pr = OP.helmholtz(args.N, args.eps, seed=args.seed)
+    gh = O.spectrum(pr["g_block"], OP.embedding(args.N))
+    return O, pr, gh
+
+
+def cycles_per_solve(args):
+    """Restart cycles of the budget-capped solve (every cycle runs `restart` steps)."""
+    return max(1, -(-args.max_iter // args.restart))
+
+
+def oracle_cycle(O, pr, gh, args, steps=None):
+    """One GMRES(restart) cycle of the oracle in FP64 (or `steps` Arnoldi steps):
+    the true residual, the Arnoldi steps with modified Gram-Schmidt, the
+    least-squares solve and the update.  Returns seconds."""
     c = pr["chi"] * pr["chi_scale"]
-    s = max(1, args.cpu_sample_steps)
+    s = steps or args.restart
     t0 = time.perf_counter()
     out = O.gmres(gh, c, pr["b"], restart=args.restart, maxiter=s, tol=0.0)
     dt = time.perf_counter() - t0
-    per_step = dt / max(1, out["iterations"])
-    return {"value": per_step * iters_needed, "unit": "s", "cores": threads, "kind": "port",
-            "sample": f"{out['iterations']} Arnoldi steps (incl. one FP64 residual) of the same "
-                      f"{args.N}x{args.N} system in {dt:.2f} s, scaled by {iters_needed} steps/solve"}
+    assert out["iterations"] == s, out["iterations"]
+    return dt
+
+
+def cpu_baseline(args):
+    """The oracle (plain-C restatement of the reference's CPU GMRES, MKL absent)
+    on every host thread: one whole FP64 GMRES(restart) cycle of the same
+    system, scaled by the cycles of the budget-capped solve; next to it the
+    reference's own algorithm (FFT_GMRES_with_MKL restated: complex64, no
+    restart, modified Gram-Schmidt, explicit Givens products and LU) on one
+    core, as the reference's makefile links MKL sequential, timed over its
+    first 10 Arnoldi steps."""
+    O, pr, gh = oracle_system(args)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    oracle_cycle(O, pr, gh, args, steps=5)  # thread pool and page warm-up
+    dt = oracle_cycle(O, pr, gh, args)
+    cyc = cycles_per_solve(args)
+    out = {"value": dt * cyc, "unit": "s", "cores": threads, "kind": "port",
+           "sample": f"one whole FP64 GMRES({args.restart}) cycle of the same {args.N}x{args.N} system "
+                     f"({args.restart} Arnoldi steps, true residual, update) in {dt:.2f} s on {threads} threads, "
+                     f"x {cyc} cycles of the capped solve"}
+    O.set_threads(1)
+    s10 = 10
+    g64 = gh.astype(np.complex64)
+    t0 = time.perf_counter()
+    O.gmres_reference(g64, pr["chi"] * pr["chi_scale"], pr["b"], np.zeros_like(pr["b"]), s10, 0.0,
+                      precision="c64")
+    d1 = time.perf_counter() - t0
+    O.set_threads(threads)
+    out["reference_1core_c64"] = {
+        "value": d1 / s10, "unit": "s per Arnoldi step", "cores": 1, "kind": "port",
+        "sample": f"first {s10} steps of FFT_GMRES_with_MKL restated (complex64, unrestarted, MGS) on the "
+                  f"{args.N}x{args.N} system, one thread, {d1:.2f} s"}
+    return out
 
 
 def timed_solves(s, b, kw, steps, stream):
@@ -304,24 +357,49 @@ def sweep_side(args):
 
 
 def run_reference(args, rank, world):
-    """The reference's CPU GMRES (oracle port: MKL absent) on the host cores."""
+    """The reference's CPU GMRES (oracle port: MKL absent) on the host cores,
+    rank 0 only; nothing of this library is loaded."""
     if rank != 0:
         return
-    pr = make_problem(args)
-    iters = int(os.environ.get("CUGMRES_BENCH_ITERS", "0")) or args.max_iter
-    times = []
-    for i in range(args.warmup + args.steps):
-        b = cpu_baseline(args, pr, iters)
-        if i >= args.warmup:
-            times.append(b["value"])
-    v = float(np.mean(times))
+    O, pr, gh = oracle_system(args)
+    threads = os.cpu_count() or 1
+    O.set_threads(threads)
+    for _ in range(args.warmup):
+        oracle_cycle(O, pr, gh, args, steps=5)
+    times = [oracle_cycle(O, pr, gh, args) for _ in range(args.steps)]
+    cyc = cycles_per_solve(args)
+    per_cycle = float(np.mean(times))
+    v = per_cycle * cyc
+    sample = (f"each timed step is one whole FP64 GMRES({args.restart}) cycle of the oracle (modified "
+              f"Gram-Schmidt, {threads} threads) on the same {args.N}x{args.N} system, mean {per_cycle:.2f} s; "
+              f"value = cycle time x {cyc} cycles of the budget-capped solve; warm-up steps run 5 Arnoldi steps")
     line = {"metric": METRIC, "impl": "reference", "value": v, "unit": "s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": per_cycle * 1e3,
+            "ms_per_step_unit": "ms per restart cycle (the timed sample)", "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": workload(args), "cpu_baseline": {"kind": b["kind"], "cores": b["cores"],
-                                                       "sample": b["sample"], "value": v, "unit": "s"},
+            "config": workload(args),
+            "cpu_baseline": {"kind": "port", "cores": threads, "sample": sample, "value": v, "unit": "s"},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def profile_case(args):
+    """Fixed launch sequence for profiler captures (see the module docstring)."""
+    import cugmres_b200 as cg
+    from cugmres_b200 import problems as P
+    pr = P.helmholtz(args.N, args.eps, seed=args.seed)
+    s = cg.Solver(0)
+    s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x = np.random.default_rng(0).standard_normal((args.N, args.N)) + 0j
+    for _ in range(3):
+        s.matvec(x)
+    x32 = x.astype(np.complex64)
+    for _ in range(3):
+        s.matvec(x32, precision="fp32")
+    _, info = s.solve(pr["b"], restart=args.case_steps, max_iter=args.case_steps, tol=1e-14,
+                      precision=args.precision)
+    s.close()
+    print("ok", info["iterations"], info["status_text"], flush=True)
 
 
 def main():
@@ -331,6 +409,8 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.profile_case:
+        return profile_case(args)
 
     import torch
     import torch.distributed as dist
@@ -394,9 +474,10 @@ def main():
     phases = {k: v for k, v in prof.items() if v["ms"] > 0}
     dom = max(phases.items(), key=lambda kv: kv[1]["ms"])
     tot_ms = sum(v["ms"] for v in phases.values())
-    # DRAM traffic per launch of the dominant kernel: ncu (dram__bytes_read.sum + dram__bytes_write.sum)
-    # of one launch at step k = 30 of the 1024^2 FP64 solve, as a ratio to that launch's algorithmic
-    # bytes, applied to this run's mean algorithmic bytes per launch (profiles/dcgs2_passes_1024x1024_k30.md)
+    # DRAM traffic per launch of the dominant kernel is not measurable without a profiler: it is taken
+    # from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the launch at step k = 30
+    # of this 1024^2 FP64 solve (bench.py --profile-case), as a ratio to that launch's algorithmic
+    # bytes, applied to this run's mean algorithmic bytes per launch; "traffic_source" says so
     ncu_ratio = {"dots": (536.904 + 4.625) / 536.871, "axpy": (536.961 + 8.369) / 570.425}
     launches = max(1, dom[1].get("launches", 0))
     alg_per_launch = dom[1].get("bytes", 0.0) / launches
@@ -404,6 +485,8 @@ def main():
     roof = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1]["gbs"], 1), "peak": hbm, "unit": "GB/s",
             "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind,
             "traffic": round(traffic) if traffic else None, "traffic_unit": "bytes/launch",
+            "traffic_source": ("ncu capture of the same kernel at step 30 of this solve (--profile-case), its "
+                               "DRAM bytes / algorithmic bytes ratio applied to this run's mean launch"),
             "algorithmic_bytes_per_launch": round(alg_per_launch),
             "phases": {k: {"share": round(v["ms"] / tot_ms, 4), "gbs": round(v["gbs"], 1),
                            "ms": round(v["ms"], 3)} for k, v in phases.items()}}
@@ -436,7 +519,7 @@ def main():
     if rank == 0 and world == 1 and args.sweep > 0:
         line.setdefault("side", {})["sweep"] = sweep_side(args)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, pr, last["iterations"])
+        line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:
         print(json.dumps(line), flush=True)
     s.close()

@@ -341,8 +341,8 @@ __global__ void k_cycle_begin(KrylovPtrs kp, int nparts) {
         stop = 1;
     }
     st->brk = 0;
-    st->cycles += 1;
     if (!stop) {
+        st->cycles += 1;  // cycles that run Arnoldi steps (the final check is not one)
         // CGS2 normalises V_0 lazily; the delayed scheme normalises it in its first step
         if (st->ortho == 1) kp.scale[0] = 1.0 / beta;
         kp.g[0] = make_double2(beta, 0.0);

@@ -15,6 +15,9 @@
 //   * the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (once per device, with that device current); make
 //     that first call before any stream capture;
+//   * that address is kept for the life of the process: the library must not
+//     outlive a cudaDeviceReset (or any other teardown of the device's primary
+//     context), after which the kept address would be stale;
 //   * all calls on a device share the one array, so calls whose work overlaps
 //     on the GPU (different streams, or different host threads) race; serialise
 //     them on one stream;
@@ -64,13 +67,17 @@ int na_scratch(int dev, unsigned char **out) {
     return CG_OK;
 }
 
-bool na_on_device(const void *p) {
+// True when p is device (or managed) memory that belongs to device `dev`; a
+// pointer into another GPU's memory is refused, since the kernels would read it
+// over the peer link (or fault without peer access).
+bool na_on_device(const void *p, int dev) {
     cudaPointerAttributes a;
     if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
         cudaGetLastError();
         return false;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged) return false;
+    return a.device == dev;
 }
 
 // the four per-stage twiddle tables of cg_fft.cuh (16- and 8-point plans,
@@ -114,11 +121,12 @@ extern "C" int cugmres_matvec_noalloc(int N, const cg_c128 *g_block, const doubl
                                       const cg_c128 *x, cg_c128 *y, void *stream) {
     if (N < 1 || !g_block || !chi || !x || !y || !isfinite(chi_scale)) return CG_ERR_INVALID;
     if (N > NA_MAX_N) return CG_ERR_INVALID;  // beyond the fixed scratch: use cugmres_matvec
-    if (!na_on_device(g_block) || !na_on_device(chi) || !na_on_device(x) || !na_on_device(y)) return CG_ERR_INVALID;
-    int L = 16;
-    while (L < 2 * N - 1) L *= 2;
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return CG_ERR_CUDA;
+    if (!na_on_device(g_block, dev) || !na_on_device(chi, dev) || !na_on_device(x, dev) || !na_on_device(y, dev))
+        return CG_ERR_INVALID;
+    int L = 16;
+    while (L < 2 * N - 1) L *= 2;
     unsigned char *base = nullptr;
     int st = na_scratch(dev, &base);
     if (st != CG_OK) return st;

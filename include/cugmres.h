@@ -246,7 +246,8 @@ int cugmres_fast_gmres(const cg_c64 *g_prep, const unsigned char *mask, cg_c64 *
  *   - g_block (N x N), chi (N x N), x and y must be device memory of the current
  *     device, otherwise CG_ERR_INVALID;
  *   - the first call on a device looks up the scratch array's address (once per
- *     device); make it before any stream capture;
+ *     device) and keeps it for the life of the process; make that call before
+ *     any stream capture, and do not use the library across a cudaDeviceReset;
  *   - calls share the scratch array: calls whose GPU work overlaps (other
  *     streams or host threads) race, so serialise them on one stream;
  *   - the work is enqueued on `stream` (a cudaStream_t, NULL = default stream);

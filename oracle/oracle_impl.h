@@ -21,11 +21,19 @@
  */
 
 /* ---------------------------------------------------------------- FFT plan */
+/* Complex product written out in real arithmetic (the same four products and
+ * two sums as C99's operator, without its Annex G NaN recovery, which the
+ * compiler otherwise calls out of the FFT's inner loops). */
+#define SFX_CMUL(a, b) __builtin_complex((REAL)(creal(a) * creal(b) - cimag(a) * cimag(b)), \
+                                         (REAL)(creal(a) * cimag(b) + cimag(a) * creal(b)))
+
 typedef struct {
     int L;
     int nrad;
     int rad[40];
-    CPLX *tw; /* tw[m] = exp(-2 pi i m / L), m = 0..L-1, computed in double */
+    CPLX *tw;       /* tw[m] = exp(-2 pi i m / L), m = 0..L-1, computed in double     */
+    CPLX *stw[2];   /* per-stage tables, [0] forward, [1] inverse: stage s at offset  */
+    int off[40];    /* off[s], entry r Ns + k = w^(k r L/(Ns R)) (k < Ns, r < R)      */
 } SFX(plan_t);
 
 static void SFX(plan_init)(SFX(plan_t) *p, int L)
@@ -33,6 +41,7 @@ static void SFX(plan_init)(SFX(plan_t) *p, int L)
     p->L = L;
     p->nrad = 0;
     int r = L;
+    while (r % 8 == 0) { p->rad[p->nrad++] = 8; r /= 8; }
     while (r % 4 == 0) { p->rad[p->nrad++] = 4; r /= 4; }
     while (r % 2 == 0) { p->rad[p->nrad++] = 2; r /= 2; }
     while (r % 3 == 0) { p->rad[p->nrad++] = 3; r /= 3; }
@@ -44,9 +53,51 @@ static void SFX(plan_init)(SFX(plan_t) *p, int L)
         double a = -2.0 * M_PI * (double)m / (double)L;
         p->tw[m] = (REAL)cos(a) + I * (REAL)sin(a);
     }
+    size_t tot = 0;
+    int Ns = 1;
+    for (int s = 0; s < p->nrad; s++) {
+        p->off[s] = (int)tot;
+        tot += (size_t)p->rad[s] * Ns;
+        Ns *= p->rad[s];
+    }
+    p->stw[0] = (CPLX *)malloc(sizeof(CPLX) * (tot ? tot : 1));
+    p->stw[1] = (CPLX *)malloc(sizeof(CPLX) * (tot ? tot : 1));
+    Ns = 1;
+    for (int s = 0; s < p->nrad; s++) {
+        const int R = p->rad[s];
+        const int step = L / (Ns * R);
+        for (int q = 0; q < R; q++)
+            for (int k = 0; k < Ns; k++) {
+                /* the same table entry the plain loop indexes: (k r step) mod L */
+                const CPLX w = p->tw[(int)(((long long)k * q * step) % L)];
+                p->stw[0][p->off[s] + q * Ns + k] = w;
+                p->stw[1][p->off[s] + q * Ns + k] = conj(w);
+            }
+        Ns *= R;
+    }
 }
 
-static void SFX(plan_free)(SFX(plan_t) *p) { free(p->tw); p->tw = NULL; }
+static void SFX(plan_free)(SFX(plan_t) *p)
+{
+    free(p->tw);
+    free(p->stw[0]);
+    free(p->stw[1]);
+    p->tw = p->stw[0] = p->stw[1] = NULL;
+}
+
+/* 4-point DFT, sign = -1 forward, +1 inverse. */
+static inline void SFX(dft4)(const CPLX *v, CPLX *V, int sign)
+{
+    CPLX t0 = v[0] + v[2], t1 = v[0] - v[2];
+    CPLX t2 = v[1] + v[3], t3 = v[1] - v[3];
+    /* multiply t3 by -i (forward) or +i (inverse) */
+    CPLX t3r = (sign < 0) ? __builtin_complex((REAL)cimag(t3), (REAL)-creal(t3))
+                          : __builtin_complex((REAL)-cimag(t3), (REAL)creal(t3));
+    V[0] = t0 + t2;
+    V[2] = t0 - t2;
+    V[1] = t1 + t3r;
+    V[3] = t1 - t3r;
+}
 
 /* One length-L transform of contiguous data `a` (result left in `a`), `b` is
  * scratch of length L.  Stockham auto-sort: stage with radix R and span Ns
@@ -59,44 +110,57 @@ static void SFX(fft1d)(const SFX(plan_t) *p, CPLX *a, CPLX *b, int sign)
     CPLX *src = a, *dst = b;
     int Ns = 1;
     CPLX v[64], V[64];
+    const CPLX *stw = p->stw[sign > 0 ? 1 : 0];
     for (int s = 0; s < p->nrad; s++) {
         const int R = p->rad[s];
         const int LR = L / R;
-        for (int j = 0; j < LR; j++) {
-            const int k = j % Ns;
-            const int step = L / (Ns * R);
-            for (int r = 0; r < R; r++) {
-                int m = (k * r * step) % L;
-                CPLX w = p->tw[m];
-                if (sign > 0) w = conj(w);
-                v[r] = src[j + r * LR] * w;
-            }
-            if (R == 2) {
-                V[0] = v[0] + v[1];
-                V[1] = v[0] - v[1];
-            } else if (R == 4) {
-                CPLX t0 = v[0] + v[2], t1 = v[0] - v[2];
-                CPLX t2 = v[1] + v[3], t3 = v[1] - v[3];
-                /* multiply t3 by -i (forward) or +i (inverse) */
-                CPLX t3r = (sign < 0) ? (cimag(t3) - I * creal(t3)) : (-cimag(t3) + I * creal(t3));
-                V[0] = t0 + t2;
-                V[2] = t0 - t2;
-                V[1] = t1 + t3r;
-                V[3] = t1 - t3r;
-            } else {
-                for (int q = 0; q < R; q++) {
-                    CPLX acc = 0;
-                    for (int r = 0; r < R; r++) {
-                        int m = ((r * q) % R) * LR;
-                        CPLX w = p->tw[m];
-                        if (sign > 0) w = conj(w);
-                        acc += v[r] * w;
+        const CPLX *ws = stw + p->off[s];
+        for (int jb = 0; jb < LR; jb += Ns) {
+            for (int k = 0; k < Ns; k++) {
+                const int j = jb + k;
+                v[0] = src[j];
+                for (int r = 1; r < R; r++) v[r] = SFX_CMUL(src[j + r * LR], ws[r * Ns + k]);
+                if (R == 2) {
+                    V[0] = v[0] + v[1];
+                    V[1] = v[0] - v[1];
+                } else if (R == 4) {
+                    SFX(dft4)(v, V, sign);
+                } else if (R == 8) {
+                    /* two 4-point DFTs of the even and odd samples, joined with
+                     * the 8th roots of unity: V[q] = a[q] + w8^q b[q],
+                     * V[q+4] = a[q] - w8^q b[q] */
+                    CPLX e4[4] = {v[0], v[2], v[4], v[6]}, o4[4] = {v[1], v[3], v[5], v[7]};
+                    CPLX a4[4], b4[4];
+                    SFX(dft4)(e4, a4, sign);
+                    SFX(dft4)(o4, b4, sign);
+                    const REAL h = (REAL)0.70710678118654752440;
+                    const REAL sg = sign < 0 ? (REAL)-1 : (REAL)1;
+                    CPLX w1 = __builtin_complex(h, sg * h), w3 = __builtin_complex(-h, sg * h);
+                    CPLX t1 = SFX_CMUL(b4[1], w1), t3 = SFX_CMUL(b4[3], w3);
+                    CPLX t2 = __builtin_complex((REAL)(-sg * cimag(b4[2])), (REAL)(sg * creal(b4[2])));
+                    V[0] = a4[0] + b4[0];
+                    V[4] = a4[0] - b4[0];
+                    V[1] = a4[1] + t1;
+                    V[5] = a4[1] - t1;
+                    V[2] = a4[2] + t2;
+                    V[6] = a4[2] - t2;
+                    V[3] = a4[3] + t3;
+                    V[7] = a4[3] - t3;
+                } else {
+                    for (int q = 0; q < R; q++) {
+                        CPLX acc = 0;
+                        for (int r = 0; r < R; r++) {
+                            int m = ((r * q) % R) * LR;
+                            CPLX w = p->tw[m];
+                            if (sign > 0) w = conj(w);
+                            acc += SFX_CMUL(v[r], w);
+                        }
+                        V[q] = acc;
                     }
-                    V[q] = acc;
                 }
+                const int idxD = (j / Ns) * Ns * R + k;
+                for (int q = 0; q < R; q++) dst[idxD + q * Ns] = V[q];
             }
-            const int idxD = (j / Ns) * Ns * R + k;
-            for (int q = 0; q < R; q++) dst[idxD + q * Ns] = V[q];
         }
         CPLX *t = src; src = dst; dst = t;
         Ns *= R;
@@ -104,24 +168,52 @@ static void SFX(fft1d)(const SFX(plan_t) *p, CPLX *a, CPLX *b, int sign)
     if (src != a) memcpy(a, src, sizeof(CPLX) * (size_t)L);
 }
 
+/* Columns are gathered OR_CB at a time so that every row access reads whole
+ * cache lines. */
+#define OR_CB 8
+
+/* 2D DFT of an L x L row-major array in place: row transforms of rows
+ * [0, rows_in) (the other rows must be zero on input, so their transforms are
+ * zero and are skipped), then all column transforms, then -- for the inverse
+ * pass of the matvec -- nothing else: only rows [0, rows_out) of the result are
+ * guaranteed; with rows_in = rows_out = L this is the full transform. */
+static void SFX(fft2d_rows)(const SFX(plan_t) *p, int L, CPLX *a, int sign, int rows)
+{
+#pragma omp parallel
+    {
+        CPLX *buf = (CPLX *)malloc(sizeof(CPLX) * (size_t)L);
+#pragma omp for schedule(static)
+        for (int i = 0; i < rows; i++) SFX(fft1d)(p, a + (size_t)i * L, buf, sign);
+        free(buf);
+    }
+}
+
+static void SFX(fft2d_cols)(const SFX(plan_t) *p, int L, CPLX *a, int sign)
+{
+#pragma omp parallel
+    {
+        CPLX *buf = (CPLX *)malloc(sizeof(CPLX) * (size_t)L * (OR_CB + 1));
+        CPLX *scr = buf + (size_t)L * OR_CB;
+#pragma omp for schedule(static)
+        for (int c0 = 0; c0 < L; c0 += OR_CB) {
+            const int nc = (L - c0) < OR_CB ? (L - c0) : OR_CB;
+            for (int i = 0; i < L; i++)
+                for (int q = 0; q < nc; q++) buf[(size_t)q * L + i] = a[(size_t)i * L + c0 + q];
+            for (int q = 0; q < nc; q++) SFX(fft1d)(p, buf + (size_t)q * L, scr, sign);
+            for (int i = 0; i < L; i++)
+                for (int q = 0; q < nc; q++) a[(size_t)i * L + c0 + q] = buf[(size_t)q * L + i];
+        }
+        free(buf);
+    }
+}
+
 /* Full 2D DFT of an L x L row-major array in place (rows, then columns). */
 void SFX(or_fft2d)(int L, CPLX *a, int sign)
 {
     SFX(plan_t) p;
     SFX(plan_init)(&p, L);
-#pragma omp parallel
-    {
-        CPLX *buf = (CPLX *)malloc(sizeof(CPLX) * (size_t)L * 2);
-#pragma omp for schedule(static)
-        for (int i = 0; i < L; i++) SFX(fft1d)(&p, a + (size_t)i * L, buf, sign);
-#pragma omp for schedule(static)
-        for (int c = 0; c < L; c++) {
-            for (int i = 0; i < L; i++) buf[L + i] = a[(size_t)i * L + c];
-            SFX(fft1d)(&p, buf + L, buf, sign);
-            for (int i = 0; i < L; i++) a[(size_t)i * L + c] = buf[L + i];
-        }
-        free(buf);
-    }
+    SFX(fft2d_rows)(&p, L, a, sign, L);
+    SFX(fft2d_cols)(&p, L, a, sign);
     SFX(plan_free)(&p);
 }
 
@@ -155,14 +247,29 @@ void SFX(or_spectrum)(int N, int L, const CPLX *g_block, CPLX *ghat)
 void SFX(or_matvec)(int N, int L, const CPLX *ghat, const REAL *chi,
                     const CPLX *x, const CPLX *plus_b, CPLX *y)
 {
-    CPLX *e = (CPLX *)calloc((size_t)L * L, sizeof(CPLX));
-    for (int i = 0; i < N; i++)
-        for (int j = 0; j < N; j++)
-            e[(size_t)i * L + j] = chi[(size_t)i * N + j] * x[(size_t)i * N + j];
-    SFX(or_fft2d)(L, e, -1);
-    for (size_t m = 0; m < (size_t)L * L; m++) e[m] *= ghat[m];
-    SFX(or_fft2d)(L, e, +1);
+    CPLX *e = (CPLX *)malloc(sizeof(CPLX) * (size_t)L * L);
+    SFX(plan_t) p;
+    SFX(plan_init)(&p, L);
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < L; i++) {
+        CPLX *row = e + (size_t)i * L;
+        int j = 0;
+        if (i < N)
+            for (; j < N; j++) row[j] = chi[(size_t)i * N + j] * x[(size_t)i * N + j];
+        for (; j < L; j++) row[j] = 0;
+    }
+    /* forward 2D DFT: rows N..L-1 of the padded field are zero, so are their
+     * row transforms; inverse: only rows 0..N-1 survive the crop.  Both
+     * omissions leave every kept value bit for bit what the full transforms give. */
+    SFX(fft2d_rows)(&p, L, e, -1, N);
+    SFX(fft2d_cols)(&p, L, e, -1);
+#pragma omp parallel for schedule(static)
+    for (long long m = 0; m < (long long)L * L; m++) e[m] = SFX_CMUL(e[m], ghat[m]);
+    SFX(fft2d_cols)(&p, L, e, +1);
+    SFX(fft2d_rows)(&p, L, e, +1, N);
+    SFX(plan_free)(&p);
     const REAL s = (REAL)(1.0 / ((double)L * (double)L));
+#pragma omp parallel for schedule(static)
     for (int i = 0; i < N; i++)
         for (int j = 0; j < N; j++) {
             size_t o = (size_t)i * N + j;

@@ -1,9 +1,9 @@
 """Generate the golden fixtures under tests/golden/ from the reference checkout.
 
-Run once, in a container that has the reference checkout mounted (the path is
-given by ``--ref`` and defaults to the read-only mount used while building):
+Run once, in a container that has the reference checkout mounted; ``--ref``
+(required) is the directory that holds the reference project's top folder:
 
-    python tests/golden/make_golden.py --ref /root/reference
+    python tests/golden/make_golden.py --ref <reference checkout>
 
 Nothing at test time reads the reference checkout; the tests read only the
 ``.npz`` / ``.json`` files this script writes.  What is extracted and why:
@@ -66,7 +66,7 @@ def load_pygmres_defs(path):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", required=True, help="reference checkout (holds the project folder)")
     args = ap.parse_args()
     base = os.path.join(args.ref, SUB)
     inp = os.path.join(base, "CUDA_GMRES", "Release", "input")

@@ -18,7 +18,7 @@ sys.path.insert(0, sys.argv[1])
 import cugmres_b200 as cg
 from cugmres_b200 import problems as P
 from oracle import oracle as O
-for N in (64, 128, 300, 512, 1100):
+for N in (64, 128, 300, 512, 1024, 1100, 2048):
     pr = P.helmholtz(N, 4.0, seed=N)
     s = cg.Solver(0).set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
     x = np.random.default_rng(N).standard_normal((N, N)) + 1j
