@@ -72,8 +72,8 @@ def parse():
     ap.add_argument("--no-extras", action="store_true", help="skip the mixed-precision and 256^2 side measurements")
     ap.add_argument("--no-learned", action="store_true", help="skip the learned-preconditioner side measurement")
     ap.add_argument("--learned-steps", type=int, default=1500)
-    ap.add_argument("--sweep", type=int, default=0, help="also solve a sweep of this many systems (config 4)")
-    ap.add_argument("--sweep-max-iter", type=int, default=3000)
+    ap.add_argument("--sweep", type=int, default=64, help="also solve a sweep of this many systems (config 4; 0: none)")
+    ap.add_argument("--sweep-max-iter", type=int, default=2000)
     return ap.parse_args()
 
 
@@ -326,34 +326,49 @@ def learned_side(args, stream):
     return out
 
 
-def sweep_side(args):
+def sweep_side(args, rank, world, device):
     """Config 4: independent systems with sides drawn from {96,...,512}, lambda/h
-    ~ U(15, 30), eps_r ~ U(2, 12), one design seed each, solved by
-    cugmres_solve_batch (operators built on the GPU, 8 worker contexts),
-    GMRES(200) to 1e-10 within --sweep-max-iter steps.  Wall time of the whole
-    batch call; per-system latency = set-up + solve."""
+    ~ U(15, 30), eps_r ~ U(2, 12), one design seed each, solved in lockstep
+    buckets (cugmres_solve_buckets: one launch per kernel per Arnoldi step for
+    all systems of a bucket, one CUDA-graph replay per restart cycle, operators
+    built on the GPU), GMRES(200) to 1e-10 within --sweep-max-iter steps.  With
+    N ranks the systems are sharded largest-first over the ranks (no collective
+    on the solve path); the job time is the maximum over ranks of each rank's
+    synchronous sweep call (it returns when its GPU work is done), and the
+    per-system records are gathered to every rank."""
     import cugmres_b200 as cg
+    from cugmres_b200 import dist as D
     from cugmres_b200 import problems as P
     systems = P.sweep(nsys=args.sweep, seed=0, with_green=False)
-    # untimed: one short solve per grid side on one worker, so every embedding
-    # size is autotuned on a quiet GPU (a one-time cost per device, cached on
-    # disk) before the clock starts
+    kw = dict(device=device, mode="buckets", restart=200, tol=args.tol)
+    # untimed: one short solve per grid side of this rank's share, so every
+    # embedding size is autotuned before the clock starts
+    mine = D.shard_systems([s["N"] for s in systems], rank, world)
     warm, seen = [], set()
-    for s in systems:
-        if s["N"] not in seen:
-            seen.add(s["N"])
-            warm.append(s)
-    cg.solve_batch(warm, workers=1, restart=200, max_iter=50, tol=args.tol)
-    t0 = time.perf_counter()
-    xs, infos = cg.solve_batch(systems, workers=8, restart=200, max_iter=args.sweep_max_iter, tol=args.tol)
-    wall = time.perf_counter() - t0
-    lat = np.array([i["seconds"] for i in infos])
-    conv = [i for i in infos if i["status"] == 0]
-    return {"systems": len(infos), "converged": len(conv), "wall_s": wall, "solves_per_s": len(infos) / wall,
-            "latency_p50_s": float(np.percentile(lat, 50)), "latency_p99_s": float(np.percentile(lat, 99)),
-            "arnoldi_steps": int(sum(i["iterations"] for i in infos)),
-            "matvecs_per_s": float(sum(i["iterations"] + i["cycles"] for i in infos) / wall),
-            "note": f"GMRES(200), tol {args.tol:g}, at most {args.sweep_max_iter} steps per system"}
+    for i in mine:
+        if systems[i]["N"] not in seen:
+            seen.add(systems[i]["N"])
+            warm.append(systems[i])
+    if warm:
+        cg.solve_batch(warm, max_iter=20, **kw)
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+    def solve_fn(lst):
+        return cg.solve_batch(lst, max_iter=args.sweep_max_iter, **kw)[1]
+
+    records, stats = D.run_sweep(systems, rank, world, solve_fn, device=f"cuda:{device}")
+    stats.update({"gpus": world, "matvecs_per_s": float(sum(r["iterations"] + r["cycles"] for r in records) /
+                                                        stats["wall_s"]) if stats["wall_s"] else None,
+                  "arnoldi_steps": int(sum(r["iterations"] for r in records)),
+                  "by_side": {str(N): {"systems": sum(1 for r in records if r["N"] == N),
+                                       "converged": sum(1 for r in records if r["N"] == N and r["status"] == 0)}
+                              for N in sorted({r["N"] for r in records})},
+                  "note": (f"GMRES(200), tol {args.tol:g}, at most {args.sweep_max_iter} steps per system; "
+                           "latency = from the start of the system's bucket (set-up included) to the cycle "
+                           "at which it finished")})
+    return stats
 
 
 def run_reference(args, rank, world):
@@ -516,8 +531,9 @@ def main():
         line["side"] = side_measurements(args, stream)
         if not args.no_learned:
             line["side"]["learned"] = learned_side(args, stream)
-    if rank == 0 and world == 1 and args.sweep > 0:
-        line.setdefault("side", {})["sweep"] = sweep_side(args)
+    if args.sweep > 0:
+        sw = sweep_side(args, rank, world, local)
+        line.setdefault("side", {})["sweep"] = sw
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:

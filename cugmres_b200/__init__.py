@@ -221,14 +221,21 @@ class Solver:
 
 
 def solve_batch(systems, device=0, workers=8, restart=100, max_iter=10000, tol=1e-10, precision="fp64",
-                givens="unitary", inner_tol=1e-5, ortho="dcgs2", device_green=False):
-    """Solve many independent systems concurrently (cugmres_solve_batch).
+                givens="unitary", inner_tol=1e-5, ortho="dcgs2", device_green=False, mode="buckets", max_bucket=0):
+    """Solve many independent systems.
+
+    mode="buckets" (cugmres_solve_buckets): systems of one grid side are solved
+    in lockstep, every Arnoldi-step kernel one launch for the whole bucket and
+    every restart cycle one CUDA-graph replay (FP64, delayed CGS2; max_bucket
+    caps the systems per bucket, 0 = as many as fit in half the free memory).
+    mode="contexts" (cugmres_solve_batch): `workers` concurrent contexts, each
+    with its own stream, take systems largest first (any precision / scheme).
 
     systems: iterable of dicts with g_block (or k0 and h: the GFIEM block is
     then built on the GPU; device_green=True forces that), chi, chi_scale, b
     and optionally x0.
     Returns (xs, infos): solutions (complex128 N x N) and per-system dicts with
-    status, iterations, rel_residual_true and seconds (set-up + solve latency)."""
+    status, iterations, rel_residual_true and seconds (latency)."""
     systems = list(systems)
     keep, arr = [], (_lib.CgSystem * max(1, len(systems)))()
     xs = []
@@ -248,8 +255,15 @@ def solve_batch(systems, device=0, workers=8, restart=100, max_iter=10000, tol=1
     o.restart, o.max_iter, o.tol = int(restart), int(max_iter), float(tol)
     o.precision, o.givens, o.inner_tol, o.ortho = _PREC[precision], _GIV[givens], float(inner_tol), _ORTHO[ortho]
     res = (_lib.CgResult * max(1, len(systems)))()
-    check(_lib.lib().cugmres_solve_batch(int(device), len(systems), arr, ctypes.byref(o), int(workers), res),
-          "cugmres_solve_batch")
+    if mode == "buckets":
+        o.zero_x0 = int(all(sysd.get("x0") is None for sysd in systems))
+        check(_lib.lib().cugmres_solve_buckets(int(device), len(systems), arr, ctypes.byref(o), int(max_bucket), res),
+              "cugmres_solve_buckets")
+    elif mode == "contexts":
+        check(_lib.lib().cugmres_solve_batch(int(device), len(systems), arr, ctypes.byref(o), int(workers), res),
+              "cugmres_solve_batch")
+    else:
+        raise ValueError(mode)
     infos = [dict(status=r.status, status_text=_lib.strerror(r.status), iterations=r.iterations, cycles=r.cycles,
                   rel_residual_true=r.rel_residual_true, rel_residual_estimate=r.rel_residual_estimate,
                   seconds=r.seconds) for r in res[: len(systems)]]

@@ -41,7 +41,7 @@ EXPORTS = (
     "cugmres_fno_info", "cugmres_fno_get_params", "cugmres_fno_set_params", "cugmres_fno_forward",
     "cugmres_fno_loss_grad", "cugmres_fno_train_step", "cugmres_set_preconditioner", "cugmres_gemm_bf16",
     "cugmres_matvec_transpose", "cugmres_fno_forward_train", "cugmres_fno_backward", "cugmres_fno_set_local_last",
-    "cugmres_set_operator_green", "cugmres_green_block_device",
+    "cugmres_set_operator_green", "cugmres_green_block_device", "cugmres_solve_buckets",
 )
 
 PHASES = ("matvec", "dots", "axpy", "small", "update", "residual", "precond")
@@ -157,6 +157,8 @@ def _declare(L):
     L.cugmres_matvec_shapes.argtypes = [P, I, ctypes.POINTER(I)]
     L.cugmres_solve_batch.argtypes = [I, I, ctypes.POINTER(CgSystem), ctypes.POINTER(CgOpts), I,
                                       ctypes.POINTER(CgResult)]
+    L.cugmres_solve_buckets.argtypes = [I, I, ctypes.POINTER(CgSystem), ctypes.POINTER(CgOpts), I,
+                                        ctypes.POINTER(CgResult)]
     L.cugmres_profile.argtypes = [P, I]
     L.cugmres_profile_read.argtypes = [P, ctypes.POINTER(CgPhaseStats)]
     LL, ULL = ctypes.c_longlong, ctypes.c_ulonglong

@@ -89,6 +89,18 @@ namespace cg {
 void ctx_set_shared_gpu(cg_ctx *c, bool on) {
     if (c) c->shared_gpu = on;
 }
+int ctx_op_view(const cg_ctx *c, OpView *v) {
+    if (!c || !v || !c->have_op) return CG_ERR_NO_OPERATOR;
+    v->N = c->N;
+    v->L = c->L;
+    v->sms = c->sms;
+    for (int p = 0; p < 3; p++) v->var[p] = c->var[0][p];
+    v->gq64 = c->gq64;
+    v->c64 = c->c64;
+    v->tw64 = c->tw64;
+    v->stream = c->stream;
+    return CG_OK;
+}
 }  // namespace cg
 
 namespace {
@@ -397,7 +409,7 @@ int autotune(cg_ctx *c, int prec) {
     }
     // the key carries the tuner's version so that choices made by an older
     // tuner or for older kernels are not reused
-    std::string key = std::string(c->devname) + "|" + std::to_string(c->L) + "|" + std::to_string(prec) + "|t2" +
+    std::string key = std::string(c->devname) + "|" + std::to_string(c->L) + "|" + std::to_string(prec) + "|t3" +
                       (c->shared_gpu ? "s" : "");
     for (char &ch : key)
         if (ch == ' ') ch = '_';

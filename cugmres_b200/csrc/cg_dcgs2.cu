@@ -176,6 +176,8 @@ __device__ __forceinline__ double warp_sum4_scatter(double a0, double a1, double
 }
 template <typename CV, int U>
 __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -243,6 +245,8 @@ __global__ void __launch_bounds__(D2_THREADS, 2) k_dots2t(const CV *__restrict__
 // without atomics; block partials and the last-block sum as in k_dots2t.
 template <typename CV, int U>
 __global__ void __launch_bounds__(D2_THREADS) k_dots2s(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -304,6 +308,8 @@ __global__ void __launch_bounds__(D2_THREADS) k_dots2s(const CV *__restrict__ V,
 
 template <typename CV, bool COMP, int D2_J, int U>
 __global__ void __launch_bounds__(D2_THREADS) k_dots2(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     DevState *st = kp.st;
     if (st->stop) return;
     const int k = st->k;
@@ -490,6 +496,7 @@ static __device__ __forceinline__ void block_sum4(double &a, double &b, double &
 // One block: normalisation of q_k, column k-1 of H, Givens update, residual
 // estimate, stop decision and the coefficients of the axpy pass.
 __global__ void __launch_bounds__(STEP_THREADS) k_dcgs2_step(KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
     DevState *st = kp.st;
     if (st->stop) return;
     extern __shared__ __align__(16) unsigned char smraw[];
@@ -689,6 +696,8 @@ __device__ __forceinline__ void axpy2_prologue(const KrylovPtrs &kp, const DevSt
 // the current one is accumulated into both outputs.
 template <typename CV, int U>
 __global__ void __launch_bounds__(AX2_THREADS, 2) k_axpy2t(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     typedef typename real_of<CV>::type R;
     typedef typename scalar_of<CV>::type CS;
     DevState *st = kp.st;
@@ -753,6 +762,8 @@ __global__ void __launch_bounds__(AX2_THREADS, 2) k_axpy2t(CV *__restrict__ V, l
 // Shared memory: P, S coefficients (2 (mcap+1) elements) + 2 * warps * 32U elements.
 template <typename CV, int U>
 __global__ void __launch_bounds__(AX2_THREADS) k_axpy2s(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     typedef typename real_of<CV>::type R;
     constexpr int W = AX2_THREADS / 32;
     constexpr int TILE = 32 * U;
@@ -823,6 +834,8 @@ __global__ void __launch_bounds__(AX2_THREADS) k_axpy2s(CV *__restrict__ V, long
 
 template <typename CV, int JU>
 __global__ void __launch_bounds__(AX2_THREADS) k_axpy2(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -1045,9 +1058,16 @@ int dots2_blocks(int prec_v, int sms, int mcap, long long n) {
 int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
     const int v = dots2_shape(prec_v, n, sms);
     const size_t smem = dots2_smem(v, kp.mcap);
-    if (dots2_vec(prec_v, n, v)) dots2_vec_kernel(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const float4 *)V, n / 2, kp);
-    else if (prec_v == 0) dots2_kernel<double2, false>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const double2 *)V, n, kp);
-    else dots2_kernel<float2, true>(v, smem)<<<nblk, D2_THREADS, smem, s>>>((const float2 *)V, n, kp);
+    const dim3 grid(nblk, kp.nsys);
+    if (dots2_vec(prec_v, n, v)) {
+        KrylovPtrs kq = kp;
+        kq.sys_v = kp.sys_v / 2;  // the basis in pairs of complex values
+        dots2_vec_kernel(v, smem)<<<grid, D2_THREADS, smem, s>>>((const float4 *)V, n / 2, kq);
+    } else if (prec_v == 0) {
+        dots2_kernel<double2, false>(v, smem)<<<grid, D2_THREADS, smem, s>>>((const double2 *)V, n, kp);
+    } else {
+        dots2_kernel<float2, true>(v, smem)<<<grid, D2_THREADS, smem, s>>>((const float2 *)V, n, kp);
+    }
     return (int)cudaGetLastError();
 }
 
@@ -1058,7 +1078,7 @@ int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s) {
         cudaError_t e = cudaFuncSetAttribute(k_dcgs2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return (int)e;
     }
-    k_dcgs2_step<<<1, STEP_THREADS, smem, s>>>(kp);
+    k_dcgs2_step<<<dim3(1, kp.nsys), STEP_THREADS, smem, s>>>(kp);
     return (int)cudaGetLastError();
 }
 
@@ -1107,14 +1127,17 @@ int axpy2_blocks(int prec_v, int sms, int mcap, long long n) {
 int launch_axpy2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, int nblk, int sms, cudaStream_t s) {
     const int v = axpy2_shape(prec_v, n, sms);
     const size_t smem = axpy2_smem(v, prec_v, kp.mcap);
+    const dim3 grid(nblk, kp.nsys);
     if (axpy2_vec(prec_v, n, v)) {
-        axpy2_vec_kernel(v, smem)<<<nblk, AX2_THREADS, smem, s>>>((float4 *)V, n / 2, kp);
+        KrylovPtrs kq = kp;
+        kq.sys_v = kp.sys_v / 2;  // the basis in pairs of complex values
+        axpy2_vec_kernel(v, smem)<<<grid, AX2_THREADS, smem, s>>>((float4 *)V, n / 2, kq);
         return (int)cudaGetLastError();
     }
     int e = prec_v == 0 ? axpy2_prepare<double2>(v, smem) : axpy2_prepare<float2>(v, smem);
     if (e) return e;
-    if (prec_v == 0) Axpy2Table<double2>::get(v)<<<nblk, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
-    else Axpy2Table<float2>::get(v)<<<nblk, AX2_THREADS, smem, s>>>((float2 *)V, n, kp);
+    if (prec_v == 0) Axpy2Table<double2>::get(v)<<<grid, AX2_THREADS, smem, s>>>((double2 *)V, n, kp);
+    else Axpy2Table<float2>::get(v)<<<grid, AX2_THREADS, smem, s>>>((float2 *)V, n, kp);
     return (int)cudaGetLastError();
 }
 

@@ -221,10 +221,22 @@ __host__ __device__ inline int twiddle_exponent(int L, int E0, int i) {
     return -1;
 }
 
+// Barrier of the threads that share one transform: the whole block (NT = 0)
+// or the NT threads of named barrier `id` (1..15; NT a multiple of 32), so
+// that several transforms in one block do not wait on each other.
+template <int NT> __device__ __forceinline__ void fft_barrier(int id) {
+    if constexpr (NT == 0) {
+        __syncthreads();
+    } else {
+        static_assert(NT % 32 == 0, "named barriers count whole warps");
+        asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(NT) : "memory");
+    }
+}
+
 // One Stockham stage S of a length-L transform (compile-time radix and span).
 // tmp holds the previous stage's butterfly outputs (tmp[b*Rp + q]) on entry
 // and this stage's outputs on exit; the last stage stores canonical reg.
-template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
+template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS, int NT = 0> struct Stage {
     typedef Plan<L, E0> P;
     static constexpr int E = P::E;
     static constexpr int TPR = P::TPR;
@@ -232,13 +244,14 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
     static constexpr int Ns = P::span(S);
     static constexpr int NB = E / R;  // butterflies per thread in this stage
     template <typename C>
-    static __device__ __forceinline__ void run(C (&reg)[E], C (&tmp)[E], C *sm, const C *__restrict__ tw, int t) {
+    static __device__ __forceinline__ void run(C (&reg)[E], C (&tmp)[E], C *sm, const C *__restrict__ tw, int t,
+                                               int bar) {
         if constexpr (S > 0) {
             // write the previous stage's outputs, then read this stage's inputs
             constexpr int Rp = P::radix(S - 1);
             constexpr int Nsp = P::span(S - 1);
             constexpr int NBp = E / Rp;
-            __syncthreads();
+            fft_barrier<NT>(bar);
 #pragma unroll
             for (int b = 0; b < NBp; b++) {
                 const int j = t + b * TPR;
@@ -246,7 +259,7 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
 #pragma unroll
                 for (int q = 0; q < Rp; q++) sm[P::pad(base + q * Nsp) * SMS] = tmp[b * Rp + q];
             }
-            __syncthreads();
+            fft_barrier<NT>(bar);
 #pragma unroll
             for (int b = 0; b < NB; b++) {
                 const int j = t + b * TPR;
@@ -276,7 +289,7 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
 #pragma unroll
                 for (int q = 0; q < R; q++) reg[b + q * NB] = tmp[b * R + q];
         } else {
-            Stage<L, E0, INV, HALF_IN, S + 1, SMS>::run(reg, tmp, sm, tw, t);
+            Stage<L, E0, INV, HALF_IN, S + 1, SMS, NT>::run(reg, tmp, sm, tw, t, bar);
         }
     }
 };
@@ -287,13 +300,14 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS> struct Stage {
 // (SMS > 1 interleaves the regions of SMS transforms element by element, which
 // keeps the column kernels' accesses on distinct banks).
 // HALF_IN: inputs L/2 .. L-1 are zero (first stage uses dft_half_input).
-// Every thread of the block must call this the same number of times
-// (it contains __syncthreads()).  tw is the base of the 4 L-entry table set
-// (tw_table picks the plan's and direction's table).
-template <int L, int E0, bool INV, bool HALF_IN, int SMS = 1, typename C>
-__device__ __forceinline__ void fft_run(C (&reg)[Plan<L, E0>::E], C *sm, const C *__restrict__ tw, int t) {
+// Every thread of the block (NT = 0), or of named barrier `bar` (NT threads),
+// must call this the same number of times (it contains barriers).  tw is the
+// base of the 4 L-entry table set (tw_table picks the plan's and direction's table).
+template <int L, int E0, bool INV, bool HALF_IN, int SMS = 1, int NT = 0, typename C>
+__device__ __forceinline__ void fft_run(C (&reg)[Plan<L, E0>::E], C *sm, const C *__restrict__ tw, int t,
+                                        int bar = 0) {
     C tmp[Plan<L, E0>::E];
-    Stage<L, E0, INV, HALF_IN, 0, SMS>::run(reg, tmp, sm, tw_table<L, E0, INV>(tw), t);
+    Stage<L, E0, INV, HALF_IN, 0, SMS, NT>::run(reg, tmp, sm, tw_table<L, E0, INV>(tw), t, bar);
 }
 
 }  // namespace cg

@@ -63,7 +63,30 @@ struct KrylovPtrs {
     double *gpart;   // [ceil(nblk_dots2 / 16) * 4 * part_ld] group sums of the dot partials
     unsigned int *tickets;  // [ceil(nblk_dots2 / 16)] arrival counters of those groups (reset by the last)
     int mcap;        // allocated restart capacity (leading dimension of Rm / part)
+    // Bucket of systems solved in lockstep (one launch covers all of them,
+    // system = blockIdx.y): every array above (st included) of system s lies
+    // s * sys_ws bytes after system 0's, and its basis s * sys_v elements after
+    // V.  A single solve has nsys = 1 and zero strides.
+    long long sys_ws = 0;
+    long long sys_v = 0;
+    int nsys = 1;
 };
+
+// This block's system of a bucket: kp with every workspace pointer moved to
+// system blockIdx.y (no change for a single solve).
+__device__ __forceinline__ KrylovPtrs kp_sys(KrylovPtrs kp) {
+    if (kp.sys_ws == 0) return kp;
+    const long long o = (long long)blockIdx.y * kp.sys_ws;
+#define CG_MOVE(f) kp.f = reinterpret_cast<decltype(kp.f)>(reinterpret_cast<char *>(kp.f) + o)
+    CG_MOVE(st); CG_MOVE(scale); CG_MOVE(h1); CG_MOVE(h2); CG_MOVE(Rm); CG_MOVE(cs); CG_MOVE(sn);
+    CG_MOVE(g); CG_MOVE(y); CG_MOVE(hist); CG_MOVE(part); CG_MOVE(npart); CG_MOVE(Hm); CG_MOVE(D1);
+    CG_MOVE(D2); CG_MOVE(tv); CG_MOVE(P); CG_MOVE(S); CG_MOVE(gpart); CG_MOVE(tickets);
+#undef CG_MOVE
+    return kp;
+}
+template <typename T> __device__ __forceinline__ T *sys_vec(T *V, const KrylovPtrs &kp) {
+    return V + (long long)blockIdx.y * kp.sys_v;
+}
 
 // Matvec launch parameters for one precision (C = double2 or float2, R its real type).
 struct MatvecArgs {
@@ -75,7 +98,23 @@ struct MatvecArgs {
     void *T;            // N x L intermediate (C)
     int transpose = 0;  // 1: A^T x = x - diag(c) G x (contrast applied after the convolution)
     int sms = 148;      // multiprocessors of the device (grid of the persistent column pass)
+    int nsys = 1;       // systems of a bucket (grid.y of every pass)
+    // per-system strides of a bucket: workspace bytes (DevState, scale and the
+    // norm partials move with it), then elements of the contrast, of T, of the
+    // quarter spectrum and of the right-hand side
+    long long sys_ws = 0, sys_c = 0, sys_T = 0, sys_gq = 0, sys_b = 0;
 };
+
+// The per-system strides a matvec kernel needs (see MatvecArgs).
+struct SysSel {
+    long long ws, c, T, gq, b;
+};
+inline SysSel sys_sel(const MatvecArgs &a) { return SysSel{a.sys_ws, a.sys_c, a.sys_T, a.sys_gq, a.sys_b}; }
+template <typename T> __device__ __forceinline__ T *sys_move_bytes(T *p, long long stride_bytes) {
+    return p ? reinterpret_cast<T *>(reinterpret_cast<char *>(const_cast<void *>((const void *)p)) +
+                                     (long long)blockIdx.y * stride_bytes)
+             : p;
+}
 
 // Reference to a basis vector selected by the device-side Arnoldi index:
 // ptr = base + (st ? st->k + koff : 0) * stride.
@@ -83,6 +122,7 @@ struct VecSel {
     void *base;
     long long stride;
     int koff;
+    long long sys = 0;  // elements between the vectors of consecutive systems of a bucket
 };
 
 // kernel launchers (cg_matvec.cu)
@@ -101,6 +141,17 @@ int matvec_variant_persistent(int v);
 // marks a context whose GPU is shared with other contexts' solves (set by the
 // batch solver before its first operator)
 void ctx_set_shared_gpu(cg_ctx *c, bool on);
+// Device buffers of a context's current operator (FP64), read by the bucket
+// solver, which copies each system's spectrum and contrast into its own arrays.
+struct OpView {
+    int N, L, sms;
+    int var[3];  // FP64 launch shapes of the three matvec passes
+    const double2 *gq64;
+    const double *c64;
+    const double2 *tw64;
+    cudaStream_t stream;
+};
+int ctx_op_view(const cg_ctx *c, OpView *v);
 
 // full (unpruned) forward 2D transform of an L x L FP64 array, used to build the spectrum
 int launch_fft2d_full_fp64(int L, double2 *a, const double2 *tw, cudaStream_t s);

@@ -58,10 +58,14 @@ static __device__ __forceinline__ bool last_block(unsigned int *ticket) {
 template <typename CV, typename CW, bool COMP>
 __global__ void __launch_bounds__(DOT_THREADS)
 k_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp, VecSel w, double2 *__restrict__ out, int ctr, int gate) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     DevState *st = kp.st;
     if (gate == GATE_STOP && st->stop) return;
     const int nj = st->k + 1;
-    const CW *wv = reinterpret_cast<const CW *>(w.base) + (long long)(st->k + w.koff) * w.stride;
+    const CW *wv = reinterpret_cast<const CW *>(w.base) + (long long)(st->k + w.koff) * w.stride +
+                   (long long)blockIdx.y * w.sys;
+    out = sys_move_bytes(out, kp.sys_ws);
     long long e0, e1;
     block_range(n, gridDim.x, blockIdx.x, e0, e1);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -144,10 +148,13 @@ template <typename CV, typename CW>
 __global__ void __launch_bounds__(AXPY_THREADS)
 k_axpy(const CV *__restrict__ V, long long n, KrylovPtrs kp, const double2 *__restrict__ src, double sign, int nj_mode,
        VecSel w, int want_norm, int ctr, int gate) {
+    kp = kp_sys(kp);  // this block's system of a bucket
+    V = sys_vec(V, kp);
     typedef typename real_of<CW>::type R;
     DevState *st = kp.st;
     if (gate == GATE_STOP && st->stop) return;
     const int nj = (nj_mode == NJ_K_PLUS_1) ? st->k + 1 : (nj_mode == NJ_K ? st->k : st->ncol);
+    src = sys_move_bytes(src, kp.sys_ws);
     extern __shared__ __align__(16) unsigned char smraw[];
     CW *coef = reinterpret_cast<CW *>(smraw);
     __shared__ double wsum[AXPY_THREADS / 32];
@@ -157,7 +164,7 @@ k_axpy(const CV *__restrict__ V, long long n, KrylovPtrs kp, const double2 *__re
         coef[j] = mk<CW>((R)(v.x * s), (R)(v.y * s));
     }
     __syncthreads();
-    CW *wv = reinterpret_cast<CW *>(w.base) + (long long)(st->k + w.koff) * w.stride;
+    CW *wv = reinterpret_cast<CW *>(w.base) + (long long)(st->k + w.koff) * w.stride + (long long)blockIdx.y * w.sys;
     double nrm = 0.0;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += stride) {
@@ -211,6 +218,7 @@ k_axpy(const CV *__restrict__ V, long long n, KrylovPtrs kp, const double2 *__re
 //             J(i,i) = J(i+1,i+1) = Htemp(i,i)/rho, J(i,i+1) = Htemp(i+1,i)/rho,
 //             J(i+1,i) = -conj(Htemp(i+1,i))/rho).
 __global__ void k_givens(KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
     DevState *st = kp.st;
     if (st->stop) return;
     const int k = st->k;
@@ -278,6 +286,7 @@ __global__ void k_givens(KrylovPtrs kp) {
 // One warp: y = R^{-1} g for the kk = st->k columns of this cycle, column-
 // oriented so the lanes update the remaining right-hand side in parallel.
 __global__ void k_backsolve(KrylovPtrs kp) {
+    kp = kp_sys(kp);  // this block's system of a bucket
     DevState *st = kp.st;
     const int kk = st->ncol;
     const int ld = kp.mcap + 1;
@@ -306,6 +315,7 @@ __global__ void k_backsolve(KrylovPtrs kp) {
 // One warp: ||r||^2 partials of the residual pass -> beta, true residual,
 // convergence / budget / breakdown decisions, reset of the cycle state.
 __global__ void k_cycle_begin(KrylovPtrs kp, int nparts) {
+    kp = kp_sys(kp);  // this block's system of a bucket
     DevState *st = kp.st;
     const int lane = threadIdx.x;
     double acc = 0.0;
@@ -323,6 +333,10 @@ __global__ void k_cycle_begin(KrylovPtrs kp, int nparts) {
     if (st->cycles == 0) kp.hist[0] = rel;
     st->k = 0;
     st->ncol = 0;
+    if (st->status != 0) {  // a system of a bucket that has finished stays finished
+        st->stop = 1;
+        return;
+    }
     int stop = 0;
     if (!isfinite(beta)) {
         st->status = 4;
@@ -389,9 +403,9 @@ __global__ void k_convert(const CI *__restrict__ a, CO *__restrict__ b, long lon
 int launch_dots(int prec_v, const void *V, long long n, const KrylovPtrs &kp, VecSel w, double2 *out, int ctr,
                 int nblk, int gate, cudaStream_t s) {
     if (prec_v == 0)
-        k_dots<double2, double2, false><<<nblk, DOT_THREADS, 0, s>>>((const double2 *)V, n, kp, w, out, ctr, gate);
+        k_dots<double2, double2, false><<<dim3(nblk, kp.nsys), DOT_THREADS, 0, s>>>((const double2 *)V, n, kp, w, out, ctr, gate);
     else
-        k_dots<float2, float2, true><<<nblk, DOT_THREADS, 0, s>>>((const float2 *)V, n, kp, w, out, ctr, gate);
+        k_dots<float2, float2, true><<<dim3(nblk, kp.nsys), DOT_THREADS, 0, s>>>((const float2 *)V, n, kp, w, out, ctr, gate);
     return (int)cudaGetLastError();
 }
 
@@ -409,13 +423,13 @@ int launch_axpy(int prec_v, int prec_w, const void *V, long long n, const Krylov
     else if (prec_v == 1 && prec_w == 0) e = smem_attr(k_axpy<float2, double2>, smem);
     if (e) return e;
     if (prec_v == 0 && prec_w == 0)
-        k_axpy<double2, double2><<<nblk, AXPY_THREADS, smem, s>>>((const double2 *)V, n, kp, src, sign, nj_mode, w,
+        k_axpy<double2, double2><<<dim3(nblk, kp.nsys), AXPY_THREADS, smem, s>>>((const double2 *)V, n, kp, src, sign, nj_mode, w,
                                                                     want_norm, ctr, gate);
     else if (prec_v == 1 && prec_w == 1)
-        k_axpy<float2, float2><<<nblk, AXPY_THREADS, smem, s>>>((const float2 *)V, n, kp, src, sign, nj_mode, w,
+        k_axpy<float2, float2><<<dim3(nblk, kp.nsys), AXPY_THREADS, smem, s>>>((const float2 *)V, n, kp, src, sign, nj_mode, w,
                                                                   want_norm, ctr, gate);
     else if (prec_v == 1 && prec_w == 0)
-        k_axpy<float2, double2><<<nblk, AXPY_THREADS, smem, s>>>((const float2 *)V, n, kp, src, sign, nj_mode, w,
+        k_axpy<float2, double2><<<dim3(nblk, kp.nsys), AXPY_THREADS, smem, s>>>((const float2 *)V, n, kp, src, sign, nj_mode, w,
                                                                    want_norm, ctr, gate);
     else
         return -1;
@@ -423,7 +437,7 @@ int launch_axpy(int prec_v, int prec_w, const void *V, long long n, const Krylov
 }
 
 int launch_givens(const KrylovPtrs &kp, cudaStream_t s) {
-    k_givens<<<1, 32, 0, s>>>(kp);
+    k_givens<<<dim3(1, kp.nsys), 32, 0, s>>>(kp);
     return (int)cudaGetLastError();
 }
 
@@ -431,7 +445,7 @@ int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s) {
     const size_t smem = (size_t)(kp.mcap + 1) * sizeof(double2);
     int e = smem_attr(k_backsolve, smem);
     if (e) return e;
-    k_backsolve<<<1, 32, smem, s>>>(kp);
+    k_backsolve<<<dim3(1, kp.nsys), 32, smem, s>>>(kp);
     return (int)cudaGetLastError();
 }
 
@@ -440,18 +454,19 @@ int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s) {
 // delayed-CGS2 cycles): the only mode-specific part of a cycle's start is the
 // lazy normalisation of V_0 that CGS2 keeps in scale[0].
 __global__ void k_set_ortho(KrylovPtrs kp, int ortho) {
+    kp = kp_sys(kp);  // this block's system of a bucket
     DevState *st = kp.st;
     st->ortho = ortho;
     if (!st->stop) kp.scale[0] = ortho == 1 ? 1.0 / st->beta0 : 1.0;
 }
 
 int launch_set_ortho(const KrylovPtrs &kp, int ortho, cudaStream_t s) {
-    k_set_ortho<<<1, 1, 0, s>>>(kp, ortho);
+    k_set_ortho<<<dim3(1, kp.nsys), 1, 0, s>>>(kp, ortho);
     return (int)cudaGetLastError();
 }
 
 int launch_cycle_begin(const KrylovPtrs &kp, int nparts, cudaStream_t s) {
-    k_cycle_begin<<<1, 32, 0, s>>>(kp, nparts);
+    k_cycle_begin<<<dim3(1, kp.nsys), 32, 0, s>>>(kp, nparts);
     return (int)cudaGetLastError();
 }
 

@@ -62,7 +62,12 @@ typedef MvShape<8, 256, 512, 512, 1, 1> MvV6;   // V2 with the pipelined column 
 // against 53.4 us (one column per 128-thread block: its loads use 16 of each
 // 32-byte sector of T).
 typedef MvShape<16, 256, 128, 256, 2> MvV7;
-constexpr int MV_VARIANTS = 8;
+// V0's transforms with the grouped pipelined column pass (k_cols_convolve_grp):
+// each column transform of a block is an independent worker with its own
+// staging and named barrier, so one transform's shared-memory exchanges can
+// overlap another's butterflies instead of the whole block stepping together.
+typedef MvShape<16, 256, 256, 512, 1, 2> MvV8;
+constexpr int MV_VARIANTS = 9;
 
 template <int L, typename SH> struct RowCfg {
     typedef Plan<L, SH::E> P;
@@ -87,17 +92,21 @@ template <int L, typename SH, int ESZ> struct ColCfg {
 template <typename C, int L, typename SH>
 __global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
 k_rows_forward(VecSel xs, const double *__restrict__ xscale, const typename real_of<C>::type *__restrict__ cdiag,
-               C *__restrict__ T, const C *__restrict__ tw, int N, const DevState *st, int gate) {
+               C *__restrict__ T, const C *__restrict__ tw, int N, const DevState *st, int gate, SysSel sy) {
     typedef typename real_of<C>::type R;
     typedef Plan<L, SH::E> P;
     constexpr int E = P::E, TPR = P::TPR;
+    st = sys_move_bytes(st, sy.ws);
     if (gated(st, gate)) return;
+    xscale = sys_move_bytes(xscale, sy.ws);
+    if (cdiag) cdiag += (long long)blockIdx.y * sy.c;
+    T += (long long)blockIdx.y * sy.T;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int lr = threadIdx.x / TPR, t = threadIdx.x % TPR;
     C *sm = reinterpret_cast<C *>(smraw) + lr * P::SMEM_ELEMS;
     const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
     const long long ks = sel_index(st, xs.koff);
-    const C *x = reinterpret_cast<const C *>(xs.base) + ks * xs.stride;
+    const C *x = reinterpret_cast<const C *>(xs.base) + ks * xs.stride + (long long)blockIdx.y * xs.sys;
     const R s = xscale ? (R)xscale[ks] : (R)1;
     C reg[E];
     const bool live = row < N;
@@ -124,11 +133,14 @@ k_rows_forward(VecSel xs, const double *__restrict__ xscale, const typename real
 template <typename C, int L, typename SH>
 __global__ void __launch_bounds__(ColCfg<L, SH, sizeof(C)>::THREADS, SH::MINB)
 k_cols_convolve(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict__ tw, int N, const DevState *st,
-                int gate) {
+                int gate, SysSel sy) {
     typedef Plan<L, SH::E> P;
     typedef ColCfg<L, SH, sizeof(C)> Q;
     constexpr int E = P::E, TPR = P::TPR, CPB = Q::CPB;
+    st = sys_move_bytes(st, sy.ws);
     if (gated(st, gate)) return;
+    T += (long long)blockIdx.y * sy.T;
+    gq += (long long)blockIdx.y * sy.gq;
     extern __shared__ __align__(16) unsigned char smraw[];
     const int cl = threadIdx.x % CPB, t = threadIdx.x / CPB;
     C *sm = reinterpret_cast<C *>(smraw) + cl;
@@ -193,12 +205,15 @@ template <int L, typename SH, int ESZ> struct PipeCfg {
 template <typename C, int L, typename SH>
 __global__ void __launch_bounds__(ColCfg<L, SH, sizeof(C)>::THREADS, 1)
 k_cols_convolve_pipe(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict__ tw, int N, const DevState *st,
-                     int gate) {
+                     int gate, SysSel sy) {
     typedef Plan<L, SH::E> P;
     typedef ColCfg<L, SH, sizeof(C)> Q;
     typedef PipeCfg<L, SH, sizeof(C)> G;
     constexpr int E = P::E, TPR = P::TPR, CPB = Q::CPB, THREADS = Q::THREADS, LQ = G::LQ;
+    st = sys_move_bytes(st, sy.ws);
     if (gated(st, gate)) return;
+    T += (long long)blockIdx.y * sy.T;
+    gq += (long long)blockIdx.y * sy.gq;
     extern __shared__ __align__(16) unsigned char smraw[];
     C *sx = reinterpret_cast<C *>(smraw);  // FFT exchange, Q::SMEM_ELEMS
     C *buf = sx + Q::SMEM_ELEMS;           // two staging slots
@@ -257,18 +272,108 @@ k_cols_convolve_pipe(C *__restrict__ T, const C *__restrict__ gq, const C *__res
     cp_async_wait<0>();
 }
 
+// Pass 2, grouped: the G = CPB column transforms of a block are independent
+// workers.  Worker w = blockIdx.x G + g walks columns w, w + W, ... (W = gridDim.x
+// G); it stages its next column (rows 0..N-1 of T) and that column's
+// quarter-spectrum column into its own half of a double buffer with cp.async
+// while it transforms the current one, and its barriers are the named barrier
+// 1 + g of its TPR threads only.  Same arithmetic, in the same order, as
+// k_cols_convolve.  Used where TPR is a whole number of warps and G <= 15
+// (GrpCfg::OK); otherwise the shape falls back to k_cols_convolve_pipe.
+template <int L, typename SH, int ESZ> struct GrpCfg {
+    typedef Plan<L, SH::E> P;
+    typedef ColCfg<L, SH, ESZ> Q;
+    static constexpr int TPR = P::TPR;
+    static constexpr int G = Q::CPB;
+    static constexpr int THREADS = Q::THREADS;
+    static constexpr bool OK = (TPR % 32 == 0) && G <= 15;
+    static constexpr int NT = G > 1 ? TPR : 0;  // one group: block barrier
+    static constexpr int LQ = L / 2 + 1;
+    static constexpr int TD = L / 2;               // staged column: rows < L/2 (N <= L/2)
+    static constexpr int GD = ((LQ + 1) / 2) * 2;  // staged spectrum column (even count)
+    static constexpr int SLOT = TD + GD;
+    static constexpr int GROUP_ELEMS = P::SMEM_ELEMS + 2 * SLOT;
+    static constexpr int SMEM_ELEMS = G * GROUP_ELEMS;
+};
+
+template <typename C, int L, typename SH>
+__global__ void __launch_bounds__(ColCfg<L, SH, sizeof(C)>::THREADS, 1)
+k_cols_convolve_grp(C *__restrict__ T, const C *__restrict__ gq, const C *__restrict__ tw, int N, const DevState *st,
+                    int gate, SysSel sy) {
+    typedef Plan<L, SH::E> P;
+    typedef GrpCfg<L, SH, sizeof(C)> G;
+    constexpr int E = P::E, TPR = P::TPR, LQ = G::LQ, NT = G::NT;
+    st = sys_move_bytes(st, sy.ws);
+    if (gated(st, gate)) return;
+    T += (long long)blockIdx.y * sy.T;
+    gq += (long long)blockIdx.y * sy.gq;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int g = threadIdx.x / TPR, t = threadIdx.x % TPR;
+    const int bar = 1 + g;
+    C *sm = reinterpret_cast<C *>(smraw) + g * G::GROUP_ELEMS;  // this worker's FFT exchange
+    C *buf = sm + P::SMEM_ELEMS;                                // and its two staging slots
+    const int W = gridDim.x * G::G;
+    auto issue = [&](int col, int slot) {
+        C *td = buf + slot * G::SLOT;
+        C *gd = td + G::TD;
+        for (int e = t; e < N; e += TPR) cp_async_elem(td + e, T + (size_t)e * L + col);
+        const int qc = col <= L / 2 ? col : L - col;
+        for (int e = t; e < LQ; e += TPR) cp_async_elem(gd + e, gq + (size_t)qc * LQ + e);
+        cp_async_commit();
+    };
+    int col = blockIdx.x * G::G + g;
+    if (col < L) issue(col, 0);
+    for (int it = 0; col < L; it++, col += W) {
+        const int slot = it & 1;
+        if (col + W < L) issue(col + W, slot ^ 1);
+        else cp_async_commit();  // empty group: the wait below always leaves one group pending
+        cp_async_wait<1>();
+        fft_barrier<NT>(bar);
+        const C *td = buf + slot * G::SLOT;
+        const C *gd = td + G::TD;
+        C reg[E];
+#pragma unroll
+        for (int p = 0; p < E; p++) {
+            const int k = t + p * TPR;
+            reg[p] = czero<C>();
+            if (p < E / 2 && k < N) reg[p] = td[k];
+        }
+        fft_run<L, SH::E, false, true, 1, NT>(reg, sm, tw, t, bar);
+#pragma unroll
+        for (int p = 0; p < E; p++) {
+            const int k1 = t + p * TPR;
+            const int qr = k1 <= L / 2 ? k1 : L - k1;
+            reg[p] = cmul(reg[p], gd[qr]);
+        }
+        fft_run<L, SH::E, true, false, 1, NT>(reg, sm, tw, t, bar);
+#pragma unroll
+        for (int p = 0; p < E / 2; p++) {
+            const int k = t + p * TPR;
+            if (k < N) T[(size_t)k * L + col] = reg[p];
+        }
+        fft_barrier<NT>(bar);  // this slot is refilled by the next iteration's issue
+    }
+    cp_async_wait<0>();
+}
+
 // ---------------------------------------------------------------- pass 3
 template <typename C, typename CO, int L, int MODE, typename SH>
 __global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
 k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xscale, const C *__restrict__ bvec,
                VecSel ys, double *__restrict__ npart, const C *__restrict__ tw, int N, const DevState *st, int gate,
-               const typename real_of<C>::type *__restrict__ cout) {
+               const typename real_of<C>::type *__restrict__ cout, SysSel sy) {
     typedef typename real_of<C>::type R;
     typedef typename real_of<CO>::type RO;
     typedef Plan<L, SH::E> P;
     constexpr int E = P::E, TPR = P::TPR;
     constexpr int NWARP = (RowCfg<L, SH>::THREADS + 31) / 32;
+    st = sys_move_bytes(st, sy.ws);
     if (gated(st, gate)) return;
+    T += (long long)blockIdx.y * sy.T;
+    xscale = sys_move_bytes(xscale, sy.ws);
+    npart = sys_move_bytes(npart, sy.ws);
+    if (bvec) bvec += (long long)blockIdx.y * sy.b;
+    if (cout) cout += (long long)blockIdx.y * sy.c;
     extern __shared__ __align__(16) unsigned char smraw[];
     __shared__ double wsum[NWARP];
     const int lr = threadIdx.x / TPR, t = threadIdx.x % TPR;
@@ -276,6 +381,22 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
     const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
     const bool live = row < N;
     C reg[E];
+    const long long kx = sel_index(st, xs.koff);
+    const long long ky = sel_index(st, ys.koff);
+    const C *x = reinterpret_cast<const C *>(xs.base) + kx * xs.stride + (long long)blockIdx.y * xs.sys;
+    CO *y = reinterpret_cast<CO *>(ys.base) + ky * ys.stride + (long long)blockIdx.y * ys.sys;
+    const R s = xscale ? (R)xscale[kx] : (R)1;
+    const size_t rb = (size_t)row * (size_t)N;
+    // the epilogue's operands x (and b) are loaded before the transform so that
+    // their latency overlaps its arithmetic
+    C xv[E / 2], bv[E / 2];
+#pragma unroll
+    for (int p = 0; p < E / 2; p++) {
+        const int idx = t + p * TPR;
+        const bool ok = live && idx < N;
+        xv[p] = ok ? x[rb + idx] : czero<C>();
+        bv[p] = (MODE != 0 && ok) ? bvec[rb + idx] : czero<C>();
+    }
     if (live) {
         const C *in = T + (size_t)row * L;
 #pragma unroll
@@ -285,25 +406,18 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
         for (int p = 0; p < E; p++) reg[p] = czero<C>();
     }
     fft_run<L, SH::E, true, false>(reg, sm, tw, t);
-    const long long kx = sel_index(st, xs.koff);
-    const long long ky = sel_index(st, ys.koff);
-    const C *x = reinterpret_cast<const C *>(xs.base) + kx * xs.stride;
-    CO *y = reinterpret_cast<CO *>(ys.base) + ky * ys.stride;
-    const R s = xscale ? (R)xscale[kx] : (R)1;
     double acc = 0.0;
     if (live) {
-        const size_t rb = (size_t)row * (size_t)N;
 #pragma unroll
         for (int p = 0; p < E / 2; p++) {
             const int idx = t + p * TPR;
             if (idx < N) {
-                const C xv = x[rb + idx];
                 if (cout) reg[p] = cscale(reg[p], cout[rb + idx]);  // transpose: contrast after G
                 C o;
                 if (MODE == 0) {
-                    o = csub(cscale(xv, s), reg[p]);
+                    o = csub(cscale(xv[p], s), reg[p]);
                 } else {
-                    o = cadd(csub(bvec[rb + idx], xv), reg[p]);
+                    o = cadd(csub(bv[p], xv[p]), reg[p]);
                 }
                 CO oo;
                 oo.x = (RO)o.x;
@@ -390,36 +504,51 @@ template <typename SH0, int L> struct Passes {
             auto kern = k_rows_forward<double2, L, SH>;
             int e = set_smem(kern, smem);
             if (e) return e;
-            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, a.transpose ? nullptr : (const double *)a.cdiag,
-                                                (double2 *)a.T, (const double2 *)a.tw, a.N, st, gate);
+            kern<<<dim3(grid, a.nsys), Q::THREADS, smem, s>>>(x, xs, a.transpose ? nullptr : (const double *)a.cdiag,
+                                                              (double2 *)a.T, (const double2 *)a.tw, a.N, st, gate,
+                                                              sys_sel(a));
         } else {
             const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(float2);
             auto kern = k_rows_forward<float2, L, SH>;
             int e = set_smem(kern, smem);
             if (e) return e;
-            kern<<<grid, Q::THREADS, smem, s>>>(x, xs, a.transpose ? nullptr : (const float *)a.cdiag,
-                                                (float2 *)a.T, (const float2 *)a.tw, a.N, st, gate);
+            kern<<<dim3(grid, a.nsys), Q::THREADS, smem, s>>>(x, xs, a.transpose ? nullptr : (const float *)a.cdiag,
+                                                              (float2 *)a.T, (const float2 *)a.tw, a.N, st, gate,
+                                                              sys_sel(a));
         }
         return (int)cudaGetLastError();
     }
 
     template <typename C> static int cols_t(const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s) {
         typedef ColCfg<L, CS, sizeof(C)> Q;
-        if constexpr (CS::PIPE) {
+        if constexpr (CS::PIPE == 2 && GrpCfg<L, CS, sizeof(C)>::OK) {
+            typedef GrpCfg<L, CS, sizeof(C)> G;
+            const size_t smem = (size_t)G::SMEM_ELEMS * sizeof(C);
+            auto kern = k_cols_convolve_grp<C, L, CS>;
+            int e = set_smem(kern, smem);
+            if (e) return e;
+            const int nblk = (L + G::G - 1) / G::G;
+            const int grid = nblk < a.sms ? nblk : a.sms;
+            kern<<<dim3(grid, a.nsys), G::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate,
+                                                              sys_sel(a));
+            return (int)cudaGetLastError();
+        } else if constexpr (CS::PIPE) {
             const size_t smem = (size_t)PipeCfg<L, CS, sizeof(C)>::SMEM_ELEMS * sizeof(C);
             auto kern = k_cols_convolve_pipe<C, L, CS>;
             int e = set_smem(kern, smem);
             if (e) return e;
             const int ntiles = L / Q::CPB;
             const int grid = ntiles < a.sms ? ntiles : a.sms;
-            kern<<<grid, Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate);
+            kern<<<dim3(grid, a.nsys), Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate,
+                                                              sys_sel(a));
             return (int)cudaGetLastError();
         } else {
             const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
             auto kern = k_cols_convolve<C, L, CS>;
             int e = set_smem(kern, smem);
             if (e) return e;
-            kern<<<L / Q::CPB, Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st, gate);
+            kern<<<dim3(L / Q::CPB, a.nsys), Q::THREADS, smem, s>>>((C *)a.T, (const C *)a.gq, (const C *)a.tw, a.N, st,
+                                                                    gate, sys_sel(a));
             return (int)cudaGetLastError();
         }
     }
@@ -437,8 +566,9 @@ template <typename SH0, int L> struct Passes {
         if (e) return e;
         const int grid = (a.N + Q::RPC - 1) / Q::RPC;
         typedef typename real_of<C>::type R;
-        kern<<<grid, Q::THREADS, smem, s>>>((const C *)a.T, x, xs, (const C *)b, y, npart, (const C *)a.tw, a.N,
-                                              st, gate, a.transpose ? (const R *)a.cdiag : nullptr);
+        kern<<<dim3(grid, a.nsys), Q::THREADS, smem, s>>>((const C *)a.T, x, xs, (const C *)b, y, npart,
+                                                            (const C *)a.tw, a.N, st, gate,
+                                                            a.transpose ? (const R *)a.cdiag : nullptr, sys_sel(a));
         return (int)cudaGetLastError();
     }
     static int inv(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xs, const void *b,
@@ -482,6 +612,7 @@ template <template <typename> class F, typename... A> static int dispatch(int va
         case 5: CG_V_CASES(MvV5)
         case 6: CG_V_CASES(MvV6)
         case 7: CG_V_CASES(MvV7)
+        case 8: CG_V_CASES(MvV8)
         default: return -1;
     }
 #undef CG_V_CASES
@@ -514,7 +645,7 @@ int fft_supported(int L) {
 
 int matvec_variants(int L) { return L >= 128 ? MV_VARIANTS : 1; }
 
-int matvec_variant_persistent(int v) { return v == 5 || v == 6; }
+int matvec_variant_persistent(int v) { return v == 5 || v == 6 || v == 8; }
 
 int rows_per_block(int variant, int L) { return dispatch<RpcF>(variant, L); }
 

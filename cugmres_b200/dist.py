@@ -61,20 +61,21 @@ def sweep_stats(records, wall_s):
             "iterations_total": int(sum(r["iterations"] for r in records))}
 
 
-def run_sweep(systems, rank, world, solve_fn, timer=None):
+def run_sweep(systems, rank, world, solve_fn, timer=None, device=None):
     """Solve this rank's share with solve_fn(list_of_systems) -> list of info
     dicts, gather every record, return (records, stats).  `timer` returns
-    seconds for the local share (device time); the job time is the max over
-    ranks."""
+    seconds for the local share (default: the duration of the synchronous
+    solve_fn call); the job time is the max over ranks (all-reduce on
+    `device`: the rank's GPU under NCCL, None for gloo)."""
     import time
-    sizes = [s["g_block"].shape[0] for s in systems]
+    sizes = [int(s["N"]) if "N" in s else s["g_block"].shape[0] for s in systems]
     mine = shard_systems(sizes, rank, world)
     t0 = time.perf_counter()
     infos = solve_fn([systems[i] for i in mine]) if mine else []
     local = timer() if timer else time.perf_counter() - t0
     recs = [dict(index=i, N=sizes[i], **{k: v for k, v in info.items() if k in
-                                           ("status", "iterations", "seconds", "rel_residual_true")})
+                                           ("status", "iterations", "cycles", "seconds", "rel_residual_true")})
             for i, info in zip(mine, infos)]
     records = gather_records(recs)
-    job = max_over_ranks(local)
+    job = max_over_ranks(local, device=device)
     return records, sweep_stats(records, job)

@@ -198,6 +198,22 @@ typedef struct {
 int cugmres_solve_batch(int device, int nsys, const cg_system *systems, const cg_opts *opts, int nworkers,
                         cg_result *results);
 
+/* Solves nsys independent systems in lockstep buckets -- the batched
+ * counterpart of the reference's serial sweep over sizes and repetitions
+ * (CUDA_GMRES/launch_GMRES.cuh:88-235), which solves one system per call.
+ * Systems are grouped by grid side N (largest first), ordered by difficulty
+ * (optical size N k0 h sqrt(1 + max chi)), and cut into buckets of at most
+ * max_bucket systems (0: as many as fit in half of the free device memory).
+ * Every kernel of an Arnoldi step is one launch for the whole bucket; each
+ * restart cycle of a bucket is one CUDA-graph replay; systems that stop early
+ * skip the rest of their bucket's launches.  results[i].seconds is the time
+ * from the start of system i's bucket (its operator set-up included) to the
+ * cycle boundary at which it finished.  Supports FP64, CG_ORTHO_DCGS2, no
+ * preconditioner, A x = b; other options return CG_ERR_NOT_IMPLEMENTED.
+ * Per-system convergence is in results[i].status. */
+int cugmres_solve_buckets(int device, int nsys, const cg_system *systems, const cg_opts *opts, int max_bucket,
+                          cg_result *results);
+
 /* Per-phase device timing of cugmres_solve, the counterpart of the reference's
  * clock_gettime step stamps (CUDA_GMRES/GMRES.cuh:39-445, labels in
  * launch_GMRES.cuh:245-307): CUDA events recorded between kernel groups on the

@@ -18,7 +18,7 @@ sys.path.insert(0, sys.argv[1])
 import cugmres_b200 as cg
 from cugmres_b200 import problems as P
 from oracle import oracle as O
-for N in (64, 128, 300, 512, 1024, 1100, 2048):
+for N in (64, 128, 300, 512, 1024, 1100):
     pr = P.helmholtz(N, 4.0, seed=N)
     s = cg.Solver(0).set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
     x = np.random.default_rng(N).standard_normal((N, N)) + 1j
@@ -35,7 +35,7 @@ for N in (64, 128, 300, 512, 1024, 1100, 2048):
 """
 
 
-@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "4", "5", "6", "7", "tuned"])
+@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "4", "5", "6", "7", "8", "tuned"])
 def test_matvec_shape_parity(cuda_device, shape, tmp_path):
     env = dict(os.environ)
     env["CUGMRES_TUNE_CACHE"] = str(tmp_path / "tune.txt")
