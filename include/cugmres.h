@@ -154,7 +154,7 @@ int cugmres_set_operator_circulant(cg_ctx *ctx, int N, const cg_c64 *g_prep, con
 int cugmres_grid_size(const cg_ctx *ctx, int *N, int *L);
 /* Launch shapes the autotuner chose for the three matvec passes (row forward,
  * column convolution, row inverse) of `precision`; shapes[3] receives indices
- * 0..7 (0 for embeddings L < 128).  Tuning runs in cugmres_set_operator and is
+ * 0..8 (0 for embeddings L < 128).  Tuning runs in cugmres_set_operator and is
  * cached per device in $CUGMRES_TUNE_CACHE (default
  * ~/.cache/cugmres_b200/autotune.txt); CUGMRES_AUTOTUNE=0 keeps shape 0. */
 int cugmres_matvec_shapes(const cg_ctx *ctx, int precision, int *shapes);
