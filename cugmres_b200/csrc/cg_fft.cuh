@@ -233,10 +233,90 @@ template <int NT> __device__ __forceinline__ void fft_barrier(int id) {
     }
 }
 
+// Twiddles w^{k r}, r = 1..R-1, of one butterfly (w = w_{Ns R}), from its two
+// base values w^k and (R >= 8) w^{4k}: the other powers are products of at
+// most three factors, so each carries a few units of rounding more than a
+// table entry (well inside the transform's own error), while the table reads
+// -- the largest share of a pass's L1/L2 load traffic when every power was
+// read -- drop from R-1 to 2.  CONJ: the conjugate powers (the inverse
+// transform from the forward table's bases).  w[0] is unused.
+template <int R, bool CONJ, typename C> __device__ __forceinline__ void stage_twiddles(C w1, C w4, C (&w)[R]) {
+    if constexpr (CONJ) {
+        w1 = cconj(w1);
+        w4 = cconj(w4);
+    }
+    w[0] = mk<C>(1, 0);
+    w[1] = w1;
+    if constexpr (R == 4) {
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[2], w[1]);
+    } else if constexpr (R >= 8) {
+        w[4] = w4;
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[2], w[1]);
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+        if constexpr (R == 16) {
+            w[8] = cmul(w[4], w[4]);
+            w[12] = cmul(w[8], w[4]);
+#pragma unroll
+            for (int r = 1; r < 4; r++) {
+                w[8 + r] = cmul(w[8], w[r]);
+                w[12 + r] = cmul(w[12], w[r]);
+            }
+        }
+    }
+}
+
+// Base twiddles of every butterfly a thread runs in stages 1.. of a length-L
+// transform (stage 0 has none): per butterfly w^k and, for radix >= 8, w^{4k}
+// (table entries r = 1 and r = 4 of the stage's [r][k] layout).  They depend
+// only on the thread, so kernels that run many transforms (the persistent
+// column passes) load them once and keep them in registers.
+template <int L, int E0> struct TwBase {
+    typedef Plan<L, E0> P;
+    __host__ __device__ static constexpr int per(int s) {
+        return s == 0 ? 0 : (P::E / P::radix(s)) * (P::radix(s) >= 8 ? 2 : 1);
+    }
+    __host__ __device__ static constexpr int off(int s) { return s <= 1 ? 0 : off(s - 1) + per(s - 1); }
+    __host__ __device__ static constexpr int total() { return P::NST <= 1 ? 0 : off(P::NST - 1) + per(P::NST - 1); }
+    static constexpr int COUNT = total() > 0 ? total() : 1;
+};
+
+template <int L, int E0, int S> struct TwBaseLoad {
+    typedef Plan<L, E0> P;
+    template <typename C>
+    static __device__ __forceinline__ void run(const C *__restrict__ tw, int t, C (&wb)[TwBase<L, E0>::COUNT]) {
+        if constexpr (S < P::NST) {
+            constexpr int R = P::radix(S), Ns = P::span(S), NB = P::E / R, O = TwBase<L, E0>::off(S);
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const int k = (t + b * P::TPR) % Ns;
+                const C *__restrict__ ts = tw + P::twoff(S) + k;
+                if constexpr (R >= 8) {
+                    wb[O + 2 * b] = __ldg(ts);
+                    wb[O + 2 * b + 1] = __ldg(ts + 3 * Ns);
+                } else {
+                    wb[O + b] = __ldg(ts);
+                }
+            }
+            TwBaseLoad<L, E0, S + 1>::run(tw, t, wb);
+        }
+    }
+};
+
+// Loads this thread's base twiddles from the table set `tw` (the forward
+// table of the E0 plan).
+template <int L, int E0, typename C>
+__device__ __forceinline__ void load_tw_base(const C *__restrict__ tw, int t, C (&wb)[TwBase<L, E0>::COUNT]) {
+    TwBaseLoad<L, E0, 1>::run(tw_table<L, E0, false>(tw), t, wb);
+}
+
 // One Stockham stage S of a length-L transform (compile-time radix and span).
 // tmp holds the previous stage's butterfly outputs (tmp[b*Rp + q]) on entry
 // and this stage's outputs on exit; the last stage stores canonical reg.
-template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS, int NT = 0> struct Stage {
+template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS, int NT = 0, bool CONJ = false> struct Stage {
     typedef Plan<L, E0> P;
     static constexpr int E = P::E;
     static constexpr int TPR = P::TPR;
@@ -244,8 +324,8 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS, int NT = 0> str
     static constexpr int Ns = P::span(S);
     static constexpr int NB = E / R;  // butterflies per thread in this stage
     template <typename C>
-    static __device__ __forceinline__ void run(C (&reg)[E], C (&tmp)[E], C *sm, const C *__restrict__ tw, int t,
-                                               int bar) {
+    static __device__ __forceinline__ void run(C (&reg)[E], C (&tmp)[E], C *sm, const C (&wb)[TwBase<L, E0>::COUNT],
+                                               int t, int bar) {
         if constexpr (S > 0) {
             // write the previous stage's outputs, then read this stage's inputs
             constexpr int Rp = P::radix(S - 1);
@@ -263,12 +343,14 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS, int NT = 0> str
 #pragma unroll
             for (int b = 0; b < NB; b++) {
                 const int j = t + b * TPR;
-                const int k = j % Ns;
-                const C *__restrict__ ts = tw + P::twoff(S) + k;
+                constexpr int O = TwBase<L, E0>::off(S);
+                C w[R];
+                if constexpr (R >= 8) stage_twiddles<R, CONJ>(wb[O + 2 * b], wb[O + 2 * b + 1], w);
+                else stage_twiddles<R, CONJ>(wb[O + b], wb[O + b], w);
 #pragma unroll
                 for (int r = 0; r < R; r++) {
                     C v = sm[P::pad(j + r * (L / R)) * SMS];
-                    if (r > 0) v = cmul(v, __ldg(ts + (r - 1) * Ns));
+                    if (r > 0) v = cmul(v, w[r]);
                     tmp[b * R + r] = v;
                 }
             }
@@ -289,7 +371,7 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS, int NT = 0> str
 #pragma unroll
                 for (int q = 0; q < R; q++) reg[b + q * NB] = tmp[b * R + q];
         } else {
-            Stage<L, E0, INV, HALF_IN, S + 1, SMS, NT>::run(reg, tmp, sm, tw, t, bar);
+            Stage<L, E0, INV, HALF_IN, S + 1, SMS, NT, CONJ>::run(reg, tmp, sm, wb, t, bar);
         }
     }
 };
@@ -303,11 +385,25 @@ template <int L, int E0, bool INV, bool HALF_IN, int S, int SMS, int NT = 0> str
 // Every thread of the block (NT = 0), or of named barrier `bar` (NT threads),
 // must call this the same number of times (it contains barriers).  tw is the
 // base of the 4 L-entry table set (tw_table picks the plan's and direction's table).
+// The stage twiddles' base values are loaded at the start (all stages at
+// once, so their latency overlaps the first stage), from the direction's own
+// table.
 template <int L, int E0, bool INV, bool HALF_IN, int SMS = 1, int NT = 0, typename C>
 __device__ __forceinline__ void fft_run(C (&reg)[Plan<L, E0>::E], C *sm, const C *__restrict__ tw, int t,
                                         int bar = 0) {
     C tmp[Plan<L, E0>::E];
-    Stage<L, E0, INV, HALF_IN, 0, SMS, NT>::run(reg, tmp, sm, tw_table<L, E0, INV>(tw), t, bar);
+    C wb[TwBase<L, E0>::COUNT];
+    TwBaseLoad<L, E0, 1>::run(tw_table<L, E0, INV>(tw), t, wb);
+    Stage<L, E0, INV, HALF_IN, 0, SMS, NT>::run(reg, tmp, sm, wb, t, bar);
+}
+
+// Same with base twiddles the caller loaded once (load_tw_base, forward
+// table); the inverse uses their conjugates.
+template <int L, int E0, bool INV, bool HALF_IN, int SMS = 1, int NT = 0, typename C>
+__device__ __forceinline__ void fft_run_wb(C (&reg)[Plan<L, E0>::E], C *sm, const C (&wb)[TwBase<L, E0>::COUNT],
+                                           int t, int bar = 0) {
+    C tmp[Plan<L, E0>::E];
+    Stage<L, E0, INV, HALF_IN, 0, SMS, NT, INV>::run(reg, tmp, sm, wb, t, bar);
 }
 
 }  // namespace cg

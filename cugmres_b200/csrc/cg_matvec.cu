@@ -236,6 +236,9 @@ k_cols_convolve_pipe(C *__restrict__ T, const C *__restrict__ gq, const C *__res
         }
         cp_async_commit();
     };
+    // this thread's base twiddles, loaded once for every tile it transforms
+    C wb[TwBase<L, SH::E>::COUNT];
+    load_tw_base<L, SH::E>(tw, t, wb);
     int v = blockIdx.x;
     if (v < ntiles) issue(v, 0);
     for (int it = 0; v < ntiles; it++, v += gridDim.x) {
@@ -254,14 +257,14 @@ k_cols_convolve_pipe(C *__restrict__ T, const C *__restrict__ gq, const C *__res
             reg[p] = czero<C>();
             if (p < E / 2 && k < N) reg[p] = td[k * CPB + cl];
         }
-        fft_run<L, SH::E, false, true, CPB>(reg, sm, tw, t);
+        fft_run_wb<L, SH::E, false, true, CPB>(reg, sm, wb, t);
 #pragma unroll
         for (int p = 0; p < E; p++) {
             const int k1 = t + p * TPR;
             const int qr = k1 <= L / 2 ? k1 : L - k1;
             reg[p] = cmul(reg[p], gd[cl * LQ + qr]);
         }
-        fft_run<L, SH::E, true, false, CPB>(reg, sm, tw, t);
+        fft_run_wb<L, SH::E, true, false, CPB>(reg, sm, wb, t);
 #pragma unroll
         for (int p = 0; p < E / 2; p++) {
             const int k = t + p * TPR;
@@ -321,6 +324,8 @@ k_cols_convolve_grp(C *__restrict__ T, const C *__restrict__ gq, const C *__rest
         for (int e = t; e < LQ; e += TPR) cp_async_elem(gd + e, gq + (size_t)qc * LQ + e);
         cp_async_commit();
     };
+    C wb[TwBase<L, SH::E>::COUNT];  // base twiddles, loaded once for every column
+    load_tw_base<L, SH::E>(tw, t, wb);
     int col = blockIdx.x * G::G + g;
     if (col < L) issue(col, 0);
     for (int it = 0; col < L; it++, col += W) {
@@ -338,14 +343,14 @@ k_cols_convolve_grp(C *__restrict__ T, const C *__restrict__ gq, const C *__rest
             reg[p] = czero<C>();
             if (p < E / 2 && k < N) reg[p] = td[k];
         }
-        fft_run<L, SH::E, false, true, 1, NT>(reg, sm, tw, t, bar);
+        fft_run_wb<L, SH::E, false, true, 1, NT>(reg, sm, wb, t, bar);
 #pragma unroll
         for (int p = 0; p < E; p++) {
             const int k1 = t + p * TPR;
             const int qr = k1 <= L / 2 ? k1 : L - k1;
             reg[p] = cmul(reg[p], gd[qr]);
         }
-        fft_run<L, SH::E, true, false, 1, NT>(reg, sm, tw, t, bar);
+        fft_run_wb<L, SH::E, true, false, 1, NT>(reg, sm, wb, t, bar);
 #pragma unroll
         for (int p = 0; p < E / 2; p++) {
             const int k = t + p * TPR;
