@@ -65,7 +65,7 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
-    ap.add_argument("--inner-tol", type=float, default=1e-5)
+    ap.add_argument("--inner-tol", type=float, default=1e-5, help="mixed: a complex64 cycle ends when its estimate fell by this")
     ap.add_argument("--profile-case", action="store_true", help="fixed launch sequence for profiler captures")
     ap.add_argument("--case-steps", type=int, default=60)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -237,17 +237,19 @@ def rel_err(x, ref):
     return float(np.linalg.norm(x - ref) / np.linalg.norm(ref))
 
 
-def tight_reference(s, b):
-    """FP64 GMRES(2500) solve tightened to 1e-13 (at most 5000 steps), the
-    reference the time-to-tol results are compared with; None if it does not
-    get there."""
-    x, info = s.solve(b, restart=2500, max_iter=5000, tol=1e-13, precision="fp64")
+def tight_reference(s, b, restart=2500, max_iter=5000):
+    """FP64 GMRES solve tightened to 1e-13, the reference the time-to-tol
+    results are compared with; None if it does not get there."""
+    x, info = s.solve(b, restart=restart, max_iter=max_iter, tol=1e-13, precision="fp64")
     return x if info["status"] == 0 else None
 
 
 def side_measurements(args, stream):
-    """Mixed precision on the same capped solve, and time-to-tol on the 256^2
-    system of the same construction, where unrestarted GMRES converges."""
+    """Mixed precision on the same capped solve; time-to-1e-10 where GMRES
+    converges: the 256^2 and 512^2 systems of the same construction
+    (unrestarted; mixed = complex64 cycles that end when their estimate fell by
+    1e-7, FP64 refinement); the config-3 grid (2048^2, eps_r = 12.25, restart
+    50) within a budget of 1000 steps, FP64 and mixed."""
     import torch
     import cugmres_b200 as cg
     from cugmres_b200 import problems as P
@@ -263,20 +265,36 @@ def side_measurements(args, stream):
     out["mixed_capped_solve"] = {"s": ms / 1e3, "steps": info["iterations"], "rel_residual_true": info["rel_residual_true"],
                                  "ms_per_step": ms / max(1, info["iterations"])}
     s.close()
-    pr2 = P.helmholtz(256, args.eps, seed=args.seed)
+    for N, R, reps in ((256, 2500, 1), (512, 4400, 0)):
+        prn = P.helmholtz(N, args.eps, seed=args.seed)
+        s = cg.Solver(torch.cuda.current_device())
+        s.set_stream(stream.cuda_stream)
+        s.set_operator(prn["g_block"], prn["chi"], prn["chi_scale"])
+        bn = torch.from_numpy(prn["b"]).cuda()
+        xref = tight_reference(s, bn, restart=R, max_iter=2 * R)
+        for prec in ("fp64", "mixed"):
+            kwn = dict(restart=R, max_iter=3 * R, tol=args.tol, precision=prec, inner_tol=1e-7)
+            for _ in range(reps):  # warm-up solve (the 512^2 ones are timed cold: graphs are built in their first cycle)
+                s.solve(bn, **kwn)
+            ms, info, x = timed_solves(s, bn, kwn, 1, stream)
+            out[f"time_to_tol_{N}_unrestarted_{prec}"] = {
+                "s": ms / 1e3, "steps": info["iterations"], "cycles": info["cycles"], "status": info["status_text"],
+                "rel_residual_true": info["rel_residual_true"], "err_vs_fp64_tol1e-13": rel_err(x, xref)}
+        s.close()
+    pr3 = P.helmholtz(2048, 12.25, seed=args.seed)
     s = cg.Solver(torch.cuda.current_device())
     s.set_stream(stream.cuda_stream)
-    s.set_operator(pr2["g_block"], pr2["chi"], pr2["chi_scale"])
-    b2 = torch.from_numpy(pr2["b"]).cuda()
-    xref = tight_reference(s, b2)
+    s.set_operator(pr3["g_block"], pr3["chi"], pr3["chi_scale"])
+    b3 = torch.from_numpy(pr3["b"]).cuda()
+    row = {}
     for prec in ("fp64", "mixed"):
-        kw2 = dict(restart=2500, max_iter=2500, tol=args.tol, precision=prec, inner_tol=1e-6)
-        s.solve(b2, **kw2)
-        ms, info, x = timed_solves(s, b2, kw2, 1, stream)
-        out[f"time_to_tol_256_unrestarted_{prec}"] = {
-            "s": ms / 1e3, "steps": info["iterations"], "status": info["status_text"],
-            "rel_residual_true": info["rel_residual_true"],
-            "err_vs_fp64_tol1e-13": rel_err(x, xref)}
+        kw3 = dict(restart=50, max_iter=1000, tol=args.tol, precision=prec, inner_tol=1e-5)
+        ms, info, _ = timed_solves(s, b3, kw3, 1, stream)
+        row[prec] = {"s": ms / 1e3, "steps": info["iterations"], "status": info["status_text"],
+                     "rel_residual_true": info["rel_residual_true"]}
+    row["note"] = ("2048x2048, eps_r = 12.25, GMRES-IR with complex64 cycles of 50 steps; 1e-10 is not reached "
+                   "within the 1000-step budget, so no error against a 1e-13 solve exists")
+    out["config3_2048_restart50_budget1000"] = row
     s.close()
     return out
 

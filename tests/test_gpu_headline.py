@@ -77,3 +77,19 @@ def test_restart_cycle_1024_fp64_vs_oracle(solver, oracle, system1024, ortho):
     assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-10
     assert np.allclose(info["res_hist"][1:], o["res_hist"][1:], rtol=1e-9)
     assert abs(info["rel_residual_true"] - o["true_res"]) < 1e-9 * o["true_res"]
+
+
+def test_restart_cycle_2048_fp64_vs_oracle(solver, oracle):
+    """The config-3 grid (2048^2, 4096^2 embedding, eps_r = 12.25): a GMRES(50)
+    run of 55 FP64 Arnoldi steps (one cycle, the residual and update, five
+    steps of the next) against the oracle's modified Gram-Schmidt GMRES."""
+    N = 2048
+    pr = OP.helmholtz(N, 12.25, seed=0)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    assert solver.L == 4096
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    x, info = solver.solve(pr["b"], restart=50, max_iter=55, tol=0.0)
+    o = oracle.gmres(gh, pr["chi"] * pr["chi_scale"], pr["b"], restart=50, maxiter=55, tol=0.0)
+    assert info["iterations"] == o["iterations"] == 55 and info["cycles"] == o["cycles"] == 2
+    assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-10
+    assert np.allclose(info["res_hist"][1:], o["res_hist"][1:], rtol=1e-9)
