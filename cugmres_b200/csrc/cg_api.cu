@@ -94,10 +94,14 @@ int ctx_op_view(const cg_ctx *c, OpView *v) {
     v->N = c->N;
     v->L = c->L;
     v->sms = c->sms;
-    for (int p = 0; p < 3; p++) v->var[p] = c->var[0][p];
+    for (int q = 0; q < 2; q++)
+        for (int p = 0; p < 3; p++) v->var[q][p] = c->var[q][p];
     v->gq64 = c->gq64;
+    v->gq32 = c->gq32;
     v->c64 = c->c64;
+    v->c32 = c->c32;
     v->tw64 = c->tw64;
+    v->tw32 = c->tw32;
     v->stream = c->stream;
     return CG_OK;
 }

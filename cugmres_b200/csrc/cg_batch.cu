@@ -100,7 +100,8 @@ extern "C" int cugmres_solve_batch(int device, int nsys, const cg_system *sys, c
 // CGS2 steps, back-solve, update, the next true residual and cycle decisions
 // of all systems) is captured once per bucket as a CUDA graph and replayed
 // with one launch per cycle, one host synchronisation per cycle.
-// Scope: FP64, delayed CGS2, no preconditioner, A x = b (not the transposed
+// Scope: FP64 or mixed precision (complex64 cycles, FP64 residual and
+// update), delayed CGS2, no preconditioner, A x = b (not the transposed
 // system), restarted semantics; other options return CG_ERR_NOT_IMPLEMENTED.
 namespace {
 
@@ -164,14 +165,15 @@ WsLayout ws_layout(int mc, int maxit, size_t npart, size_t part, size_t gpart, s
 }
 
 struct BucketBufs {
-    void *V = nullptr, *T = nullptr, *G = nullptr, *C = nullptr, *X = nullptr, *B = nullptr, *WS = nullptr;
+    void *V = nullptr, *T = nullptr, *G = nullptr, *C = nullptr, *G32 = nullptr, *C32 = nullptr, *X = nullptr,
+         *B = nullptr, *WS = nullptr;
     DevState *st_host = nullptr;
     cudaStream_t cap = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaEvent_t ev = nullptr;
     ~BucketBufs() {
         if (gexec) cudaGraphExecDestroy(gexec);
-        for (void *p : {V, T, G, C, X, B, WS})
+        for (void *p : {V, T, G, C, G32, C32, X, B, WS})
             if (p) cudaFree(p);
         if (st_host) cudaFreeHost(st_host);
         if (cap) cudaStreamDestroy(cap);
@@ -212,6 +214,8 @@ int solve_bucket(cg_ctx *ctx, const cg_system *sys, const std::vector<int> &idx,
     const int nb = (int)idx.size();
     const int N = sys[idx[0]].N;
     const long long n = (long long)N * N;
+    const int prec = o.precision == CG_PREC_MIXED ? 1 : 0;  // Arnoldi cycles in complex64
+    const size_t esz = prec ? sizeof(float2) : sizeof(double2);
     const double t0 = now_s();
     BucketBufs bb;
     // operator of every system: the context builds it (GPU Green's block or the
@@ -232,6 +236,16 @@ int solve_bucket(cg_ctx *ctx, const cg_system *sys, const std::vector<int> &idx,
             BK_CU(cudaMalloc(&bb.C, sizeof(double) * (size_t)n * nb));
             BK_CU(cudaMalloc(&bb.X, sizeof(double2) * (size_t)n * nb));
             BK_CU(cudaMalloc(&bb.B, sizeof(double2) * (size_t)n * nb));
+            if (prec) {
+                BK_CU(cudaMalloc(&bb.G32, sizeof(float2) * gq_elems * nb));
+                BK_CU(cudaMalloc(&bb.C32, sizeof(float) * (size_t)n * nb));
+            }
+        }
+        if (prec) {
+            BK_CU(cudaMemcpyAsync((float2 *)bb.G32 + gq_elems * q, ov.gq32, sizeof(float2) * gq_elems,
+                                  cudaMemcpyDeviceToDevice, ov.stream));
+            BK_CU(cudaMemcpyAsync((float *)bb.C32 + (size_t)n * q, ov.c32, sizeof(float) * n, cudaMemcpyDeviceToDevice,
+                                  ov.stream));
         }
         BK_CU(cudaMemcpyAsync((double2 *)bb.G + gq_elems * q, ov.gq64, sizeof(double2) * gq_elems,
                               cudaMemcpyDeviceToDevice, ov.stream));
@@ -254,17 +268,17 @@ int solve_bucket(cg_ctx *ctx, const cg_system *sys, const std::vector<int> &idx,
     const int L = ov.L;
     const int m = o.restart;
     const int sms_eff = std::max(1, ov.sms / nb);  // each system's share of the GPU
-    const int ndot2 = dots2_blocks(0, sms_eff, m, n);
-    const int nax2 = axpy2_blocks(0, sms_eff, m, n);
+    const int ndot2 = dots2_blocks(prec, sms_eff, m, n);
+    const int nax2 = axpy2_blocks(prec, sms_eff, m, n);
     const int nax = std::max(1, (int)std::min<long long>((n + 255) / 256, 4LL * sms_eff));
-    const int rpc = rows_per_block(ov.var[2], L);
+    const int rpc = rows_per_block(ov.var[0][2], L);
     const int nrb = (N + rpc - 1) / rpc;
     const size_t pld = (size_t)dots2_part_ld(m);
     const size_t ngroups = ((size_t)ndot2 + 15) / 16;
     const WsLayout wl = ws_layout(m, std::max(1, o.max_iter), std::max<size_t>(nrb, (size_t)nax) + 32,
                                   4 * (size_t)ndot2 * pld, 4 * ngroups * pld, ngroups);
     const size_t vsys = (size_t)(m + 2) * (size_t)n;
-    BK_CU(cudaMalloc(&bb.V, sizeof(double2) * vsys * nb));
+    BK_CU(cudaMalloc(&bb.V, esz * vsys * nb));
     BK_CU(cudaMalloc(&bb.T, sizeof(double2) * (size_t)N * L * nb));
     BK_CU(cudaMalloc(&bb.WS, wl.bytes * nb));
     BK_CU(cudaMemsetAsync(bb.WS, 0, wl.bytes * nb, s));
@@ -303,6 +317,7 @@ int solve_bucket(cg_ctx *ctx, const cg_system *sys, const std::vector<int> &idx,
         h.maxit = o.max_iter;
         h.rotation = o.givens == CG_GIVENS_REFERENCE ? 1 : 0;
         h.tol = o.tol;
+        h.inner_tol = prec ? o.inner_tol : 0.0;
         h.ortho = 0;  // delayed CGS2
         BK_CU(cudaMemcpyAsync(ws + (size_t)q * wl.bytes + wl.st, &h, sizeof(h), cudaMemcpyHostToDevice, s));
         BK_CU(cudaStreamSynchronize(s));  // h lives on this stack frame
@@ -310,23 +325,33 @@ int solve_bucket(cg_ctx *ctx, const cg_system *sys, const std::vector<int> &idx,
     k_bucket_nb<<<dim3(1, nb), 1024, 0, s>>>((const double2 *)bb.B, n, ws + wl.st, (long long)wl.bytes);
     BK_CU(cudaGetLastError());
 
-    MatvecArgs a;
-    a.N = N;
-    a.L = L;
-    a.vfwd = ov.var[0];
-    a.vcols = ov.var[1];
-    a.vinv = ov.var[2];
-    a.gq = bb.G;
-    a.cdiag = bb.C;
-    a.tw = ov.tw64;
-    a.T = bb.T;
-    a.sms = ov.sms;
-    a.nsys = nb;
-    a.sys_ws = (long long)wl.bytes;
-    a.sys_c = n;
-    a.sys_T = (long long)N * L;
-    a.sys_gq = (long long)gq_elems;
-    a.sys_b = n;
+    // FP64 operator (true residual) and the cycles' operator (FP64, or FP32 in mixed precision)
+    MatvecArgs a64;
+    a64.N = N;
+    a64.L = L;
+    a64.vfwd = ov.var[0][0];
+    a64.vcols = ov.var[0][1];
+    a64.vinv = ov.var[0][2];
+    a64.gq = bb.G;
+    a64.cdiag = bb.C;
+    a64.tw = ov.tw64;
+    a64.T = bb.T;
+    a64.sms = ov.sms;
+    a64.nsys = nb;
+    a64.sys_ws = (long long)wl.bytes;
+    a64.sys_c = n;
+    a64.sys_T = (long long)N * L;
+    a64.sys_gq = (long long)gq_elems;
+    a64.sys_b = n;
+    MatvecArgs ap = a64;
+    if (prec) {
+        ap.vfwd = ov.var[1][0];
+        ap.vcols = ov.var[1][1];
+        ap.vinv = ov.var[1][2];
+        ap.gq = bb.G32;
+        ap.cdiag = bb.C32;
+        ap.tw = ov.tw32;
+    }
     VecSel vk;  // u_k of each system: V_s + k n
     vk.base = bb.V;
     vk.stride = n;
@@ -343,23 +368,23 @@ int solve_bucket(cg_ctx *ctx, const cg_system *sys, const std::vector<int> &idx,
     xs.sys = n;
 
     auto enqueue_begin = [&](cudaStream_t q) -> int {
-        BK_LAUNCH(launch_rows_forward(0, a, xs, nullptr, nullptr, GATE_NONE, q));
-        BK_LAUNCH(launch_cols_convolve(0, a, nullptr, GATE_NONE, q));
-        BK_LAUNCH(launch_rows_inverse(0, 1, 0, a, xs, nullptr, bb.B, v0, kp.npart, nullptr, GATE_NONE, q));
+        BK_LAUNCH(launch_rows_forward(0, a64, xs, nullptr, nullptr, GATE_NONE, q));
+        BK_LAUNCH(launch_cols_convolve(0, a64, nullptr, GATE_NONE, q));
+        BK_LAUNCH(launch_rows_inverse(0, 1, prec, a64, xs, nullptr, bb.B, v0, kp.npart, nullptr, GATE_NONE, q));
         BK_LAUNCH(launch_cycle_begin(kp, nrb, q));
         return CG_OK;
     };
     auto enqueue_cycle = [&](cudaStream_t q) -> int {
         for (int i = 0; i < m + 1; i++) {
-            BK_LAUNCH(launch_rows_forward(0, a, vk, nullptr, kp.st, GATE_STOP, q));
-            BK_LAUNCH(launch_cols_convolve(0, a, kp.st, GATE_STOP, q));
-            BK_LAUNCH(launch_rows_inverse(0, 0, 0, a, vk, nullptr, nullptr, vk1, nullptr, kp.st, GATE_STOP, q));
-            BK_LAUNCH(launch_dots2(0, bb.V, n, kp, ndot2, sms_eff, q));
+            BK_LAUNCH(launch_rows_forward(prec, ap, vk, nullptr, kp.st, GATE_STOP, q));
+            BK_LAUNCH(launch_cols_convolve(prec, ap, kp.st, GATE_STOP, q));
+            BK_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vk, nullptr, nullptr, vk1, nullptr, kp.st, GATE_STOP, q));
+            BK_LAUNCH(launch_dots2(prec, bb.V, n, kp, ndot2, sms_eff, q));
             BK_LAUNCH(launch_dcgs2_step(kp, q));
-            BK_LAUNCH(launch_axpy2(0, bb.V, n, kp, nax2, sms_eff, q));
+            BK_LAUNCH(launch_axpy2(prec, bb.V, n, kp, nax2, sms_eff, q));
         }
         BK_LAUNCH(launch_backsolve(kp, q));
-        BK_LAUNCH(launch_axpy(0, 0, bb.V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, q));
+        BK_LAUNCH(launch_axpy(prec, 0, bb.V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, q));
         return CG_OK;
     };
     // capture [cycle + next residual and decisions] once; replay per cycle
@@ -455,7 +480,8 @@ extern "C" int cugmres_solve_buckets(int device, int nsys, const cg_system *sys,
     if (opts_in) o = *opts_in;
     else cugmres_default_opts(&o);
     if (o.restart < 1 || o.max_iter < 0 || !(o.tol >= 0.0)) return CG_ERR_INVALID;
-    if (o.precision != CG_PREC_FP64 || o.ortho != CG_ORTHO_DCGS2 || o.preconditioner != CG_PRECOND_NONE ||
+    if ((o.precision != CG_PREC_FP64 && o.precision != CG_PREC_MIXED) || o.ortho != CG_ORTHO_DCGS2 ||
+        o.preconditioner != CG_PRECOND_NONE ||
         o.transpose || o.fixed_iterations || o.restart > 4500)
         return CG_ERR_NOT_IMPLEMENTED;
     for (int i = 0; i < nsys; i++)
@@ -493,9 +519,11 @@ extern "C" int cugmres_solve_buckets(int device, int nsys, const cg_system *sys,
         int L = 16;
         while (L < 2 * N - 1) L *= 2;
         const long long n = (long long)N * N;
-        const size_t per = sizeof(double2) * ((size_t)(o.restart + 2) * n + (size_t)N * L + (size_t)(L / 2 + 1) * (L / 2 + 1) +
-                                              2 * (size_t)n) +
-                           sizeof(double) * (size_t)n + ((size_t)16 << 20);
+        const size_t esz = o.precision == CG_PREC_MIXED ? sizeof(float2) : sizeof(double2);
+        const size_t per = esz * (size_t)(o.restart + 2) * n +
+                           sizeof(double2) * ((size_t)N * L + (size_t)(L / 2 + 1) * (L / 2 + 1) + 2 * (size_t)n) +
+                           sizeof(float2) * (size_t)(L / 2 + 1) * (L / 2 + 1) + (sizeof(double) + sizeof(float)) * n +
+                           ((size_t)16 << 20);
         int cap = (int)std::max<size_t>(1, (free_b / 2) / per);
         if (max_bucket > 0) cap = std::min(cap, max_bucket);
         for (size_t b0 = 0; b0 < ids.size(); b0 += cap) {

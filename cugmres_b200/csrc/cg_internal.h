@@ -145,10 +145,13 @@ void ctx_set_shared_gpu(cg_ctx *c, bool on);
 // solver, which copies each system's spectrum and contrast into its own arrays.
 struct OpView {
     int N, L, sms;
-    int var[3];  // FP64 launch shapes of the three matvec passes
+    int var[2][3];  // launch shapes of the three matvec passes, FP64 and FP32
     const double2 *gq64;
+    const float2 *gq32;
     const double *c64;
+    const float *c32;
     const double2 *tw64;
+    const float2 *tw32;
     cudaStream_t stream;
 };
 int ctx_op_view(const cg_ctx *c, OpView *v);

@@ -67,7 +67,12 @@ typedef MvShape<16, 256, 128, 256, 2> MvV7;
 // staging and named barrier, so one transform's shared-memory exchanges can
 // overlap another's butterflies instead of the whole block stepping together.
 typedef MvShape<16, 256, 256, 512, 1, 2> MvV8;
-constexpr int MV_VARIANTS = 9;
+// Pipelined forward row pass (k_rows_forward_pipe: persistent workers of 256
+// threads, two per block, each staging its next row's x and contrast with
+// cp.async while it transforms the current row), 8 points per thread; its
+// column pass is V6's.
+typedef MvShape<8, 512, 512, 512, 1, 3> MvV9;
+constexpr int MV_VARIANTS = 10;
 
 template <int L, typename SH> struct RowCfg {
     typedef Plan<L, SH::E> P;
@@ -187,6 +192,16 @@ template <typename C> static __device__ __forceinline__ void cp_async_elem(C *ds
         asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(cg_smem_u32(dst)), "l"(src) : "memory");
     else
         asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(cg_smem_u32(dst)), "l"(src) : "memory");
+}
+// copy of one 4-, 8- or 16-byte value (the type's size)
+template <typename T> static __device__ __forceinline__ void cp_async_val(T *dst, const T *src) {
+    static_assert(sizeof(T) == 4 || sizeof(T) == 8 || sizeof(T) == 16, "cp.async copies 4, 8 or 16 bytes");
+    if constexpr (sizeof(T) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(cg_smem_u32(dst)), "l"(src) : "memory");
+    else if constexpr (sizeof(T) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(cg_smem_u32(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(cg_smem_u32(dst)), "l"(src) : "memory");
 }
 static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 template <int NPEND> static __device__ __forceinline__ void cp_async_wait() {
@@ -361,6 +376,90 @@ k_cols_convolve_grp(C *__restrict__ T, const C *__restrict__ gq, const C *__rest
     cp_async_wait<0>();
 }
 
+// Pass 1, persistent and double-buffered: the block's G = THREADS / TPR
+// transforms are independent workers (named barrier 1 + g, or the block's when
+// G = 1).  Worker w = blockIdx.x G + g walks rows w, w + W, ... (W = gridDim.x G)
+// and stages its next row of x and of the contrast (contiguous, so every copy
+// is coalesced) into its own half of a double buffer with cp.async while it
+// transforms the current row; its base twiddles stay in registers.  Same
+// arithmetic, in the same order, as k_rows_forward.
+template <int L, typename SH, int ESZ> struct RowPipeCfg {
+    typedef Plan<L, SH::E> P;
+    static constexpr int TPR = P::TPR;
+    static constexpr int THREADS = SH::ROWT > TPR ? SH::ROWT : TPR;
+    static constexpr int G = THREADS / TPR;
+    static constexpr bool OK = (TPR % 32 == 0) && G <= 15 && G * TPR == THREADS;
+    static constexpr int NT = G > 1 ? TPR : 0;
+    static constexpr int XS = L / 2;  // staged row of x (N <= L/2), elements of the complex type
+    static constexpr int CS = L / 2;  // staged row of the contrast, elements of the real type
+    static constexpr size_t SLOT_BYTES = (size_t)XS * ESZ + (size_t)CS * (ESZ / 2);
+    static constexpr size_t GROUP_BYTES = (size_t)P::SMEM_ELEMS * ESZ + 2 * SLOT_BYTES;
+    static constexpr size_t SMEM_BYTES = G * GROUP_BYTES;
+};
+
+template <typename C, int L, typename SH>
+__global__ void __launch_bounds__(RowPipeCfg<L, SH, sizeof(C)>::THREADS, 1)
+k_rows_forward_pipe(VecSel xs, const double *__restrict__ xscale, const typename real_of<C>::type *__restrict__ cdiag,
+                    C *__restrict__ T, const C *__restrict__ tw, int N, const DevState *st, int gate, SysSel sy) {
+    typedef typename real_of<C>::type R;
+    typedef Plan<L, SH::E> P;
+    typedef RowPipeCfg<L, SH, sizeof(C)> G;
+    constexpr int E = P::E, TPR = P::TPR, NT = G::NT;
+    st = sys_move_bytes(st, sy.ws);
+    if (gated(st, gate)) return;
+    xscale = sys_move_bytes(xscale, sy.ws);
+    if (cdiag) cdiag += (long long)blockIdx.y * sy.c;
+    T += (long long)blockIdx.y * sy.T;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int g = threadIdx.x / TPR, t = threadIdx.x % TPR;
+    const int bar = 1 + g;
+    unsigned char *gb = smraw + (size_t)g * G::GROUP_BYTES;
+    C *sm = reinterpret_cast<C *>(gb);
+    unsigned char *slots = gb + (size_t)P::SMEM_ELEMS * sizeof(C);
+    const long long ks = sel_index(st, xs.koff);
+    const C *x = reinterpret_cast<const C *>(xs.base) + ks * xs.stride + (long long)blockIdx.y * xs.sys;
+    const R s = xscale ? (R)xscale[ks] : (R)1;
+    const int W = gridDim.x * G::G;
+    auto issue = [&](int row, int slot) {
+        C *xd = reinterpret_cast<C *>(slots + slot * G::SLOT_BYTES);
+        R *cd = reinterpret_cast<R *>(slots + slot * G::SLOT_BYTES + (size_t)G::XS * sizeof(C));
+        const size_t rb = (size_t)row * (size_t)N;
+        for (int e = t; e < N; e += TPR) cp_async_val(xd + e, x + rb + e);
+        if (cdiag)
+            for (int e = t; e < N; e += TPR) cp_async_val(cd + e, cdiag + rb + e);
+        cp_async_commit();
+    };
+    C wb[TwBase<L, SH::E>::COUNT];
+    load_tw_base<L, SH::E>(tw, t, wb);
+    int row = blockIdx.x * G::G + g;
+    if (row < N) issue(row, 0);
+    for (int it = 0; row < N; it++, row += W) {
+        const int slot = it & 1;
+        if (row + W < N) issue(row + W, slot ^ 1);
+        else cp_async_commit();  // empty group: the wait below always leaves one group pending
+        cp_async_wait<1>();
+        fft_barrier<NT>(bar);
+        const C *xd = reinterpret_cast<const C *>(slots + slot * G::SLOT_BYTES);
+        const R *cd = reinterpret_cast<const R *>(slots + slot * G::SLOT_BYTES + (size_t)G::XS * sizeof(C));
+        C reg[E];
+#pragma unroll
+        for (int p = 0; p < E; p++) {
+            const int idx = t + p * TPR;
+            reg[p] = czero<C>();
+            if (p < E / 2 && idx < N) {
+                const R c = cdiag ? cd[idx] * s : s;  // cdiag == null: transpose operator
+                reg[p] = cscale(xd[idx], c);
+            }
+        }
+        fft_run_wb<L, SH::E, false, true, 1, NT>(reg, sm, wb, t, bar);
+        C *out = T + (size_t)row * L;
+#pragma unroll
+        for (int p = 0; p < E; p++) out[t + p * TPR] = reg[p];
+        fft_barrier<NT>(bar);  // this slot is refilled by the next iteration's issue
+    }
+    cp_async_wait<0>();
+}
+
 // ---------------------------------------------------------------- pass 3
 template <typename C, typename CO, int L, int MODE, typename SH>
 __global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
@@ -495,7 +594,7 @@ template <typename K> static int set_smem(K kern, size_t bytes) {
 // The three passes for one launch shape SH and one embedding size L.
 // The row passes do not depend on the column fields (COLT64, COLT32, PIPE):
 // shapes that differ only in them share one row-pass instantiation.
-template <typename SH> using RowShape = MvShape<SH::E, SH::ROWT, 0, 0, SH::MINB, 0>;
+template <typename SH> using RowShape = MvShape<SH::E, SH::ROWT, 0, 0, SH::MINB, SH::PIPE == 3 ? 3 : 0>;
 
 template <typename SH0, int L> struct Passes {
     typedef RowShape<SH0> SH;  // row passes
@@ -504,6 +603,28 @@ template <typename SH0, int L> struct Passes {
                    cudaStream_t s) {
         typedef RowCfg<L, SH> Q;
         const int grid = (a.N + Q::RPC - 1) / Q::RPC;
+        if constexpr (SH::PIPE == 3 && RowPipeCfg<L, SH, 16>::OK) {
+            typedef RowPipeCfg<L, SH, 16> G64;
+            typedef RowPipeCfg<L, SH, 8> G32;
+            const int nblk = (a.N + G64::G - 1) / G64::G;
+            const int pg = nblk < a.sms ? nblk : a.sms;
+            if (prec == 0) {
+                auto kern = k_rows_forward_pipe<double2, L, SH>;
+                int e = set_smem(kern, G64::SMEM_BYTES);
+                if (e) return e;
+                kern<<<dim3(pg, a.nsys), G64::THREADS, G64::SMEM_BYTES, s>>>(
+                    x, xs, a.transpose ? nullptr : (const double *)a.cdiag, (double2 *)a.T, (const double2 *)a.tw, a.N,
+                    st, gate, sys_sel(a));
+            } else {
+                auto kern = k_rows_forward_pipe<float2, L, SH>;
+                int e = set_smem(kern, G32::SMEM_BYTES);
+                if (e) return e;
+                kern<<<dim3(pg, a.nsys), G32::THREADS, G32::SMEM_BYTES, s>>>(
+                    x, xs, a.transpose ? nullptr : (const float *)a.cdiag, (float2 *)a.T, (const float2 *)a.tw, a.N, st,
+                    gate, sys_sel(a));
+            }
+            return (int)cudaGetLastError();
+        }
         if (prec == 0) {
             const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(double2);
             auto kern = k_rows_forward<double2, L, SH>;
@@ -618,6 +739,7 @@ template <template <typename> class F, typename... A> static int dispatch(int va
         case 6: CG_V_CASES(MvV6)
         case 7: CG_V_CASES(MvV7)
         case 8: CG_V_CASES(MvV8)
+        case 9: CG_V_CASES(MvV9)
         default: return -1;
     }
 #undef CG_V_CASES
@@ -650,7 +772,7 @@ int fft_supported(int L) {
 
 int matvec_variants(int L) { return L >= 128 ? MV_VARIANTS : 1; }
 
-int matvec_variant_persistent(int v) { return v == 5 || v == 6 || v == 8; }
+int matvec_variant_persistent(int v) { return v == 5 || v == 6 || v == 8 || v == 9; }
 
 int rows_per_block(int variant, int L) { return dispatch<RpcF>(variant, L); }
 

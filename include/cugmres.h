@@ -154,7 +154,7 @@ int cugmres_set_operator_circulant(cg_ctx *ctx, int N, const cg_c64 *g_prep, con
 int cugmres_grid_size(const cg_ctx *ctx, int *N, int *L);
 /* Launch shapes the autotuner chose for the three matvec passes (row forward,
  * column convolution, row inverse) of `precision`; shapes[3] receives indices
- * 0..8 (0 for embeddings L < 128).  Tuning runs in cugmres_set_operator and is
+ * 0..9 (0 for embeddings L < 128).  Tuning runs in cugmres_set_operator and is
  * cached per device in $CUGMRES_TUNE_CACHE (default
  * ~/.cache/cugmres_b200/autotune.txt); CUGMRES_AUTOTUNE=0 keeps shape 0. */
 int cugmres_matvec_shapes(const cg_ctx *ctx, int precision, int *shapes);
@@ -208,8 +208,9 @@ int cugmres_solve_batch(int device, int nsys, const cg_system *systems, const cg
  * restart cycle of a bucket is one CUDA-graph replay; systems that stop early
  * skip the rest of their bucket's launches.  results[i].seconds is the time
  * from the start of system i's bucket (its operator set-up included) to the
- * cycle boundary at which it finished.  Supports FP64, CG_ORTHO_DCGS2, no
- * preconditioner, A x = b; other options return CG_ERR_NOT_IMPLEMENTED.
+ * cycle boundary at which it finished.  Supports CG_PREC_FP64 and CG_PREC_MIXED,
+ * CG_ORTHO_DCGS2, no preconditioner, A x = b; other options return
+ * CG_ERR_NOT_IMPLEMENTED.
  * Per-system convergence is in results[i].status. */
 int cugmres_solve_buckets(int device, int nsys, const cg_system *systems, const cg_opts *opts, int max_bucket,
                           cg_result *results);

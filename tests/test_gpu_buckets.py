@@ -63,7 +63,27 @@ def test_bucket_system_matches_oracle(cuda_device, oracle):
     assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
 
 
+def test_buckets_mixed_precision_match_single_solves(cuda_device):
+    """complex64 cycles with the FP64 residual and update, in lockstep: each
+    system converges like its single mixed-precision solve (within two steps:
+    the complex64 reductions round differently in a bucket) to the same
+    solution, and to 1e-10 in FP64."""
+    systems = [s for s in _systems()[:8]]
+    kw = dict(restart=30, max_iter=600, tol=1e-10, precision="mixed", inner_tol=1e-5)
+    xs, infos = cg.solve_batch(systems, device=cuda_device, mode="buckets", **kw)
+    for sysd, x, info in zip(systems, xs, infos):
+        with cg.Solver(cuda_device) as s:
+            s.set_operator_green(sysd["N"], sysd["chi"], sysd["chi_scale"], sysd["k0"], sysd["h"])
+            xr, ir = s.solve(sysd["b"], **kw)
+            _, rel = s.residual(sysd["b"], x)
+        assert info["status"] == ir["status"], (sysd["N"], info, ir)
+        if ir["status"] == 0:
+            assert abs(info["iterations"] - ir["iterations"]) <= 2
+            assert rel <= 1e-10
+            assert np.linalg.norm(x - xr) / np.linalg.norm(xr) < 1e-8
+
+
 def test_buckets_reject_what_they_do_not_run(cuda_device):
     systems = _systems()[:2]
     with pytest.raises(cg.CugmresError):
-        cg.solve_batch(systems, device=cuda_device, mode="buckets", precision="mixed")
+        cg.solve_batch(systems, device=cuda_device, mode="buckets", ortho="cgs2")

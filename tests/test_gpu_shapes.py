@@ -35,7 +35,7 @@ for N in (64, 128, 300, 512, 1024, 1100):
 """
 
 
-@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "4", "5", "6", "7", "8", "tuned"])
+@pytest.mark.parametrize("shape", ["0", "1", "2", "3", "4", "5", "6", "7", "8", "9", "tuned"])
 def test_matvec_shape_parity(cuda_device, shape, tmp_path):
     env = dict(os.environ)
     env["CUGMRES_TUNE_CACHE"] = str(tmp_path / "tune.txt")
