@@ -344,12 +344,14 @@ def learned_side(args, stream):
     return out
 
 
-def sweep_side(args, rank, world, device):
+def sweep_side(args, rank, world, device, precision="mixed"):
     """Config 4: independent systems with sides drawn from {96,...,512}, lambda/h
     ~ U(15, 30), eps_r ~ U(2, 12), one design seed each, solved in lockstep
     buckets (cugmres_solve_buckets: one launch per kernel per Arnoldi step for
     all systems of a bucket, one CUDA-graph replay per restart cycle, operators
-    built on the GPU), GMRES(200) to 1e-10 within --sweep-max-iter steps.  With
+    built on the GPU), GMRES(200) to 1e-10 within --sweep-max-iter steps, in
+    mixed precision (complex64 cycles that end when their estimate fell by 1e-7,
+    FP64 residual and update) or FP64.  With
     N ranks the systems are sharded largest-first over the ranks (no collective
     on the solve path); the job time is the maximum over ranks of each rank's
     synchronous sweep call (it returns when its GPU work is done), and the
@@ -358,7 +360,7 @@ def sweep_side(args, rank, world, device):
     from cugmres_b200 import dist as D
     from cugmres_b200 import problems as P
     systems = P.sweep(nsys=args.sweep, seed=0, with_green=False)
-    kw = dict(device=device, mode="buckets", restart=200, tol=args.tol)
+    kw = dict(device=device, mode="buckets", restart=200, tol=args.tol, precision=precision, inner_tol=1e-7)
     # untimed: one short solve per grid side of this rank's share, so every
     # embedding size is autotuned before the clock starts
     mine = D.shard_systems([s["N"] for s in systems], rank, world)
@@ -383,6 +385,7 @@ def sweep_side(args, rank, world, device):
                   "by_side": {str(N): {"systems": sum(1 for r in records if r["N"] == N),
                                        "converged": sum(1 for r in records if r["N"] == N and r["status"] == 0)}
                               for N in sorted({r["N"] for r in records})},
+                  "precision": precision,
                   "note": (f"GMRES(200), tol {args.tol:g}, at most {args.sweep_max_iter} steps per system; "
                            "latency = from the start of the system's bucket (set-up included) to the cycle "
                            "at which it finished")})
@@ -550,8 +553,8 @@ def main():
         if not args.no_learned:
             line["side"]["learned"] = learned_side(args, stream)
     if args.sweep > 0:
-        sw = sweep_side(args, rank, world, local)
-        line.setdefault("side", {})["sweep"] = sw
+        line.setdefault("side", {})["sweep"] = sweep_side(args, rank, world, local, "mixed")
+        line["side"]["sweep_fp64"] = sweep_side(args, rank, world, local, "fp64")
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args)
     if rank == 0:

@@ -90,12 +90,15 @@ def test_fno_forward_matches_oracle(net, B, H, W):
     assert err < 2e-2, err
 
 
-@pytest.mark.parametrize("local_last", [True, False])
-def test_fno_gradients_match_oracle(net, local_last):
+@pytest.mark.parametrize("local_last,shape", [(True, (2, 32, 40)), (False, (2, 32, 40)), (True, (1, 32, 1024))])
+def test_fno_gradients_match_oracle(net, local_last, shape):
+    """(1, 32, 1024): the width whose forward pass takes the tensor-core column
+    DFTs (BF16 twiddles, BF16 Z in the inverse) while the backward pass runs the
+    CUDA-core adjoint DFTs on what that forward saved."""
     p = _params(2)
     net.set_params(p)
     net.set_local_last(local_last)
-    chi, k0h, r, x = _inputs(2, 32, 40, 11)
+    chi, k0h, r, x = _inputs(*shape, 11)
     loss, g = net.loss_grad(chi, k0h, r, x)
     net.set_local_last(True)
     loss_ref, g_ref = FO.loss_grad(p, chi, k0h, r, x, bf16=True, local_last=local_last)
@@ -113,6 +116,62 @@ def test_fno_gradients_match_oracle(net, local_last):
         e = np.linalg.norm(g[a:b] - g_ref[a:b]) / np.linalg.norm(g_ref[a:b])
         # the oracle mirrors every BF16 rounding of the GPU; the rest is FP32 summation order
         assert e < 5e-2, (name, e)
+
+
+_CUDA_CORE_SCRIPT = r"""
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+from cugmres_b200 import learned
+d = np.load(sys.argv[2])
+n = learned.FNO(0, seed=0)
+n.set_params(d["p"])
+z = n.forward(d["chi"], d["k0h"], d["r"])
+loss, g = n.loss_grad(d["chi"], d["k0h"], d["r"], d["x"])
+np.savez(sys.argv[3], z=z, loss=np.float64(loss), g=g)
+"""
+
+
+def test_fno_tensor_core_dft_matches_cuda_core_path(net, tmp_path, capsys):
+    """The same network, inputs and parameters at W = 1024 through the
+    tensor-core column DFTs (this process) and through the CUDA-core ones
+    (a child process with CUGMRES_FNO_TC_DFT=0): forward output and every
+    gradient block agree to the BF16 rounding of the tensor-core path's Z and
+    twiddles.  Also records the error of each path against the oracle."""
+    import os
+    import subprocess
+    import sys
+    from conftest import ROOT
+    p = _params(5)
+    chi, k0h, r, x = _inputs(1, 32, 1024, 13)
+    net.set_params(p)
+    net.set_local_last(True)
+    z_tc = net.forward(chi, k0h, r)
+    loss_tc, g_tc = net.loss_grad(chi, k0h, r, x)
+    inp, out = tmp_path / "in.npz", tmp_path / "out.npz"
+    np.savez(inp, p=p, chi=chi, k0h=k0h, r=r, x=x)
+    env = dict(os.environ, CUGMRES_FNO_TC_DFT="0")
+    res = subprocess.run([sys.executable, "-c", _CUDA_CORE_SCRIPT, ROOT, str(inp), str(out)], env=env,
+                         capture_output=True, text=True, timeout=300)
+    assert res.returncode == 0, res.stdout + res.stderr
+    d = np.load(out)
+    ref = FO.forward(p, chi, k0h, r, bf16=True)
+    sc = ref["s"].numpy().reshape(-1, 1, 1)
+    corr_ref = (ref["z"].numpy() - r) / sc
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+    e_paths = rel((z_tc - r) / sc, (d["z"] - r) / sc)
+    e_tc, e_cc = rel((z_tc - r) / sc, corr_ref), rel((d["z"] - r) / sc, corr_ref)
+    assert e_paths < 1e-2, e_paths
+    assert abs(loss_tc - float(d["loss"])) <= 5e-3 * abs(float(d["loss"]))
+    worst = 0.0
+    for a, b in ((FO.OFF_P, FO.OFF_L0), (FO.OFF_L0, FO.OFF_Q1), (FO.OFF_Q1, FO.NPARAM)):
+        worst = max(worst, rel(g_tc[a:b], d["g"][a:b]))
+    assert worst < 5e-2, worst
+    with capsys.disabled():
+        print(f"\n  W=1024 correction vs oracle: tensor-core {e_tc:.2e}, CUDA-core {e_cc:.2e}; "
+              f"between the paths {e_paths:.2e}; gradients between the paths (worst block) {worst:.2e}")
 
 
 def test_fno_zero_input_gives_zero(net):
