@@ -30,7 +30,7 @@ __all__ = ["Solver", "CugmresError", "green_block", "helmholtz", "reference_cyli
 
 _PREC = {"fp64": _lib.CG_PREC_FP64, "mixed": _lib.CG_PREC_MIXED, "fp32": _lib.CG_PREC_MIXED}
 _GIV = {"unitary": _lib.CG_GIVENS_UNITARY, "reference": _lib.CG_GIVENS_REFERENCE}
-_ORTHO = {"dcgs2": _lib.CG_ORTHO_DCGS2, "cgs2": _lib.CG_ORTHO_CGS2}
+_ORTHO = {"dcgs2": _lib.CG_ORTHO_DCGS2, "cgs2": _lib.CG_ORTHO_CGS2, "sstep": _lib.CG_ORTHO_SSTEP}
 
 
 def _is_torch(a):
@@ -179,12 +179,14 @@ class Solver:
 
     def solve(self, b, x0=None, restart=100, max_iter=10000, tol=1e-10, precision="fp64", givens="unitary",
               inner_tol=1e-5, fixed_iterations=False, timeout_s=0.0, ortho="dcgs2", raise_on_failure=False,
-              preconditioner=None, learned_x0=False, transpose=False):
+              preconditioner=None, learned_x0=False, transpose=False, sstep=4):
         """Solve A x = b.  Returns (x, info) where info holds status, iterations,
         cycles, rel_residual_true / _estimate, seconds and res_hist.
         preconditioner="learned": flexible GMRES with the attached network
         (learned_x0: also start from x0 = M(b) when x0 is None).
-        transpose=True solves A^T x = b (the adjoint system of the gradient path)."""
+        transpose=True solves A^T x = b (the adjoint system of the gradient path).
+        ortho="sstep": s-step Arnoldi, `sstep` (2, 4 or 8) steps per block after a
+        first delayed-CGS2 cycle that gives the Newton shifts."""
         o = _lib.CgOpts()
         _lib.lib().cugmres_default_opts(ctypes.byref(o))
         o.restart = int(restart)
@@ -196,6 +198,7 @@ class Solver:
         o.fixed_iterations = int(bool(fixed_iterations))
         o.timeout_s = float(timeout_s)
         o.ortho = _ORTHO[ortho]
+        o.sstep = int(sstep)
         o.preconditioner = {None: 0, "none": 0, "learned": 1}[preconditioner]
         o.learned_x0 = int(bool(learned_x0))
         o.transpose = int(bool(transpose))

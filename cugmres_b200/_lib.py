@@ -25,6 +25,7 @@ CG_PREC_MIXED = 1
 CG_GIVENS_UNITARY = 0
 CG_ORTHO_DCGS2 = 0
 CG_ORTHO_CGS2 = 1
+CG_ORTHO_SSTEP = 2
 CG_GIVENS_REFERENCE = 1
 CG_GREEN_HELMHOLTZ = 0
 CG_GREEN_REFERENCE = 1
@@ -62,7 +63,8 @@ class CgOpts(ctypes.Structure):
         ("preconditioner", ctypes.c_int),
         ("learned_x0", ctypes.c_int),
         ("transpose", ctypes.c_int),
-        ("reserved", ctypes.c_int * 4),
+        ("sstep", ctypes.c_int),
+        ("reserved", ctypes.c_int * 3),
     ]
 
 

@@ -21,7 +21,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libcugmres.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["cg_matvec.cu", "cg_krylov.cu", "cg_dcgs2.cu", "cg_api.cu", "cg_noalloc.cu", "cg_batch.cu", "cg_fno.cu", "cg_green_dev.cu",
+SOURCES = ["cg_matvec.cu", "cg_krylov.cu", "cg_dcgs2.cu", "cg_sstep.cu", "cg_api.cu", "cg_noalloc.cu", "cg_batch.cu", "cg_fno.cu", "cg_green_dev.cu",
            "cg_green.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

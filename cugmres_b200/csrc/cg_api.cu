@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <array>
+#include <complex>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -257,6 +258,7 @@ void free_krylov(cg_ctx *c) {
     dfree_t(c->kp.S);
     dfree_t(c->kp.gpart);
     dfree_t(c->kp.tickets);
+    dfree_t(c->kp.ss);
     dfree(c->Z);
     c->zcap_bytes = 0;
     c->mcap = 0;
@@ -269,9 +271,10 @@ int dot_blocks(const cg_ctx *c) { return 2 * c->sms; }
 int axpy_blocks(const cg_ctx *c, long long n) { return grid_for(n, 4 * c->sms); }
 
 // Ensures basis and small-array capacity for restart m and budget maxit.
-int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
+// extra: basis slots beyond restart + 2 (an s-step block may run past the restart length)
+int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes, int extra = 0) {
     const long long n = (long long)c->N * c->N;
-    const size_t vbytes = (size_t)(m + 2) * (size_t)n * elem_bytes;
+    const size_t vbytes = (size_t)(m + 2 + extra) * (size_t)n * elem_bytes;
     const int nparts = std::max(std::max(axpy_blocks(c, n), dot_blocks(c)), std::max(c->N, 4 * c->sms));
     if (m > c->mcap || maxit > c->itcap || vbytes > c->vcap_bytes || nparts > c->nparts_cap) {
         const int mc = std::max(m, c->mcap), ic = std::max(maxit, c->itcap);
@@ -291,11 +294,17 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes) {
         const size_t part_cgs2 = 2 * (size_t)dot_blocks(c) * (mc + 1);
         const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) *
                                   (size_t)dots2_part_ld(mc);
-        CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(part_cgs2, part_dcgs2)));
-        const size_t ngroups = ((size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) + 15) / 16;
-        CG_CU(cudaMalloc((void **)&c->kp.gpart, sizeof(double) * 4 * ngroups * (size_t)dots2_part_ld(mc)));
+        const size_t nss = (size_t)sstep_blocks(c->sms, n);  // grid of the s-step block passes
+        const size_t part_ss = nss * (size_t)sstep_part_ld(mc);
+        CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(std::max(part_cgs2, part_dcgs2), part_ss)));
+        const size_t ng2 = ((size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) + 15) / 16;
+        const size_t ngs = (nss + 15) / 16;
+        const size_t ngroups = std::max(ng2, ngs);
+        CG_CU(cudaMalloc((void **)&c->kp.gpart, sizeof(double) * std::max(4 * ng2 * (size_t)dots2_part_ld(mc),
+                                                                          ngs * (size_t)sstep_part_ld(mc))));
         CG_CU(cudaMalloc((void **)&c->kp.tickets, sizeof(unsigned int) * ngroups));
         CG_CU(cudaMemset(c->kp.tickets, 0, sizeof(unsigned int) * ngroups));
+        CG_CU(cudaMalloc((void **)&c->kp.ss, sizeof(double2) * (size_t)sstep_scratch_elems(mc)));
         CG_CU(cudaMalloc((void **)&c->kp.npart, sizeof(double) * np));
         CG_CU(cudaMalloc((void **)&c->kp.Hm, sizeof(double2) * (size_t)(mc + 1) * (mc + 1)));
         CG_CU(cudaMalloc((void **)&c->kp.D1, sizeof(double2) * (mc + 2)));
@@ -545,7 +554,9 @@ int prof_mark(cg_ctx *c, CycleProf &cp, int phase, int iter, cudaStream_t s) {
 // Called once the stream has passed every recorded event.  steps_done: Arnoldi
 // steps that did work in the cycle these events cover (later steps were gated
 // off on device and move no bytes); e: element bytes of the cycle precision.
-int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed) {
+// ss > 0: the cycle ran s-step blocks of ss steps; a MATVEC interval then holds
+// the block's ss matvecs and iter is the block's first basis index.
+int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed, int ss = 0) {
     if (c->prof && cp.used >= 2) {
         for (int i = 0; i + 1 < cp.used; i++) {
             float ms = 0.f;
@@ -553,10 +564,15 @@ int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, b
             const int t = cp.tag[i], k = cp.iter[i];
             const bool live = k < steps_done;
             double bytes = 0.0;
-            switch (t) {
+            switch (ss > 0 ? -t - 100 : t) {
                 case CG_PHASE_MATVEC: bytes = live ? 16.0 * n * e : 0.0; break;
                 case CG_PHASE_DOTS: bytes = live ? (k + 2.0) * n * e : 0.0; break;
                 case CG_PHASE_AXPY: bytes = live ? (k + (delayed ? 4.0 : 3.0)) * n * e : 0.0; break;
+                case -CG_PHASE_MATVEC - 100: bytes = live ? ss * 16.0 * n * e : 0.0; break;
+                case -CG_PHASE_DOTS - 100: bytes = live ? (k + 1.0 + ss) * n * e : 0.0; break;  // Q^H W and W^H W
+                case -CG_PHASE_AXPY - 100: bytes = live ? (k + 1.0 + 2.0 * ss) * n * e : 0.0; break;  // W <- W A - Q B
+                case -CG_PHASE_UPDATE - 100: bytes = steps_done * n * e + 2.0 * n * 16.0; break;
+                case -CG_PHASE_RESIDUAL - 100: bytes = 16.0 * n * 16.0; break;
                 case CG_PHASE_UPDATE: bytes = (steps_done - (delayed ? 1 : 0)) * n * e + 2.0 * n * 16.0; break;
                 case CG_PHASE_RESIDUAL: bytes = 16.0 * n * 16.0; break;
                 default: bytes = 0.0;
@@ -572,6 +588,103 @@ int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, b
     cp.tag.clear();
     cp.iter.clear();
     return CG_OK;
+}
+
+// Eigenvalues of the leading n x n block of a complex upper Hessenberg matrix
+// (row-major, leading dimension ld): shifted QR iteration with Wilkinson
+// shifts, unitary Givens rotations and deflation at negligible subdiagonal
+// entries (Golub and Van Loan, Matrix Computations, 4th ed., sec. 7.5).  Only
+// the active window is updated, since only eigenvalues are wanted.
+std::vector<std::complex<double>> hessenberg_eigenvalues(const std::vector<double2> &Hin, int n, int ld) {
+    typedef std::complex<double> cd;
+    std::vector<cd> H((size_t)n * n, cd(0.0, 0.0)), ev(n);
+    for (int i = 0; i < n; i++)
+        for (int j = std::max(0, i - 1); j < n; j++) H[(size_t)i * n + j] = cd(Hin[(size_t)i * ld + j].x, Hin[(size_t)i * ld + j].y);
+    auto at = [&](int i, int j) -> cd & { return H[(size_t)i * n + j]; };
+    int hi = n - 1, iter = 0;
+    std::vector<cd> cs(n), sn(n);
+    while (hi >= 0) {
+        if (hi == 0) {
+            ev[0] = at(0, 0);
+            break;
+        }
+        int lo = hi;
+        while (lo > 0) {
+            const double sc = std::abs(at(lo - 1, lo - 1)) + std::abs(at(lo, lo));
+            if (std::abs(at(lo, lo - 1)) <= 1e-14 * (sc > 0.0 ? sc : 1.0)) break;
+            lo--;
+        }
+        if (lo == hi) {
+            ev[hi] = at(hi, hi);
+            hi--;
+            iter = 0;
+            continue;
+        }
+        if (++iter > 100) {  // no convergence: the diagonal of the window stands in
+            for (int i = lo; i <= hi; i++) ev[i] = at(i, i);
+            hi = lo - 1;
+            iter = 0;
+            continue;
+        }
+        const cd a = at(hi - 1, hi - 1), b = at(hi - 1, hi), c = at(hi, hi - 1), d = at(hi, hi);
+        const cd tr = a + d, det = a * d - b * c, disc = std::sqrt(tr * tr * 0.25 - det);
+        const cd m1 = tr * 0.5 + disc, m2 = tr * 0.5 - disc;
+        cd mu = std::abs(m1 - d) < std::abs(m2 - d) ? m1 : m2;
+        if (iter % 11 == 10) mu = d + 0.75 * std::abs(c);  // exceptional shift
+        for (int i = lo; i <= hi; i++) at(i, i) -= mu;
+        for (int j = lo; j < hi; j++) {
+            const cd x = at(j, j), y = at(j + 1, j);
+            const double r = std::sqrt(std::norm(x) + std::norm(y));
+            const cd cc = r > 0.0 ? x / r : cd(1.0, 0.0), ss = r > 0.0 ? y / r : cd(0.0, 0.0);
+            for (int k2 = j; k2 <= hi; k2++) {
+                const cd u = at(j, k2), v = at(j + 1, k2);
+                at(j, k2) = std::conj(cc) * u + std::conj(ss) * v;
+                at(j + 1, k2) = -ss * u + cc * v;
+            }
+            cs[j] = cc;
+            sn[j] = ss;
+        }
+        for (int j = lo; j < hi; j++) {
+            const cd cc = cs[j], ss = sn[j];
+            for (int i = lo; i <= std::min(j + 2, hi); i++) {
+                const cd u = at(i, j), v = at(i, j + 1);
+                at(i, j) = u * cc + v * ss;
+                at(i, j + 1) = -u * std::conj(ss) + v * std::conj(cc);
+            }
+        }
+        for (int i = lo; i <= hi; i++) at(i, i) += mu;
+    }
+    return ev;
+}
+
+// The first `count` points of a (modified) Leja ordering of `pts`: the largest
+// in modulus, then each next one maximising the product of distances to those
+// already taken (as logarithms); well-spread shifts keep the Newton basis of
+// the s-step blocks well conditioned (Reichel, BIT 30 (1990)).
+std::vector<std::complex<double>> leja_points(std::vector<std::complex<double>> pts, int count) {
+    std::vector<std::complex<double>> out;
+    if (pts.empty()) return out;
+    size_t first = 0;
+    for (size_t i = 1; i < pts.size(); i++)
+        if (std::abs(pts[i]) > std::abs(pts[first])) first = i;
+    out.push_back(pts[first]);
+    pts.erase(pts.begin() + first);
+    while ((int)out.size() < count && !pts.empty()) {
+        size_t best = 0;
+        double bv = -1e300;
+        for (size_t i = 0; i < pts.size(); i++) {
+            double v = 0.0;
+            for (const auto &q : out) v += std::log(std::abs(pts[i] - q) + 1e-300);
+            if (v > bv) {
+                bv = v;
+                best = i;
+            }
+        }
+        out.push_back(pts[best]);
+        pts.erase(pts.begin() + best);
+    }
+    while ((int)out.size() < count) out.push_back(out.back());
+    return out;
 }
 
 bool all_finite(const double *p, size_t n) {
@@ -925,10 +1038,16 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     else cugmres_default_opts(&o);
     if (o.restart < 1 || o.max_iter < 0 || !(o.tol >= 0.0) || (o.precision != CG_PREC_FP64 && o.precision != CG_PREC_MIXED) ||
         (o.givens != CG_GIVENS_UNITARY && o.givens != CG_GIVENS_REFERENCE) ||
-        (o.ortho != CG_ORTHO_DCGS2 && o.ortho != CG_ORTHO_CGS2) ||
+        (o.ortho != CG_ORTHO_DCGS2 && o.ortho != CG_ORTHO_CGS2 && o.ortho != CG_ORTHO_SSTEP) ||
         (o.preconditioner != CG_PRECOND_NONE && o.preconditioner != CG_PRECOND_LEARNED))
         return CG_ERR_INVALID;
     const bool learned = o.preconditioner == CG_PRECOND_LEARNED;
+    // s-step Arnoldi: S steps per block after a first delayed-CGS2 cycle (its Ritz values are the shifts)
+    const bool sstep = o.ortho == CG_ORTHO_SSTEP;
+    const int S = sstep ? (o.sstep > 0 ? o.sstep : 4) : 0;
+    if (sstep && (!sstep_supported(S) || learned || o.fixed_iterations || o.givens != CG_GIVENS_UNITARY ||
+                  o.restart < S))
+        return CG_ERR_INVALID;
     if (learned && !c->net) return CG_ERR_INVALID;
     if (learned && o.transpose) return CG_ERR_NOT_IMPLEMENTED;  // the network approximates A^-1, not A^-T
     if (learned && (c->N < 32 || c->N > 1024)) return CG_ERR_NOT_IMPLEMENTED;
@@ -940,7 +1059,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     const long long n = (long long)c->N * c->N;
     const size_t bytes = sizeof(double2) * n;
     const size_t esz = prec == 0 ? sizeof(double2) : sizeof(float2);
-    CG_TRY(ensure_krylov(c, m, std::max(1, o.max_iter), esz));
+    CG_TRY(ensure_krylov(c, m, std::max(1, o.max_iter), esz, S));
     cudaStream_t s = c->stream;
     if (learned) {
         // flexible GMRES keeps z_j = M(v_j) next to the basis
@@ -1089,6 +1208,66 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, q));
         return CG_OK;
     };
+    // s-step cycles (after the first, delayed-CGS2 cycle): ceil(m / S) blocks of
+    // S shifted matvecs, two block Gram-Schmidt passes and the Hessenberg /
+    // Givens kernel, then the back-solve and the update
+    bool ss_on = false;
+    double2 shifts[SS_MAX];
+    for (int i = 0; i < SS_MAX; i++) shifts[i] = make_double2(0.0, 0.0);
+    const int nss = sstep_blocks(c->sms, n);
+    auto enqueue_cycle_ss = [&](cudaStream_t q) -> int {
+        CG_LAUNCH(launch_ss_norm0(prec, c->V, n, kp, q));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
+        for (int b = 0; b * S < m; b++) {
+            for (int i = 0; i < S; i++) {
+                VecSel vin = vk, vout = vk;
+                vin.koff = i;
+                vout.koff = i + 1;
+                CG_LAUNCH(launch_rows_forward(prec, ap, vin, nullptr, c->st, GATE_STOP, q));
+                CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, q));
+                CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vin, nullptr, nullptr, vout, nullptr, c->st, GATE_STOP,
+                                              q, shifts[i]));
+            }
+            CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, b * S, q));
+            for (int pass = 0; pass < 2; pass++) {
+                CG_LAUNCH(launch_ss_dots(prec, c->V, n, kp, S, nss, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, b * S, q));
+                CG_LAUNCH(launch_ss_chol(kp, S, pass, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, b * S, q));
+                CG_LAUNCH(launch_ss_update(prec, c->V, n, kp, S, nss, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, b * S, q));
+            }
+            CG_LAUNCH(launch_ss_hess(kp, S, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, b * S, q));
+        }
+        CG_LAUNCH(launch_backsolve(kp, q));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
+        CG_LAUNCH(launch_axpy(prec, 0, c->V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, q));
+        CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, q));
+        return CG_OK;
+    };
+    // The first cycle's Hessenberg (delayed CGS2 keeps it unrotated in Hm)
+    // gives the shifts: Leja-ordered Ritz values.  Returns false (s-step stays
+    // off) when the cycle had fewer than S columns.
+    auto setup_shifts = [&](int ncol1) -> int {
+        if (ncol1 < S) return CG_OK;
+        const int ld = c->mcap + 1;
+        std::vector<double2> hm((size_t)ncol1 * ld);
+        CG_CU(cudaMemcpyAsync(hm.data(), kp.Hm, sizeof(double2) * hm.size(), cudaMemcpyDeviceToHost, s));
+        CG_CU(cudaStreamSynchronize(s));
+        const std::vector<std::complex<double>> ritz = hessenberg_eigenvalues(hm, ncol1, ld);
+        for (const auto &z : ritz)
+            if (!std::isfinite(z.real()) || !std::isfinite(z.imag())) return CG_OK;
+        const std::vector<std::complex<double>> th = leja_points(ritz, S);
+        for (int i = 0; i < S; i++) shifts[i] = make_double2(th[i].real(), th[i].imag());
+        // the Hessenberg kernel reads them from the scratch (offset of SsLayout::Th)
+        const long long M1 = c->mcap + 1;
+        const long long th_off = 3 * M1 * SS_MAX + 3 * SS_MAX * SS_MAX;
+        CG_CU(cudaMemcpyAsync(kp.ss + th_off, shifts, sizeof(double2) * SS_MAX, cudaMemcpyHostToDevice, s));
+        CG_CU(cudaStreamSynchronize(s));
+        ss_on = true;
+        return CG_OK;
+    };
     // Graph replay of [cycle + next residual/decisions] when nothing in it
     // changes between cycles (not while profiling, not with the network).
     // (flexible GMRES: plain cycles after the probe only)
@@ -1098,15 +1277,19 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     auto make_key = [&]() {
         memset(key, 0, sizeof(key));
         struct K {
-            int prec, delayed, m, transpose, ndot, nax, ndot2, nax2, nrb, mcap, var[2][3];
+            int prec, delayed, m, transpose, ndot, nax, ndot2, nax2, nrb, mcap, var[2][3], ss, nss;
             long long n;
             const void *V, *x, *b, *st, *scale, *part;
+            double2 shifts[SS_MAX];
         } kk;
         memset(&kk, 0, sizeof(kk));
         kk.prec = prec, kk.delayed = delayed, kk.m = m, kk.transpose = o.transpose, kk.ndot = ndot, kk.nax = nax;
         kk.ndot2 = ndot2, kk.nax2 = nax2, kk.nrb = nrb, kk.mcap = c->mcap, kk.n = n;
         memcpy(kk.var, c->var, sizeof(kk.var));
         kk.V = c->V, kk.x = xp, kk.b = bp, kk.st = c->st, kk.scale = kp.scale, kk.part = kp.part;
+        kk.ss = ss_on ? S : 0;
+        kk.nss = nss;
+        if (ss_on) memcpy(kk.shifts, shifts, sizeof(shifts));
         static_assert(sizeof(K) <= sizeof(key), "graph key");
         memcpy(key, &kk, sizeof(kk));
     };
@@ -1117,7 +1300,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             if (!c->cap_stream) CG_CU(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
             cudaGraph_t g = nullptr;
             CG_CU(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
-            int e1 = enqueue_cycle(m + (delayed ? 1 : 0), c->cap_stream);
+            int e1 = ss_on ? enqueue_cycle_ss(c->cap_stream) : enqueue_cycle(m + (delayed ? 1 : 0), c->cap_stream);
             int e2 = e1 == CG_OK ? enqueue_begin(c->cap_stream) : e1;
             cudaError_t ce = cudaStreamEndCapture(c->cap_stream, &g);
             if (e2 != CG_OK || ce != cudaSuccess) {
@@ -1144,8 +1327,12 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_CU(cudaEventRecord(c->ev, s));
         CG_CU(cudaEventSynchronize(c->ev));
         const DevState hs = *c->st_host;
-        CG_TRY(prof_collect(c, cp, nd, esz_d, hs.it - it_prev + (delayed ? 1 : 0), delayed));
+        CG_TRY(prof_collect(c, cp, nd, esz_d, hs.it - it_prev + (delayed && !ss_on ? 1 : 0), delayed && !ss_on,
+                            ss_on ? S : 0));
+        const int cycle_steps = hs.it - it_prev;
         it_prev = hs.it;
+        // the first cycle has ended and the second begun: its Hessenberg gives the shifts
+        if (sstep && !ss_on && hs.cycles == 2 && hs.status == 0) CG_TRY(setup_shifts(std::min(cycle_steps, m)));
         if (x0_learned == 1 && hs.cycles == 1 && hs.status == 0 && !(hs.true_res < 1.0)) {
             // M(b) did not beat x0 = 0: restart from zero (the cycle counter and budget are unchanged
             // because no Arnoldi step ran)
@@ -1192,8 +1379,22 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             if (d != delayed) CG_LAUNCH(launch_set_ortho(kp, d ? 0 : 1, s));
             delayed = d;
         }
-        if (graphs && !use_prec && !(learned && rate_plain < 0.0)) {
+        // s-step, first cycle: delayed CGS2 for the shifts, at most 64 steps when the
+        // restart is long (an unrestarted solve would otherwise spend its whole
+        // budget before the s-step blocks start); restarts up to 128 keep their
+        // full first cycle, so GMRES(m) iterates are those of the other schemes
+        const bool ss_probe = sstep && !ss_on;
+        if (ss_probe) {
+            int len = std::min(m <= 128 ? m : 64, o.max_iter - hs.it);
+            CG_TRY(enqueue_cycle(len + 1, s));
+            CG_TRY(prof_mark(c, cp, -1, -1, s));
+            CG_TRY(enqueue_begin(s));
+        } else if (graphs && !use_prec && !(learned && rate_plain < 0.0)) {
             CG_TRY(launch_cycle_graph());
+        } else if (ss_on) {
+            CG_TRY(enqueue_cycle_ss(s));
+            CG_TRY(prof_mark(c, cp, -1, -1, s));
+            CG_TRY(enqueue_begin(s));
         } else {
             int len = std::min(m, o.max_iter - hs.it);
             if (learned && (use_prec || rate_plain < 0.0)) len = std::min(len, LEARNED_CYCLE_STEPS);

@@ -62,6 +62,7 @@ struct KrylovPtrs {
     double2 *S;      // [m+1] axpy coefficients for u_{k+1}
     double *gpart;   // [ceil(nblk_dots2 / 16) * 4 * part_ld] group sums of the dot partials
     unsigned int *tickets;  // [ceil(nblk_dots2 / 16)] arrival counters of those groups (reset by the last)
+    double2 *ss = nullptr;  // s-step scratch (cg_sstep.cu: block coefficients, Gram, shifts, work rows)
     int mcap;        // allocated restart capacity (leading dimension of Rm / part)
     // Bucket of systems solved in lockstep (one launch covers all of them,
     // system = blockIdx.y): every array above (st included) of system s lies
@@ -77,10 +78,10 @@ struct KrylovPtrs {
 __device__ __forceinline__ KrylovPtrs kp_sys(KrylovPtrs kp) {
     if (kp.sys_ws == 0) return kp;
     const long long o = (long long)blockIdx.y * kp.sys_ws;
-#define CG_MOVE(f) kp.f = reinterpret_cast<decltype(kp.f)>(reinterpret_cast<char *>(kp.f) + o)
+#define CG_MOVE(f) kp.f = kp.f ? reinterpret_cast<decltype(kp.f)>(reinterpret_cast<char *>(kp.f) + o) : kp.f
     CG_MOVE(st); CG_MOVE(scale); CG_MOVE(h1); CG_MOVE(h2); CG_MOVE(Rm); CG_MOVE(cs); CG_MOVE(sn);
     CG_MOVE(g); CG_MOVE(y); CG_MOVE(hist); CG_MOVE(part); CG_MOVE(npart); CG_MOVE(Hm); CG_MOVE(D1);
-    CG_MOVE(D2); CG_MOVE(tv); CG_MOVE(P); CG_MOVE(S); CG_MOVE(gpart); CG_MOVE(tickets);
+    CG_MOVE(D2); CG_MOVE(tv); CG_MOVE(P); CG_MOVE(S); CG_MOVE(gpart); CG_MOVE(tickets); CG_MOVE(ss);
 #undef CG_MOVE
     return kp;
 }
@@ -129,9 +130,11 @@ struct VecSel {
 int launch_rows_forward(int prec, const MatvecArgs &a, VecSel x, const double *xscale_base, const DevState *st,
                         int gate, cudaStream_t s);
 int launch_cols_convolve(int prec, const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s);
-// mode 0: y = s*x - conv;  mode 1: y = b - x + conv (y may be float2 while the matvec is double2: out_prec)
+// mode 0: y = s (1 - shift) x - conv = (A - shift) (s x);  mode 1: y = b - x + conv
+// (y may be float2 while the matvec is double2: out_prec)
 int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xscale_base,
-                        const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s);
+                        const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s,
+                        double2 shift = double2{0.0, 0.0});
 int rows_per_block(int variant, int L);
 int fft_supported(int L);
 int matvec_variants(int L);
@@ -179,6 +182,17 @@ int launch_backsolve(const KrylovPtrs &kp, cudaStream_t s);
 int launch_cycle_begin(const KrylovPtrs &kp, int nparts, cudaStream_t s);
 // ortho 0: delayed CGS2, 1: CGS2, for the cycle k_cycle_begin has just set up
 int launch_set_ortho(const KrylovPtrs &kp, int ortho, cudaStream_t s);
+// s-step Arnoldi (cg_sstep.cu): S steps per block, S in {2, 4, 8}
+constexpr int SS_MAX = 8;
+int sstep_supported(int S);
+long long sstep_scratch_elems(int mcap);  // double2 entries of KrylovPtrs::ss
+int sstep_part_ld(int mcap);              // partials per block of the block dot pass
+int sstep_blocks(int sms, long long n);   // grid of the block dot and update passes
+int launch_ss_norm0(int prec, void *V, long long n, const KrylovPtrs &kp, cudaStream_t s);
+int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int nblk, cudaStream_t s);
+int launch_ss_chol(const KrylovPtrs &kp, int S, int pass, cudaStream_t s);
+int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int nblk, cudaStream_t s);
+int launch_ss_hess(const KrylovPtrs &kp, int S, cudaStream_t s);
 int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
                  cudaStream_t s);
 int launch_convert(int from_prec, int to_prec, const void *src, void *dst, long long n, cudaStream_t s);

@@ -465,7 +465,7 @@ template <typename C, typename CO, int L, int MODE, typename SH>
 __global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
 k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xscale, const C *__restrict__ bvec,
                VecSel ys, double *__restrict__ npart, const C *__restrict__ tw, int N, const DevState *st, int gate,
-               const typename real_of<C>::type *__restrict__ cout, SysSel sy) {
+               const typename real_of<C>::type *__restrict__ cout, SysSel sy, double2 shift) {
     typedef typename real_of<C>::type R;
     typedef typename real_of<CO>::type RO;
     typedef Plan<L, SH::E> P;
@@ -519,7 +519,8 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
                 if (cout) reg[p] = cscale(reg[p], cout[rb + idx]);  // transpose: contrast after G
                 C o;
                 if (MODE == 0) {
-                    o = csub(cscale(xv[p], s), reg[p]);
+                    // (A - shift) applied to s x: s (1 - shift) x - G c s x
+                    o = csub(cmul(xv[p], mk<C>((R)(s * (1.0 - shift.x)), (R)(-s * shift.y))), reg[p]);
                 } else {
                     o = cadd(csub(bv[p], xv[p]), reg[p]);
                 }
@@ -684,7 +685,7 @@ template <typename SH0, int L> struct Passes {
 
     template <typename C, typename CO, int MODE>
     static int inv_t(const MatvecArgs &a, VecSel x, const double *xs, const void *b, VecSel y, double *npart,
-                     const DevState *st, int gate, cudaStream_t s) {
+                     const DevState *st, int gate, cudaStream_t s, double2 shift) {
         typedef RowCfg<L, SH> Q;
         const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
         auto kern = k_rows_inverse<C, CO, L, MODE, SH>;
@@ -694,18 +695,19 @@ template <typename SH0, int L> struct Passes {
         typedef typename real_of<C>::type R;
         kern<<<dim3(grid, a.nsys), Q::THREADS, smem, s>>>((const C *)a.T, x, xs, (const C *)b, y, npart,
                                                             (const C *)a.tw, a.N, st, gate,
-                                                            a.transpose ? (const R *)a.cdiag : nullptr, sys_sel(a));
+                                                            a.transpose ? (const R *)a.cdiag : nullptr, sys_sel(a),
+                                                            shift);
         return (int)cudaGetLastError();
     }
     static int inv(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xs, const void *b,
-                   VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s) {
+                   VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s, double2 sh) {
         if (prec == 0) {
-            if (mode == 0) return inv_t<double2, double2, 0>(a, x, xs, b, y, npart, st, gate, s);
-            return out_prec == 0 ? inv_t<double2, double2, 1>(a, x, xs, b, y, npart, st, gate, s)
-                                 : inv_t<double2, float2, 1>(a, x, xs, b, y, npart, st, gate, s);
+            if (mode == 0) return inv_t<double2, double2, 0>(a, x, xs, b, y, npart, st, gate, s, sh);
+            return out_prec == 0 ? inv_t<double2, double2, 1>(a, x, xs, b, y, npart, st, gate, s, sh)
+                                 : inv_t<double2, float2, 1>(a, x, xs, b, y, npart, st, gate, s, sh);
         }
-        if (mode == 0) return inv_t<float2, float2, 0>(a, x, xs, b, y, npart, st, gate, s);
-        return inv_t<float2, float2, 1>(a, x, xs, b, y, npart, st, gate, s);
+        if (mode == 0) return inv_t<float2, float2, 0>(a, x, xs, b, y, npart, st, gate, s, sh);
+        return inv_t<float2, float2, 1>(a, x, xs, b, y, npart, st, gate, s, sh);
     }
     static int rpc() { return RowCfg<L, SH>::RPC; }
 };
@@ -758,8 +760,8 @@ template <typename PS> struct ColsF {
 };
 template <typename PS> struct InvF {
     static int run(int prec, int mode, int out_prec, const MatvecArgs *a, VecSel x, const double *xs, const void *b,
-                   VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s) {
-        return PS::inv(prec, mode, out_prec, *a, x, xs, b, y, npart, st, gate, s);
+                   VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s, double2 sh) {
+        return PS::inv(prec, mode, out_prec, *a, x, xs, b, y, npart, st, gate, s, sh);
     }
 };
 template <typename PS> struct RpcF {
@@ -786,8 +788,9 @@ int launch_cols_convolve(int prec, const MatvecArgs &a, const DevState *st, int 
 }
 
 int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xs,
-                        const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s) {
-    return dispatch<InvF>(a.vinv, a.L, prec, mode, out_prec, &a, x, xs, b, y, npart, st, gate, s);
+                        const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s,
+                        double2 shift) {
+    return dispatch<InvF>(a.vinv, a.L, prec, mode, out_prec, &a, x, xs, b, y, npart, st, gate, s, shift);
 }
 
 template <int L> static int fft2d_full_t(double2 *A, const double2 *tw, cudaStream_t s) {

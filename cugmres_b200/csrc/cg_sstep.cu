@@ -1,0 +1,661 @@
+// s-step (communication-avoiding) Arnoldi for GMRES.
+//
+// The delayed CGS2 step (cg_dcgs2.cu) reads the basis twice per Arnoldi step,
+// which is most of a step's bytes at restart 100 (the dot and axpy passes run
+// at the HBM roofline).  Here S steps are taken at once (Hoemmen, "Communication-
+// avoiding Krylov subspace methods", PhD thesis, UC Berkeley 2010, ch. 3):
+//
+//   1. matrix powers: S matvecs build a Newton basis from the last orthonormal
+//      vector q_k,  w_1 = (A - th_0) q_k,  w_{i+1} = (A - th_i) w_i,  into V[k+1..k+S]
+//      (the shift is fused into the inverse row pass of each matvec);
+//   2. block Gram-Schmidt with the Pythagorean Cholesky (BCGS-PIP, Barlow,
+//      SIAM J. Matrix Anal. Appl. 40 (2019); Carson, Lund, Rozloznik, SIAM J.
+//      Matrix Anal. Appl. 42 (2021)), twice: one pass computes C = Q^H W and the
+//      Gram matrix G = W^H W together, a one-block kernel factors
+//      G - C^H C = R^H R, one pass writes W <- (W - Q C) R^-1.  Four passes
+//      over the basis per S steps instead of 2 S;
+//   3. the S new Hessenberg columns follow from the change of basis:
+//      A [q_k, Q_new(0:S-1)] = (R_all T - [H_old C''; 0]) Rhat^-1, with T the
+//      (S+1) x S bidiagonal of the shifts, R_all the block's coefficients on
+//      the whole basis, C'' their part on q_0..q_{k-1}; then the Givens
+//      rotations, residual estimates and stop decisions of those S columns.
+//
+// The shifts are the Leja-ordered Ritz values of the first restart cycle, which
+// runs the delayed CGS2 step (cg_api.cu).  A block whose Cholesky fails (the
+// Newton basis lost rank numerically) ends the cycle at the columns already
+// finished, so the solve restarts from the true residual instead of breaking.
+// Numbers, layout and reductions follow the rest of the library: the basis is
+// q_j normalised at V + j n, FP64 (or FP32 in mixed precision) complex,
+// reductions in fixed order (two-level over blocks, as cg_dcgs2.cu).
+#include "cg_common.cuh"
+#include "cg_internal.h"
+
+namespace cg {
+
+static constexpr int SS_THREADS = 256;
+static constexpr int SS_WARPS = SS_THREADS / 32;
+static constexpr int SS_CHUNK = 64;  // basis vectors per shared-memory chunk
+
+// offsets (in double2) of the s-step scratch arrays in kp.ss; M1 = mcap + 1
+struct SsLayout {
+    long long C, Ct, Bc, G, Rt, Ai, Th, Mh, end;
+    __host__ __device__ explicit SsLayout(int mcap) {
+        const long long M1 = mcap + 1;
+        C = 0;
+        Ct = C + M1 * SS_MAX;
+        Bc = Ct + M1 * SS_MAX;
+        G = Bc + M1 * SS_MAX;
+        Rt = G + SS_MAX * SS_MAX;
+        Ai = Rt + SS_MAX * SS_MAX;
+        Th = Ai + SS_MAX * SS_MAX;
+        Mh = Th + SS_MAX;                        // [(mcap + SS_MAX + 1) * SS_MAX] work rows of k_ss_hess
+        end = Mh + (M1 + SS_MAX) * SS_MAX;
+    }
+};
+
+long long sstep_scratch_elems(int mcap) { return SsLayout(mcap).end; }
+static __host__ __device__ __forceinline__ int ss_pld(int mcap) { return 2 * SS_MAX * (mcap + 1) + 2 * SS_MAX * SS_MAX; }
+int sstep_part_ld(int mcap) { return ss_pld(mcap); }
+
+static __device__ __forceinline__ bool ss_last_of(unsigned int *ticket, unsigned int count) {
+    __shared__ bool is_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int t = atomicAdd(ticket, 1u);
+        is_last = (t == count - 1);
+        if (is_last) *ticket = 0u;
+    }
+    __syncthreads();
+    if (is_last) __threadfence();
+    return is_last;
+}
+
+// Warp sum of V values (V a power of two, at most 32) by a reduce-scatter
+// butterfly (V - 1 shuffles, then the remaining full-reduction rounds): on
+// return lane L holds the total of value scatter_index<V>(L); fixed order.
+template <int V> __device__ __forceinline__ int scatter_index(int lane) {
+    int idx = 0;
+#pragma unroll
+    for (int off = 16, cnt = V; cnt > 1; off >>= 1, cnt >>= 1) idx = 2 * idx + ((lane & off) ? 1 : 0);
+    return idx;
+}
+template <int V> __device__ __forceinline__ double warp_sum_scatter(double (&v)[V], int lane) {
+    static_assert(V >= 1 && V <= 32 && (V & (V - 1)) == 0, "power of two");
+    int off = 16;
+#pragma unroll
+    for (int cnt = V; cnt > 1; cnt >>= 1, off >>= 1) {
+        const bool upper = (lane & off) != 0;
+#pragma unroll
+        for (int i = 0; i < cnt / 2; i++) {
+            const double send = upper ? v[i] : v[i + cnt / 2];
+            const double keep = upper ? v[i + cnt / 2] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, off);
+        }
+    }
+    double t = v[0];
+    for (; off >= 1; off >>= 1) t += __shfl_xor_sync(0xffffffffu, t, off);
+    return t;
+}
+// lanes that write a scattered total: one per value index
+template <int V> __device__ __forceinline__ bool scatter_writer(int lane) { return (lane & ((32 / V) - 1)) == 0; }
+
+// ------------------------------------------------------------ block dots
+// C[j][i] = <q_j, w_i> (j = 0..k, i < S), G[i][l] = <w_i, w_l>; tile-major:
+// every warp keeps its tile of the S block vectors in registers and streams
+// the basis over it.  Per-block partial rows part[b][2 S (k+1) + 2 S S] are
+// summed in two fixed-order levels (groups of 16 blocks, then the groups).
+template <typename CV, int S, int U>
+__global__ void __launch_bounds__(SS_THREADS) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    typedef typename real_of<CV>::type R;
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int nq = k + 1;
+    const CV *W = V + (long long)(k + 1) * n;
+    const int pld = ss_pld(kp.mcap);
+    extern __shared__ double sacc[];  // [SS_WARPS][SS_CHUNK][2 S], then [SS_WARPS][2 S S]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double *my = sacc + (size_t)warp * SS_CHUNK * 2 * S;
+    double *myg = sacc + (size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)warp * 2 * S * S;
+    const long long TILE = 32LL * U;
+    const long long ntile = (n + TILE - 1) / TILE;
+    const long long nw = (long long)gridDim.x * SS_WARPS;
+    for (int q = lane; q < 2 * S * S; q += 32) myg[q] = 0.0;
+    double *part = kp.part + (size_t)blockIdx.x * pld;
+    bool gram_done = false;
+    for (int jc = 0; jc < nq; jc += SS_CHUNK) {
+        const int nj = nq - jc < SS_CHUNK ? nq - jc : SS_CHUNK;
+        for (int q = lane; q < nj * 2 * S; q += 32) my[q] = 0.0;
+        __syncwarp();
+        for (long long tile = (long long)blockIdx.x * SS_WARPS + warp; tile < ntile; tile += nw) {
+            const long long e0 = tile * TILE + lane;
+            const bool full = tile * TILE + TILE <= n;
+            CV w[S][U];
+#pragma unroll
+            for (int i = 0; i < S; i++)
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    w[i][t] = (full || e < n) ? W[(long long)i * n + e] : czero<CV>();
+                }
+            if (!gram_done) {
+                // Gram matrix of the block from the registers (upper triangle, once per tile)
+#pragma unroll
+                for (int i = 0; i < S; i++)
+#pragma unroll
+                    for (int l = i; l < S; l++) {
+                        R gr = 0, gi = 0;
+#pragma unroll
+                        for (int t = 0; t < U; t++) {
+                            gr += w[i][t].x * w[l][t].x + w[i][t].y * w[l][t].y;
+                            gi += w[i][t].x * w[l][t].y - w[i][t].y * w[l][t].x;
+                        }
+                        const double sr = warp_sum((double)gr), si = warp_sum((double)gi);
+                        if (lane == 0) {
+                            myg[2 * (i * S + l)] += sr;
+                            myg[2 * (i * S + l) + 1] += si;
+                        }
+                    }
+            }
+            for (int j = 0; j < nj; j++) {
+                const CV *qj = V + (long long)(jc + j) * n;
+                CV a[U];
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    a[t] = (full || e < n) ? __ldcs(qj + e) : czero<CV>();
+                }
+                double d[2 * S];
+#pragma unroll
+                for (int i = 0; i < S; i++) {
+                    R sr = 0, si = 0;
+#pragma unroll
+                    for (int t = 0; t < U; t++) {
+                        sr += a[t].x * w[i][t].x + a[t].y * w[i][t].y;
+                        si += a[t].x * w[i][t].y - a[t].y * w[i][t].x;
+                    }
+                    d[2 * i] = (double)sr;
+                    d[2 * i + 1] = (double)si;
+                }
+                const double tot = warp_sum_scatter<2 * S>(d, lane);
+                if (scatter_writer<2 * S>(lane)) my[2 * S * j + scatter_index<2 * S>(lane)] += tot;
+            }
+        }
+        gram_done = true;
+        __syncthreads();
+        for (int q = threadIdx.x; q < nj * 2 * S; q += blockDim.x) {
+            double t = 0.0;
+            for (int wq = 0; wq < SS_WARPS; wq++) t += sacc[(size_t)wq * SS_CHUNK * 2 * S + q];
+            part[2 * S * jc + q] = t;
+        }
+        __syncthreads();
+    }
+    for (int q = threadIdx.x; q < 2 * S * S; q += blockDim.x) {
+        double t = 0.0;
+        for (int wq = 0; wq < SS_WARPS; wq++) t += sacc[(size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)wq * 2 * S * S + q];
+        part[2 * S * nq + q] = t;
+    }
+    // two-level fixed-order sum of the block rows
+    const int nvals = 2 * S * nq + 2 * S * S;
+    const int nb = gridDim.x, ng = (nb + 15) / 16;
+    const int g = blockIdx.x / 16;
+    const int gsz = nb - g * 16 < 16 ? nb - g * 16 : 16;
+    if (!ss_last_of(&kp.tickets[g], (unsigned int)gsz)) return;
+    for (int q = threadIdx.x; q < nvals; q += blockDim.x) {
+        double s = 0.0;
+        for (int b = g * 16; b < g * 16 + gsz; b++) s += __ldcg(kp.part + (size_t)b * pld + q);
+        kp.gpart[(size_t)g * pld + q] = s;
+    }
+    if (!ss_last_of(&st->counter[5], (unsigned int)ng)) return;
+    const SsLayout L(kp.mcap);
+    double *C = reinterpret_cast<double *>(kp.ss + L.C);
+    double *G = reinterpret_cast<double *>(kp.ss + L.G);
+    for (int q = threadIdx.x; q < nvals; q += blockDim.x) {
+        double s = 0.0;
+        for (int gg = 0; gg < ng; gg++) s += __ldcg(kp.gpart + (size_t)gg * pld + q);
+        if (q < 2 * S * nq) {
+            const int j = q / (2 * S), i = (q / 2) % S;
+            C[2 * (j * SS_MAX + i) + (q & 1)] = s;
+        } else {
+            const int r = q - 2 * S * nq;
+            const int i = (r / 2) / S, l = (r / 2) % S;
+            G[2 * (i * SS_MAX + l) + (r & 1)] = s;
+        }
+    }
+}
+
+// ------------------------------------------------------------ Cholesky
+// One block: Gp = G - C^H C (S x S), Gp = R^H R, A = R^-1, B = C R^-1, and the
+// running totals Ct = Ct + C Rt, Rt = R Rt (Rt = I, Ct = 0 before pass 0).
+// A failed factorisation (a pivot not above 1e-26 of the block's scale, or
+// not finite) ends the cycle at the columns already finished.
+template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_chol(KrylovPtrs kp, int pass) {
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int nq = k + 1;
+    const SsLayout L(kp.mcap);
+    const double2 *C = kp.ss + L.C;
+    double2 *Ct = kp.ss + L.Ct;
+    double2 *Bc = kp.ss + L.Bc;
+    const double2 *G = kp.ss + L.G;
+    double2 *Rt = kp.ss + L.Rt;
+    double2 *Ai = kp.ss + L.Ai;
+    __shared__ double2 gp[S][S];
+    __shared__ double2 rr[S][S];
+    __shared__ double2 ai[S][S];
+    __shared__ double2 rt_old[S][S];
+    __shared__ double red[SS_WARPS][2];
+    __shared__ int ok;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // C^H C, one entry per warp round: sum over the nq rows
+    for (int e = 0; e < S * S; e++) {
+        const int i = e / S, l = e % S;
+        if (l < i) continue;
+        double sr = 0.0, si = 0.0;
+        for (int j = tid; j < nq; j += SS_THREADS) {
+            const double2 a = C[j * SS_MAX + i], b = C[j * SS_MAX + l];
+            sr += a.x * b.x + a.y * b.y;
+            si += a.x * b.y - a.y * b.x;
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) red[warp][0] = sr, red[warp][1] = si;
+        __syncthreads();
+        if (tid == 0) {
+            double tr = 0.0, ti = 0.0;
+            for (int w = 0; w < SS_WARPS; w++) tr += red[w][0], ti += red[w][1];
+            const double2 g = G[i * SS_MAX + l];
+            gp[i][l] = make_double2(g.x - tr, g.y - ti);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        for (int i = 0; i < S; i++)
+            for (int l = 0; l < i; l++) gp[i][l] = cconj(gp[l][i]);
+        double scale = 0.0;
+        for (int i = 0; i < S; i++) scale = fmax(scale, G[i * SS_MAX + i].x);
+        int good = isfinite(scale) && scale > 0.0;
+        // Cholesky gp = R^H R (R upper), row by row
+        for (int i = 0; i < S && good; i++) {
+            double d = gp[i][i].x;
+            for (int p = 0; p < i; p++) d -= rr[p][i].x * rr[p][i].x + rr[p][i].y * rr[p][i].y;
+            if (!(d > 1e-26 * scale) || !isfinite(d)) {
+                good = 0;
+                break;
+            }
+            const double rii = sqrt(d);
+            rr[i][i] = make_double2(rii, 0.0);
+            for (int l = i + 1; l < S; l++) {
+                double2 v = gp[i][l];
+                for (int p = 0; p < i; p++) v = csub(v, cmul(cconj(rr[p][i]), rr[p][l]));
+                rr[i][l] = make_double2(v.x / rii, v.y / rii);
+            }
+            for (int l = 0; l < i; l++) rr[i][l] = make_double2(0.0, 0.0);
+        }
+        if (good) {
+            // A = R^-1 (upper), column by column
+            for (int l = 0; l < S; l++) {
+                for (int i = S - 1; i >= 0; i--) {
+                    double2 v = make_double2(i == l ? 1.0 : 0.0, 0.0);
+                    for (int p = i + 1; p < S; p++) v = csub(v, cmul(rr[i][p], ai[p][l]));
+                    const double inv = 1.0 / rr[i][i].x;
+                    ai[i][l] = make_double2(v.x * inv, v.y * inv);
+                }
+            }
+            for (int i = 0; i < S; i++)
+                for (int l = 0; l < S; l++) {
+                    rt_old[i][l] = pass == 0 ? make_double2(i == l ? 1.0 : 0.0, 0.0) : Rt[i * SS_MAX + l];
+                    Ai[i * SS_MAX + l] = ai[i][l];
+                }
+        }
+        ok = good;
+    }
+    __syncthreads();
+    if (!ok) {
+        if (tid == 0) {
+            // end the cycle with the finished columns; none finished: no progress possible
+            if (k == 0) st->brk = 1;
+            st->stop = 1;
+        }
+        return;
+    }
+    // B = C R^-1 and Ct += C Rt_old (rows j = 0..k)
+    for (int e = tid; e < nq * S; e += SS_THREADS) {
+        const int j = e / S, l = e % S;
+        double2 b = make_double2(0.0, 0.0), c = make_double2(0.0, 0.0);
+        for (int i = 0; i < S; i++) {
+            const double2 cji = C[j * SS_MAX + i];
+            b = cadd(b, cmul(cji, ai[i][l]));
+            c = cadd(c, cmul(cji, rt_old[i][l]));
+        }
+        Bc[j * SS_MAX + l] = b;
+        Ct[j * SS_MAX + l] = pass == 0 ? c : cadd(Ct[j * SS_MAX + l], c);
+    }
+    if (tid < S * S) {
+        const int i = tid / S, l = tid % S;
+        double2 v = make_double2(0.0, 0.0);
+        for (int p = 0; p < S; p++) v = cadd(v, cmul(rr[i][p], rt_old[p][l]));
+        Rt[i * SS_MAX + l] = v;
+    }
+}
+
+// ------------------------------------------------------------ update
+// W <- W A - Q B in place (A = R^-1 of the pass, B = C R^-1); tile-major.
+template <typename CV, int S, int U>
+__global__ void __launch_bounds__(SS_THREADS) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    typedef typename real_of<CV>::type R;
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int nq = k + 1;
+    CV *W = V + (long long)(k + 1) * n;
+    const SsLayout L(kp.mcap);
+    __shared__ CV sa[S][S];
+    __shared__ CV sb[SS_CHUNK][S];
+    for (int e = threadIdx.x; e < S * S; e += blockDim.x) {
+        const double2 a = kp.ss[L.Ai + (e / S) * SS_MAX + (e % S)];
+        sa[e / S][e % S] = mk<CV>((R)a.x, (R)a.y);
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const long long TILE = 32LL * U;
+    const long long ntile = (n + TILE - 1) / TILE;
+    const long long nw = (long long)gridDim.x * SS_WARPS;
+    // the coefficient chunks are shared by every tile of the block, so each
+    // tile is visited once per chunk; the partial outputs stay in registers
+    // only within one tile, hence the loop order tile -> chunk with the
+    // chunk reloaded per tile (the coefficients are tiny next to the basis)
+    for (long long tile0 = (long long)blockIdx.x * SS_WARPS; tile0 < ntile; tile0 += nw) {
+        const long long tile = tile0 + warp;
+        const bool live = tile < ntile;
+        const long long e0 = tile * TILE + lane;
+        const bool full = live && tile * TILE + TILE <= n;
+        CV acc[S][U];
+        __syncthreads();
+        if (live) {
+            CV w[S][U];
+#pragma unroll
+            for (int i = 0; i < S; i++)
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    w[i][t] = (full || e < n) ? W[(long long)i * n + e] : czero<CV>();
+                }
+#pragma unroll
+            for (int l = 0; l < S; l++)
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    CV v = czero<CV>();
+#pragma unroll
+                    for (int i = 0; i <= l; i++) v = cadd(v, cmul(w[i][t], sa[i][l]));
+                    acc[l][t] = v;
+                }
+        }
+        for (int jc = 0; jc < nq; jc += SS_CHUNK) {
+            const int nj = nq - jc < SS_CHUNK ? nq - jc : SS_CHUNK;
+            __syncthreads();
+            for (int e = threadIdx.x; e < nj * S; e += blockDim.x) {
+                const double2 b = kp.ss[L.Bc + (long long)(jc + e / S) * SS_MAX + (e % S)];
+                sb[e / S][e % S] = mk<CV>((R)b.x, (R)b.y);
+            }
+            __syncthreads();
+            if (live) {
+                for (int j = 0; j < nj; j++) {
+                    const CV *qj = V + (long long)(jc + j) * n;
+                    CV a[U];
+#pragma unroll
+                    for (int t = 0; t < U; t++) {
+                        const long long e = e0 + 32 * t;
+                        a[t] = (full || e < n) ? __ldcs(qj + e) : czero<CV>();
+                    }
+#pragma unroll
+                    for (int l = 0; l < S; l++) {
+                        const CV b = sb[j][l];
+#pragma unroll
+                        for (int t = 0; t < U; t++) acc[l][t] = csub(acc[l][t], cmul(a[t], b));
+                    }
+                }
+            }
+        }
+        if (live) {
+#pragma unroll
+            for (int l = 0; l < S; l++)
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    if (full || e < n) W[(long long)l * n + e] = acc[l][t];
+                }
+        }
+    }
+}
+
+// ------------------------------------------------------------ Hessenberg + Givens
+// One block: the S new columns k..k+S-1 of H (rows 0..k+S) from the block's
+// coefficients (Ct, Rt), the shifts and the earlier columns of H, then their
+// Givens rotations, residual estimates and the stop decision.
+template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovPtrs kp) {
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int ld = kp.mcap + 1;
+    const SsLayout L(kp.mcap);
+    const double2 *Ct = kp.ss + L.Ct;
+    const double2 *Rt = kp.ss + L.Rt;
+    const double2 *Th = kp.ss + L.Th;
+    const int tid = threadIdx.x;
+    double2 *M = kp.ss + L.Mh;  // [(k + S + 1) * S], row-major (global: long cycles do not fit shared memory)
+    __shared__ double2 rh[S][S];  // Rhat
+    const int nr = k + S + 1;
+    // Rall[r][c], c = 0..S: column 0 = e_k; column c >= 1: Ct(:, c-1) on rows <= k, Rt(:, c-1) below
+    auto rall = [&](int r, int c) -> double2 {
+        if (c == 0) return make_double2(r == k ? 1.0 : 0.0, 0.0);
+        if (r <= k) return Ct[r * SS_MAX + (c - 1)];
+        const int i = r - k - 1;
+        return i <= c - 1 ? Rt[i * SS_MAX + (c - 1)] : make_double2(0.0, 0.0);
+    };
+    // M = Rall T - [H_old C''; 0]
+    for (int e = tid; e < nr * S; e += SS_THREADS) {
+        const int r = e / S, j = e % S;
+        double2 v = cadd(cmul(rall(r, j), Th[j]), rall(r, j + 1));
+        if (r <= k && j >= 1) {
+            double2 h = make_double2(0.0, 0.0);
+            for (int l = (r > 0 ? r - 1 : 0); l < k; l++) h = cadd(h, cmul(kp.Hm[(size_t)r * ld + l], Ct[l * SS_MAX + (j - 1)]));
+            v = csub(v, h);
+        }
+        M[e] = v;
+    }
+    if (tid < S * S) {
+        const int r = tid / S, c = tid % S;
+        rh[r][c] = rall(k + r, c);
+    }
+    __syncthreads();
+    // H_new = M Rhat^-1: per row, forward substitution over the columns
+    for (int r = tid; r < nr; r += SS_THREADS) {
+        double2 hrow[S];
+#pragma unroll
+        for (int c = 0; c < S; c++) {
+            double2 v = M[r * S + c];
+#pragma unroll
+            for (int p = 0; p < c; p++) v = csub(v, cmul(hrow[p], rh[p][c]));
+            const double2 d = rh[c][c];
+            const double dd = d.x * d.x + d.y * d.y;
+            hrow[c] = cscale(cmulc(d, v), 1.0 / dd);  // v / d
+        }
+#pragma unroll
+        for (int c = 0; c < S; c++) M[r * S + c] = hrow[c];
+    }
+    __syncthreads();
+    // columns inside the restart length (a last block may reach past it)
+    const int cols = st->m - k < S ? st->m - k : S;
+    // store the Hessenberg part of the new columns (rows <= k + c + 1)
+    for (int e = tid; e < nr * S; e += SS_THREADS) {
+        const int r = e / S, c = e % S;
+        if (c < cols && r <= k + c + 1) kp.Hm[(size_t)r * ld + (k + c)] = M[e];
+    }
+    // the earlier rotations applied to each new column (one thread per column)
+    if (tid < cols) {
+        const int c = tid;
+        double2 carry = M[0 * S + c];
+        for (int j = 0; j < k; j++) {
+            const double2 cj = kp.cs[j];
+            const double sj = kp.sn[j];
+            const double2 nx = M[(j + 1) * S + c];
+            kp.Rm[(size_t)(k + c) * ld + j] = cadd(cmul(cconj(cj), carry), cscale(nx, sj));
+            carry = csub(cmul(cj, nx), cscale(carry, sj));
+        }
+        M[k * S + c] = carry;
+    }
+    __syncthreads();
+    if (tid != 0) return;
+    // the block's own rotations, column by column
+    int it = st->it, stop = 0, done = 0;
+    for (int c = 0; c < cols && !stop; c++) {
+        const int col = k + c;
+        // rotations k..col-1 (made in this block) on the rest of column col
+        double2 carry = M[k * S + c];
+        for (int j = k; j < col; j++) {
+            const double2 cj = kp.cs[j];
+            const double sj = kp.sn[j];
+            const double2 nx = M[(j + 1) * S + c];
+            kp.Rm[(size_t)col * ld + j] = cadd(cmul(cconj(cj), carry), cscale(nx, sj));
+            carry = csub(cmul(cj, nx), cscale(carry, sj));
+        }
+        // H(col+1, col) = Rt(c, c) / Rhat(c, c) is real and positive by construction
+        const double hk1 = M[(col + 1) * S + c].x;
+        const double rho = hypot(hypot(carry.x, carry.y), hk1);
+        double2 cs;
+        double sn;
+        if (!(rho > 0.0) || !isfinite(rho)) {
+            cs = make_double2(1.0, 0.0);
+            sn = 0.0;
+        } else {
+            cs = make_double2(carry.x / rho, carry.y / rho);
+            sn = hk1 / rho;
+        }
+        kp.Rm[(size_t)col * ld + col] = cadd(cmul(cconj(cs), carry), make_double2(sn * hk1, 0.0));
+        kp.cs[col] = cs;
+        kp.sn[col] = sn;
+        const double2 gk = kp.g[col];
+        kp.g[col + 1] = cscale(gk, -sn);
+        kp.g[col] = cmul(cconj(cs), gk);
+        it++;
+        const double gabs = hypot(gk.x, gk.y) * sn;
+        const double est = gabs / st->nb;
+        st->est = est;
+        kp.hist[it] = est;
+        done = c + 1;
+        if (!isfinite(est)) {
+            st->status = 4;
+            stop = 1;
+        }
+        if (gabs <= st->tol * st->nb || gabs <= st->inner_tol * st->beta0) stop = 1;
+        if (col + 1 >= st->m) stop = 1;
+        if (it >= st->maxit) stop = 1;
+        if (!(hk1 > 1e-300)) stop = 1;  // the Krylov space is invariant: exact in it
+    }
+    st->it = it;
+    st->ncol = k + done;
+    st->k = k + done;
+    st->stop = stop;
+}
+
+// q_0 = r / ||r|| at the start of an s-step cycle (k_cycle_begin leaves r in V_0)
+template <typename CV> __global__ void k_ss_norm0(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+    DevState *st = kp.st;
+    if (st->stop) return;
+    typedef typename real_of<CV>::type R;
+    const R inv = (R)(1.0 / st->beta0);
+    for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x)
+        V[e] = cscale(V[e], inv);
+}
+
+// ------------------------------------------------------------ launchers
+template <typename K> static int ss_smem(K kern, size_t bytes) {
+    if (bytes > 48 * 1024) return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    return 0;
+}
+
+// points per lane of the tile-major passes: the S block vectors of a tile stay
+// in registers (16 complex FP64 values, 32 FP32 ones per lane)
+template <int S> constexpr int ss_u64() { return 16 / S > 1 ? 16 / S : 1; }
+template <int S> constexpr int ss_u32() { return 32 / S > 1 ? 32 / S : 1; }
+static constexpr int SS_U32 = 8;  // tile width used to size the grid
+
+template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int nblk,
+                                      cudaStream_t s) {
+    const size_t smem = sizeof(double) * ((size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)SS_WARPS * 2 * S * S);
+    if (prec == 0) {
+        auto kern = k_ss_dots<double2, S, ss_u64<S>()>;
+        if (int e = ss_smem(kern, smem)) return e;
+        kern<<<nblk, SS_THREADS, smem, s>>>((const double2 *)V, n, kp);
+    } else {
+        auto kern = k_ss_dots<float2, S, ss_u32<S>()>;
+        if (int e = ss_smem(kern, smem)) return e;
+        kern<<<nblk, SS_THREADS, smem, s>>>((const float2 *)V, n, kp);
+    }
+    return (int)cudaGetLastError();
+}
+
+template <int S> static int ss_update_t(int prec, void *V, long long n, const KrylovPtrs &kp, int nblk,
+                                        cudaStream_t s) {
+    if (prec == 0) k_ss_update<double2, S, ss_u64<S>()><<<nblk, SS_THREADS, 0, s>>>((double2 *)V, n, kp);
+    else k_ss_update<float2, S, ss_u32<S>()><<<nblk, SS_THREADS, 0, s>>>((float2 *)V, n, kp);
+    return (int)cudaGetLastError();
+}
+
+template <int S> static int ss_hess_t(const KrylovPtrs &kp, cudaStream_t s) {
+    k_ss_hess<S><<<1, SS_THREADS, 0, s>>>(kp);
+    return (int)cudaGetLastError();
+}
+
+#define SS_DISPATCH(S, CALL)                  \
+    switch (S) {                              \
+        case 2: return CALL(2);               \
+        case 4: return CALL(4);               \
+        case 8: return CALL(8);               \
+        default: return -1;                   \
+    }
+
+int sstep_supported(int S) { return S == 2 || S == 4 || S == 8; }
+
+int sstep_blocks(int sms, long long n) {
+    const long long tiles = (n + 32 * SS_U32 - 1) / (32 * SS_U32);
+    long long g = 2LL * sms;
+    const long long cap = (tiles + SS_WARPS - 1) / SS_WARPS;
+    if (g > cap) g = cap;
+    return (int)(g < 1 ? 1 : g);
+}
+
+int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int nblk, cudaStream_t s) {
+#define CALL(S_) ss_dots_t<S_>(prec, V, n, kp, nblk, s)
+    SS_DISPATCH(S, CALL)
+#undef CALL
+}
+
+int launch_ss_chol(const KrylovPtrs &kp, int S, int pass, cudaStream_t s) {
+#define CALL(S_) (k_ss_chol<S_><<<1, SS_THREADS, 0, s>>>(kp, pass), (int)cudaGetLastError())
+    SS_DISPATCH(S, CALL)
+#undef CALL
+}
+
+int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int nblk, cudaStream_t s) {
+#define CALL(S_) ss_update_t<S_>(prec, V, n, kp, nblk, s)
+    SS_DISPATCH(S, CALL)
+#undef CALL
+}
+
+int launch_ss_hess(const KrylovPtrs &kp, int S, cudaStream_t s) {
+#define CALL(S_) ss_hess_t<S_>(kp, s)
+    SS_DISPATCH(S, CALL)
+#undef CALL
+}
+
+int launch_ss_norm0(int prec, void *V, long long n, const KrylovPtrs &kp, cudaStream_t s) {
+    const int nb = (int)((n + 255) / 256 > 1024 ? 1024 : (n + 255) / 256);
+    if (prec == 0) k_ss_norm0<double2><<<nb, 256, 0, s>>>((double2 *)V, n, kp);
+    else k_ss_norm0<float2><<<nb, 256, 0, s>>>((float2 *)V, n, kp);
+    return (int)cudaGetLastError();
+}
+
+}  // namespace cg

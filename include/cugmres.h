@@ -62,7 +62,10 @@ enum {
 /* Arnoldi orthogonalisation */
 enum {
     CG_ORTHO_DCGS2 = 0, /* classical Gram-Schmidt, reorthogonalisation delayed one step: 2 passes over the basis per step */
-    CG_ORTHO_CGS2 = 1   /* classical Gram-Schmidt with one immediate reorthogonalisation: 4 passes per step            */
+    CG_ORTHO_CGS2 = 1,  /* classical Gram-Schmidt with one immediate reorthogonalisation: 4 passes per step            */
+    CG_ORTHO_SSTEP = 2  /* s-step: opts->sstep Arnoldi steps per block (a Newton basis of sstep matvecs, block
+                           Gram-Schmidt twice with Pythagorean Cholesky): 4 passes over the basis per block; the
+                           first cycle runs CG_ORTHO_DCGS2 and gives the Newton shifts (its Ritz values)        */
 };
 
 /* Green's-function constructions for cugmres_green_block */
@@ -96,7 +99,8 @@ typedef struct {
     int transpose;      /* 1: solve A^T x = b, A^T = I - diag(c) G (the adjoint system of the
                            reference's gradient path, CUDA_GMRES/GMRES.cuh:97-111; the adjoint
                            A^H x = b is conj of the A^T solve with conj(b))                    */
-    int reserved[4];
+    int sstep;          /* CG_ORTHO_SSTEP: steps per block, 2, 4 or 8 (0: 4); restart >= sstep      */
+    int reserved[3];
 } cg_opts;
 
 /* right preconditioning */
