@@ -106,7 +106,7 @@ template <int V> __device__ __forceinline__ bool scatter_writer(int lane) { retu
 // the basis over it.  Per-block partial rows part[b][2 S (k+1) + 2 S S] are
 // summed in two fixed-order levels (groups of 16 blocks, then the groups).
 template <typename CV, int S, int U>
-__global__ void __launch_bounds__(SS_THREADS) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(SS_THREADS, 2) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -158,13 +158,22 @@ __global__ void __launch_bounds__(SS_THREADS) k_ss_dots(const CV *__restrict__ V
                         }
                     }
             }
-            for (int j = 0; j < nj; j++) {
-                const CV *qj = V + (long long)(jc + j) * n;
-                CV a[U];
+            CV a[U];
 #pragma unroll
-                for (int t = 0; t < U; t++) {
-                    const long long e = e0 + 32 * t;
-                    a[t] = (full || e < n) ? __ldcs(qj + e) : czero<CV>();
+            for (int t = 0; t < U; t++) {
+                const long long e = e0 + 32 * t;
+                a[t] = (full || e < n) ? __ldcs(V + (long long)jc * n + e) : czero<CV>();
+            }
+            for (int j = 0; j < nj; j++) {
+                // the next basis vector's tile in flight during this one's products and reduction
+                CV an[U];
+                if (j + 1 < nj) {
+                    const CV *qn = V + (long long)(jc + j + 1) * n;
+#pragma unroll
+                    for (int t = 0; t < U; t++) {
+                        const long long e = e0 + 32 * t;
+                        an[t] = (full || e < n) ? __ldcs(qn + e) : czero<CV>();
+                    }
                 }
                 double d[2 * S];
 #pragma unroll
@@ -180,6 +189,10 @@ __global__ void __launch_bounds__(SS_THREADS) k_ss_dots(const CV *__restrict__ V
                 }
                 const double tot = warp_sum_scatter<2 * S>(d, lane);
                 if (scatter_writer<2 * S>(lane)) my[2 * S * j + scatter_index<2 * S>(lane)] += tot;
+                if (j + 1 < nj) {
+#pragma unroll
+                    for (int t = 0; t < U; t++) a[t] = an[t];
+                }
             }
         }
         gram_done = true;
@@ -344,7 +357,7 @@ template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_chol(KrylovP
 // ------------------------------------------------------------ update
 // W <- W A - Q B in place (A = R^-1 of the pass, B = C R^-1); tile-major.
 template <typename CV, int S, int U>
-__global__ void __launch_bounds__(SS_THREADS) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -401,19 +414,31 @@ __global__ void __launch_bounds__(SS_THREADS) k_ss_update(CV *__restrict__ V, lo
             }
             __syncthreads();
             if (live) {
-                for (int j = 0; j < nj; j++) {
-                    const CV *qj = V + (long long)(jc + j) * n;
-                    CV a[U];
+                CV a[U];
 #pragma unroll
-                    for (int t = 0; t < U; t++) {
-                        const long long e = e0 + 32 * t;
-                        a[t] = (full || e < n) ? __ldcs(qj + e) : czero<CV>();
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    a[t] = (full || e < n) ? __ldcs(V + (long long)jc * n + e) : czero<CV>();
+                }
+                for (int j = 0; j < nj; j++) {
+                    CV an[U];  // the next basis vector's tile in flight
+                    if (j + 1 < nj) {
+                        const CV *qn = V + (long long)(jc + j + 1) * n;
+#pragma unroll
+                        for (int t = 0; t < U; t++) {
+                            const long long e = e0 + 32 * t;
+                            an[t] = (full || e < n) ? __ldcs(qn + e) : czero<CV>();
+                        }
                     }
 #pragma unroll
                     for (int l = 0; l < S; l++) {
                         const CV b = sb[j][l];
 #pragma unroll
                         for (int t = 0; t < U; t++) acc[l][t] = csub(acc[l][t], cmul(a[t], b));
+                    }
+                    if (j + 1 < nj) {
+#pragma unroll
+                        for (int t = 0; t < U; t++) a[t] = an[t];
                     }
                 }
             }
@@ -577,9 +602,10 @@ template <typename K> static int ss_smem(K kern, size_t bytes) {
 }
 
 // points per lane of the tile-major passes: the S block vectors of a tile stay
-// in registers (16 complex FP64 values, 32 FP32 ones per lane)
-template <int S> constexpr int ss_u64() { return 16 / S > 1 ? 16 / S : 1; }
-template <int S> constexpr int ss_u32() { return 32 / S > 1 ? 32 / S : 1; }
+// in registers (at most 16 complex FP64 values, 32 FP32 ones per lane), and
+// with the next basis tile in flight the kernels fit two blocks per SM
+template <int S> constexpr int ss_u64() { return 16 / S > 4 ? 4 : (16 / S > 1 ? 16 / S : 1); }
+template <int S> constexpr int ss_u32() { return 32 / S > 8 ? 8 : (32 / S > 1 ? 32 / S : 1); }
 static constexpr int SS_U32 = 8;  // tile width used to size the grid
 
 template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int nblk,
