@@ -264,6 +264,16 @@ def side_measurements(args, stream):
     ms, info, _ = timed_solves(s, b, kw, max(1, args.steps), stream)
     out["mixed_capped_solve"] = {"s": ms / 1e3, "steps": info["iterations"], "rel_residual_true": info["rel_residual_true"],
                                  "ms_per_step": ms / max(1, info["iterations"])}
+    # the same capped solve with s-step Arnoldi blocks (after a first delayed-CGS2 cycle for the shifts)
+    for prec in ("fp64", "mixed"):
+        for S in (4, 8):
+            kws = dict(restart=args.restart, max_iter=args.max_iter, tol=args.tol, precision=prec,
+                       inner_tol=args.inner_tol, ortho="sstep", sstep=S)
+            s.solve(b, **kws)
+            ms, info, _ = timed_solves(s, b, kws, max(1, args.steps), stream)
+            out[f"sstep{S}_{prec}_capped_solve"] = {"s": ms / 1e3, "steps": info["iterations"],
+                                                   "rel_residual_true": info["rel_residual_true"],
+                                                   "ms_per_step": ms / max(1, info["iterations"])}
     s.close()
     for N, R, reps in ((256, 2500, 1), (512, 4400, 0)):
         prn = P.helmholtz(N, args.eps, seed=args.seed)

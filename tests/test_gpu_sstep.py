@@ -46,13 +46,14 @@ def test_sstep_fixed_budget_iterates_match_oracle(solver, oracle):
     assert np.allclose(info["res_hist"][1:], o["res_hist"][1:], rtol=1e-7)
 
 
-def test_sstep_matches_dcgs2_on_the_benchmark_system(solver):
+@pytest.mark.parametrize("S", [4, 8])
+def test_sstep_matches_dcgs2_on_the_benchmark_system(solver, S):
     """The 1024^2 system (L = 2048): 300 steps of GMRES(100) by s-step and by
     delayed CGS2 give the same residual history and iterate."""
     pr = P.helmholtz(1024, 4.0, seed=0)
     solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
     xa, ia = solver.solve(pr["b"], restart=100, max_iter=300, tol=0.0, ortho="dcgs2")
-    xb, ib = solver.solve(pr["b"], restart=100, max_iter=300, tol=0.0, ortho="sstep", sstep=4)
+    xb, ib = solver.solve(pr["b"], restart=100, max_iter=300, tol=0.0, ortho="sstep", sstep=S)
     assert ia["iterations"] == ib["iterations"] == 300
     assert np.allclose(ib["res_hist"][1:], ia["res_hist"][1:], rtol=1e-8)
     assert np.linalg.norm(xb - xa) / np.linalg.norm(xa) < 1e-8
