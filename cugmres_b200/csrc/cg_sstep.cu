@@ -35,6 +35,13 @@ namespace cg {
 static constexpr int SS_THREADS = 256;
 static constexpr int SS_WARPS = SS_THREADS / 32;
 static constexpr int SS_CHUNK = 64;  // basis vectors per shared-memory chunk
+// points per lane of the tile-major passes: the S block vectors of a tile stay
+// in registers (at most 32 complex values per lane)
+template <int S> constexpr int ss_u64() { return 32 / S > 8 ? 8 : (32 / S > 1 ? 32 / S : 1); }
+template <int S> constexpr int ss_u32() { return 32 / S > 8 ? 8 : (32 / S > 1 ? 32 / S : 1); }
+// FP64 tiles are 8 points per lane at S = 4 (one block of 8 warps per SM, the
+// next basis tile in flight); FP32 ones fit two blocks per SM
+template <typename CV> constexpr int ss_minb() { return sizeof(CV) == 16 ? 1 : 2; }
 
 // offsets (in double2) of the s-step scratch arrays in kp.ss; M1 = mcap + 1
 struct SsLayout {
@@ -106,7 +113,7 @@ template <int V> __device__ __forceinline__ bool scatter_writer(int lane) { retu
 // the basis over it.  Per-block partial rows part[b][2 S (k+1) + 2 S S] are
 // summed in two fixed-order levels (groups of 16 blocks, then the groups).
 template <typename CV, int S, int U>
-__global__ void __launch_bounds__(SS_THREADS, 2) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -357,7 +364,7 @@ template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_chol(KrylovP
 // ------------------------------------------------------------ update
 // W <- W A - Q B in place (A = R^-1 of the pass, B = C R^-1); tile-major.
 template <typename CV, int S, int U>
-__global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -601,11 +608,6 @@ template <typename K> static int ss_smem(K kern, size_t bytes) {
     return 0;
 }
 
-// points per lane of the tile-major passes: the S block vectors of a tile stay
-// in registers (at most 16 complex FP64 values, 32 FP32 ones per lane), and
-// with the next basis tile in flight the kernels fit two blocks per SM
-template <int S> constexpr int ss_u64() { return 16 / S > 4 ? 4 : (16 / S > 1 ? 16 / S : 1); }
-template <int S> constexpr int ss_u32() { return 32 / S > 8 ? 8 : (32 / S > 1 ? 32 / S : 1); }
 static constexpr int SS_U32 = 8;  // tile width used to size the grid
 
 template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int nblk,
