@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--tol", type=float, default=1e-10)
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--ortho", default="sstep", choices=["sstep", "dcgs2", "cgs2"],
+                    help="Arnoldi scheme of the timed solve (s-step blocks after a first delayed-CGS2 cycle)")
+    ap.add_argument("--sstep", type=int, default=4, help="steps per s-step block")
     ap.add_argument("--inner-tol", type=float, default=1e-5, help="mixed: a complex64 cycle ends when its estimate fell by this")
     ap.add_argument("--profile-case", action="store_true", help="fixed launch sequence for profiler captures")
     ap.add_argument("--case-steps", type=int, default=60)
@@ -145,7 +148,9 @@ def make_problem(args):
 def workload(args):
     return {"workload": f"helmholtz-gfiem {args.N}x{args.N} eps_r={args.eps:g} seed={args.seed} "
                         f"restart={args.restart} tol={args.tol:g} max_iter={args.max_iter} x0=0 "
-                        f"precision={args.precision}",
+                        f"precision={args.precision} ortho={args.ortho}"
+                        + (f" sstep={args.sstep}" if args.ortho == "sstep" else ""),
+            "ortho": args.ortho, "sstep": args.sstep if args.ortho == "sstep" else None,
             "max_iter": args.max_iter,
             "N": args.N, "unknowns": args.N * args.N, "eps_r": args.eps, "lambda_over_h": 20,
             "restart": args.restart, "tol": args.tol, "precision": args.precision,
@@ -259,21 +264,23 @@ def side_measurements(args, stream):
     s.set_stream(stream.cuda_stream)
     s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
     b = torch.from_numpy(pr["b"]).cuda()
-    kw = dict(restart=args.restart, max_iter=args.max_iter, tol=args.tol, precision="mixed", inner_tol=args.inner_tol)
+    kw = dict(restart=args.restart, max_iter=args.max_iter, tol=args.tol, precision="mixed", inner_tol=args.inner_tol,
+              ortho=args.ortho, sstep=args.sstep)
     s.solve(b, **kw)
     ms, info, _ = timed_solves(s, b, kw, max(1, args.steps), stream)
     out["mixed_capped_solve"] = {"s": ms / 1e3, "steps": info["iterations"], "rel_residual_true": info["rel_residual_true"],
                                  "ms_per_step": ms / max(1, info["iterations"])}
-    # the same capped solve with s-step Arnoldi blocks (after a first delayed-CGS2 cycle for the shifts)
+    # the same capped solve with the other Arnoldi schemes: delayed CGS2 (two passes over the
+    # basis per step) and s-step blocks of 8
     for prec in ("fp64", "mixed"):
-        for S in (4, 8):
+        for name, extra in (("dcgs2", dict(ortho="dcgs2")), ("sstep8", dict(ortho="sstep", sstep=8))):
             kws = dict(restart=args.restart, max_iter=args.max_iter, tol=args.tol, precision=prec,
-                       inner_tol=args.inner_tol, ortho="sstep", sstep=S)
+                       inner_tol=args.inner_tol, **extra)
             s.solve(b, **kws)
             ms, info, _ = timed_solves(s, b, kws, max(1, args.steps), stream)
-            out[f"sstep{S}_{prec}_capped_solve"] = {"s": ms / 1e3, "steps": info["iterations"],
-                                                   "rel_residual_true": info["rel_residual_true"],
-                                                   "ms_per_step": ms / max(1, info["iterations"])}
+            out[f"{name}_{prec}_capped_solve"] = {"s": ms / 1e3, "steps": info["iterations"],
+                                                 "rel_residual_true": info["rel_residual_true"],
+                                                 "ms_per_step": ms / max(1, info["iterations"])}
     s.close()
     for N, R, reps in ((256, 2500, 1), (512, 4400, 0)):
         prn = P.helmholtz(N, args.eps, seed=args.seed)
@@ -473,7 +480,7 @@ def main():
     s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
     b_dev = torch.from_numpy(pr["b"]).cuda()
     kw = dict(restart=args.restart, max_iter=args.max_iter, tol=args.tol, precision=args.precision,
-              inner_tol=args.inner_tol)
+              inner_tol=args.inner_tol, ortho=args.ortho, sstep=args.sstep)
 
     for _ in range(args.warmup):
         x, info = s.solve(b_dev, **kw)
@@ -524,15 +531,20 @@ def main():
     # from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the launch at step k = 30
     # of this 1024^2 FP64 solve (bench.py --profile-case), as a ratio to that launch's algorithmic
     # bytes, applied to this run's mean algorithmic bytes per launch; "traffic_source" says so
-    ncu_ratio = {"dots": (536.904 + 4.625) / 536.871, "axpy": (536.961 + 8.369) / 570.425}
+    if args.ortho == "sstep":
+        # k_ss_dots / k_ss_update at k = 20 of a 1024^2 FP64 GMRES(100) s-step cycle (S = 4)
+        ncu_ratio = {"dots": (419.580 + 7.655) / 419.430, "axpy": (419.450 + 13.256) / 486.539}
+    else:
+        ncu_ratio = {"dots": (536.904 + 4.625) / 536.871, "axpy": (536.961 + 8.369) / 570.425}
     launches = max(1, dom[1].get("launches", 0))
     alg_per_launch = dom[1].get("bytes", 0.0) / launches
     traffic = ncu_ratio[dom[0]] * alg_per_launch if dom[0] in ncu_ratio and alg_per_launch > 0 else None
     roof = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1]["gbs"], 1), "peak": hbm, "unit": "GB/s",
             "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind,
             "traffic": round(traffic) if traffic else None, "traffic_unit": "bytes/launch",
-            "traffic_source": ("ncu capture of the same kernel at step 30 of this solve (--profile-case), its "
-                               "DRAM bytes / algorithmic bytes ratio applied to this run's mean launch"),
+            "traffic_source": ("ncu capture of the same kernel of this solve (delayed CGS2: step 30, s-step: the "
+                               "block at k = 20), its DRAM bytes / algorithmic bytes ratio applied to this "
+                               "run's mean launch"),
             "algorithmic_bytes_per_launch": round(alg_per_launch),
             "phases": {k: {"share": round(v["ms"] / tot_ms, 4), "gbs": round(v["gbs"], 1),
                            "ms": round(v["ms"], 3)} for k, v in phases.items()}}
@@ -553,11 +565,17 @@ def main():
             "e2e": {"value": e2e_wall, "unit": "s", "h2d_bytes_per_step": int(pr["b"].nbytes),
                     "d2h_bytes_per_step": int(pr["b"].nbytes)},
             "gpu_launches": None, "clocks": clk}
-    # our kernels per solve (delayed CGS2, one CUDA-graph replay per cycle): 6 per Arnoldi step
-    # (3 matvec passes, dots, step, axpy) for restart+1 steps per cycle (steps after the device stops
-    # the cycle return at once), back-solve, update, 3 residual passes and the cycle set-up per cycle,
-    # plus the norm of b, the first residual and cycle set-up
-    line["gpu_launches"] = int(args.steps * (last["cycles"] * (6 * (args.restart + 1) + 6) + 5))
+    # our kernels per solve, counted from the enqueued sequence (launches after the device stops a
+    # cycle return at once): the norm of b, the first residual (3 passes) and cycle set-up; per
+    # delayed-CGS2 cycle 6 per step (3 matvec passes, dots, step, axpy) for restart+1 steps, then
+    # back-solve, update, 3 residual passes and the cycle set-up; an s-step cycle instead runs q_0's
+    # normalisation, per block of S steps 3 S matvec passes, 2 x (dots, Cholesky, update) and the
+    # Hessenberg/Givens kernel, then the same 6
+    per_dcgs2 = 6 * (args.restart + 1) + 6
+    per_ss = 1 + -(-args.restart // args.sstep) * (3 * args.sstep + 7) + 6
+    cyc = last["cycles"]
+    per_solve = 5 + (per_dcgs2 + (cyc - 1) * per_ss if args.ortho == "sstep" else cyc * per_dcgs2)
+    line["gpu_launches"] = int(args.steps * per_solve)
     if rank == 0 and world == 1 and not args.no_extras:
         line["side"] = side_measurements(args, stream)
         if not args.no_learned:

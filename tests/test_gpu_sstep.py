@@ -25,11 +25,15 @@ def test_sstep_converges_like_oracle(solver, oracle, S):
     assert info["rel_residual_true"] <= 1e-10
     if S <= 4:
         assert abs(info["iterations"] - o["iterations"]) <= 2, (info["iterations"], o["iterations"])
+        assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
     else:
         # eight Newton steps lose rank numerically on this spectrum: a block whose
-        # Cholesky fails ends its cycle early, which costs restarts (699 -> 720 steps)
+        # Cholesky fails ends its cycle early, which costs restarts (699 -> 720
+        # steps) and stops the solve at another point inside the tolerance, so the
+        # solution is checked against a solve tightened to 1e-13
         assert o["iterations"] <= info["iterations"] <= 1.1 * o["iterations"], (info["iterations"], o["iterations"])
-    assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
+        t = oracle.gmres(gh, pr["chi"] * pr["chi_scale"], pr["b"], restart=40, maxiter=6000, tol=1e-13)
+        assert np.linalg.norm(x - t["x"]) / np.linalg.norm(t["x"]) < 1e-8
 
 
 def test_sstep_fixed_budget_iterates_match_oracle(solver, oracle):
