@@ -32,9 +32,12 @@ budget-capped solve (max_iter / restart).  Warm-up steps run a 5-step sample.
 
 --profile-case: a fixed launch sequence for profiler captures (no timing, no
 JSON): three FP64 and three FP32 matvecs of the 1024^2 system, then one solve of
-exactly --case-steps Arnoldi steps (tolerance 1e-14, so it never stops early):
+exactly --case-steps Arnoldi steps (tolerance 1e-14, so it never stops early) in
+cycles of min(--restart, --case-steps) steps.  Its first cycle is delayed CGS2:
 per step [k_rows_forward, k_cols_convolve, k_rows_inverse, k_dots2, k_dcgs2_step,
-k_axpy2]; `ncu -k regex:k_dots2 -s 30 -c 1` then picks the dot pass of step 30.
+k_axpy2], so `ncu -k regex:k_dots2 -s 30 -c 1` picks the dot pass of step 30; with
+--case-steps 200 the second cycle runs s-step blocks (--sstep), whose passes are
+k_ss_dots and k_ss_update.
 """
 import argparse
 import json
@@ -449,8 +452,8 @@ def profile_case(args):
     x32 = x.astype(np.complex64)
     for _ in range(3):
         s.matvec(x32, precision="fp32")
-    _, info = s.solve(pr["b"], restart=args.case_steps, max_iter=args.case_steps, tol=1e-14,
-                      precision=args.precision)
+    _, info = s.solve(pr["b"], restart=min(args.restart, args.case_steps), max_iter=args.case_steps, tol=1e-14,
+                      precision=args.precision, ortho=args.ortho, sstep=args.sstep)
     s.close()
     print("ok", info["iterations"], info["status_text"], flush=True)
 
