@@ -39,8 +39,11 @@ static constexpr int SS_CHUNK = 64;  // basis vectors per shared-memory chunk
 // in registers (at most 32 complex values per lane)
 template <int S> constexpr int ss_u64() { return 32 / S > 8 ? 8 : (32 / S > 1 ? 32 / S : 1); }
 template <int S> constexpr int ss_u32() { return 32 / S > 8 ? 8 : (32 / S > 1 ? 32 / S : 1); }
-// FP64 tiles are 8 points per lane at S = 4 (one block of 8 warps per SM, the
-// next basis tile in flight); FP32 ones fit two blocks per SM
+// the update pass keeps S x U accumulators next to the basis tiles: 4 FP64
+// points per lane at S = 4 so that two blocks fit per SM (measured faster than
+// 8 points with one block: 5.3 against 4.8 TB/s), while the dot pass is faster
+// with 8 points and one block of 8 warps (4.9 against 4.0 TB/s)
+template <int S> constexpr int ss_u64_upd() { return 16 / S > 4 ? 4 : (16 / S > 1 ? 16 / S : 1); }
 template <typename CV> constexpr int ss_minb() { return sizeof(CV) == 16 ? 1 : 2; }
 
 // offsets (in double2) of the s-step scratch arrays in kp.ss; M1 = mcap + 1
@@ -364,7 +367,7 @@ template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_chol(KrylovP
 // ------------------------------------------------------------ update
 // W <- W A - Q B in place (A = R^-1 of the pass, B = C R^-1); tile-major.
 template <typename CV, int S, int U>
-__global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -391,26 +394,32 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_update(CV *__r
         const bool live = tile < ntile;
         const long long e0 = tile * TILE + lane;
         const bool full = live && tile * TILE + TILE <= n;
+        // FP64: -Q B first, W A last, so the block vectors (read one at a time at
+        // the end) are never live next to the accumulators and the basis tiles;
+        // FP32 (twice the points per lane fit): W A first, then -Q B
+        constexpr bool WA_LAST = sizeof(CV) == 16;
         CV acc[S][U];
-        __syncthreads();
-        if (live) {
-            CV w[S][U];
 #pragma unroll
-            for (int i = 0; i < S; i++)
+        for (int l = 0; l < S; l++)
+#pragma unroll
+            for (int t = 0; t < U; t++) acc[l][t] = czero<CV>();
+        // the coefficients in sa are written before the first tile: a barrier
+        // before W A is read (the chunk loop below has its own for W A last)
+        if (!WA_LAST) __syncthreads();
+        if (!WA_LAST && live) {
+#pragma unroll
+            for (int i = 0; i < S; i++) {
+                CV w[U];
 #pragma unroll
                 for (int t = 0; t < U; t++) {
                     const long long e = e0 + 32 * t;
-                    w[i][t] = (full || e < n) ? W[(long long)i * n + e] : czero<CV>();
+                    w[t] = (full || e < n) ? W[(long long)i * n + e] : czero<CV>();
                 }
 #pragma unroll
-            for (int l = 0; l < S; l++)
+                for (int l = i; l < S; l++)
 #pragma unroll
-                for (int t = 0; t < U; t++) {
-                    CV v = czero<CV>();
-#pragma unroll
-                    for (int i = 0; i <= l; i++) v = cadd(v, cmul(w[i][t], sa[i][l]));
-                    acc[l][t] = v;
-                }
+                    for (int t = 0; t < U; t++) acc[l][t] = cadd(acc[l][t], cmul(w[t], sa[i][l]));
+            }
         }
         for (int jc = 0; jc < nq; jc += SS_CHUNK) {
             const int nj = nq - jc < SS_CHUNK ? nq - jc : SS_CHUNK;
@@ -450,7 +459,23 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_update(CV *__r
                 }
             }
         }
+        if (WA_LAST && live) {
+#pragma unroll
+            for (int i = 0; i < S; i++) {
+                CV w[U];
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    w[t] = (full || e < n) ? W[(long long)i * n + e] : czero<CV>();
+                }
+#pragma unroll
+                for (int l = i; l < S; l++)
+#pragma unroll
+                    for (int t = 0; t < U; t++) acc[l][t] = cadd(acc[l][t], cmul(w[t], sa[i][l]));
+            }
+        }
         if (live) {
+            __syncwarp();
 #pragma unroll
             for (int l = 0; l < S; l++)
 #pragma unroll
@@ -627,7 +652,7 @@ template <int S> static int ss_dots_t(int prec, const void *V, long long n, cons
 
 template <int S> static int ss_update_t(int prec, void *V, long long n, const KrylovPtrs &kp, int nblk,
                                         cudaStream_t s) {
-    if (prec == 0) k_ss_update<double2, S, ss_u64<S>()><<<nblk, SS_THREADS, 0, s>>>((double2 *)V, n, kp);
+    if (prec == 0) k_ss_update<double2, S, ss_u64_upd<S>()><<<nblk, SS_THREADS, 0, s>>>((double2 *)V, n, kp);
     else k_ss_update<float2, S, ss_u32<S>()><<<nblk, SS_THREADS, 0, s>>>((float2 *)V, n, kp);
     return (int)cudaGetLastError();
 }
