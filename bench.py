@@ -117,6 +117,13 @@ class Clocks:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
+    def wait_first(self, timeout=5.0):
+        """Block until the sampler printed its first line, so that nvidia-smi's
+        start-up (NVML initialisation) lies before the timed region."""
+        t_end = time.perf_counter() + timeout
+        while self.proc is not None and not self.lines and time.perf_counter() < t_end:
+            time.sleep(0.02)
+
     def stop(self):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -491,6 +498,7 @@ def main():
 
     clocks = Clocks(local)
     clocks.start()
+    clocks.wait_first()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()

@@ -37,6 +37,20 @@ template <typename C> __host__ __device__ __forceinline__ C cmulc(C a, C b) {
     return mk<C>(a.x * b.x + a.y * b.y, a.x * b.y - a.y * b.x);
 }
 template <typename C> __host__ __device__ __forceinline__ C cconj(C a) { return mk<C>(a.x, -a.y); }
+
+// Multiply-accumulate with every real product fused into its addition: four
+// FMAs per complex value (a + b * c written out as products and sums compiles
+// to a multiply, an FMA and an add per component).
+__device__ __forceinline__ double fma_r(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float fma_r(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+// acc + a * b
+template <typename C> __device__ __forceinline__ C cfma(C acc, C a, C b) {
+    return mk<C>(fma_r(-a.y, b.y, fma_r(a.x, b.x, acc.x)), fma_r(a.y, b.x, fma_r(a.x, b.y, acc.y)));
+}
+// acc - a * b
+template <typename C> __device__ __forceinline__ C cfms(C acc, C a, C b) {
+    return mk<C>(fma_r(a.y, b.y, fma_r(-a.x, b.x, acc.x)), fma_r(-a.y, b.x, fma_r(-a.x, b.y, acc.y)));
+}
 template <typename C>
 __host__ __device__ __forceinline__ C cscale(C a, typename real_of<C>::type s) { return mk<C>(a.x * s, a.y * s); }
 template <typename C> __host__ __device__ __forceinline__ typename real_of<C>::type cnorm2(C a) {

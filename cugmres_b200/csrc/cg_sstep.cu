@@ -158,8 +158,8 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
                         R gr = 0, gi = 0;
 #pragma unroll
                         for (int t = 0; t < U; t++) {
-                            gr += w[i][t].x * w[l][t].x + w[i][t].y * w[l][t].y;
-                            gi += w[i][t].x * w[l][t].y - w[i][t].y * w[l][t].x;
+                            gr = fma_r(w[i][t].y, w[l][t].y, fma_r(w[i][t].x, w[l][t].x, gr));
+                            gi = fma_r(-w[i][t].y, w[l][t].x, fma_r(w[i][t].x, w[l][t].y, gi));
                         }
                         const double sr = warp_sum((double)gr), si = warp_sum((double)gi);
                         if (lane == 0) {
@@ -191,8 +191,9 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
                     R sr = 0, si = 0;
 #pragma unroll
                     for (int t = 0; t < U; t++) {
-                        sr += a[t].x * w[i][t].x + a[t].y * w[i][t].y;
-                        si += a[t].x * w[i][t].y - a[t].y * w[i][t].x;
+                        // conj(q) w, four FMAs per point
+                        sr = fma_r(a[t].y, w[i][t].y, fma_r(a[t].x, w[i][t].x, sr));
+                        si = fma_r(-a[t].y, w[i][t].x, fma_r(a[t].x, w[i][t].y, si));
                     }
                     d[2 * i] = (double)sr;
                     d[2 * i + 1] = (double)si;
@@ -418,7 +419,7 @@ __global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V,
 #pragma unroll
                 for (int l = i; l < S; l++)
 #pragma unroll
-                    for (int t = 0; t < U; t++) acc[l][t] = cadd(acc[l][t], cmul(w[t], sa[i][l]));
+                    for (int t = 0; t < U; t++) acc[l][t] = cfma(acc[l][t], w[t], sa[i][l]);
             }
         }
         for (int jc = 0; jc < nq; jc += SS_CHUNK) {
@@ -450,7 +451,7 @@ __global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V,
                     for (int l = 0; l < S; l++) {
                         const CV b = sb[j][l];
 #pragma unroll
-                        for (int t = 0; t < U; t++) acc[l][t] = csub(acc[l][t], cmul(a[t], b));
+                        for (int t = 0; t < U; t++) acc[l][t] = cfms(acc[l][t], a[t], b);
                     }
                     if (j + 1 < nj) {
 #pragma unroll
@@ -471,7 +472,7 @@ __global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V,
 #pragma unroll
                 for (int l = i; l < S; l++)
 #pragma unroll
-                    for (int t = 0; t < U; t++) acc[l][t] = cadd(acc[l][t], cmul(w[t], sa[i][l]));
+                    for (int t = 0; t < U; t++) acc[l][t] = cfma(acc[l][t], w[t], sa[i][l]);
             }
         }
         if (live) {
