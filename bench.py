@@ -540,11 +540,14 @@ def main():
     tot_ms = sum(v["ms"] for v in phases.values())
     # DRAM traffic per launch of the dominant kernel is not measurable without a profiler: it is taken
     # from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the launch at step k = 30
-    # of this 1024^2 FP64 solve (bench.py --profile-case), as a ratio to that launch's algorithmic
-    # bytes, applied to this run's mean algorithmic bytes per launch; "traffic_source" says so
+    # (delayed CGS2) or of the block at k = 48 (s-step) of this 1024^2 FP64 solve (bench.py
+    # --profile-case), as a ratio to that launch's algorithmic bytes, applied to this run's mean
+    # algorithmic bytes per launch; "traffic_source" says so
     if args.ortho == "sstep":
-        # k_ss_dots / k_ss_update at k = 20 of a 1024^2 FP64 GMRES(100) s-step cycle (S = 4)
-        ncu_ratio = {"dots": (419.580 + 7.655) / 419.430, "axpy": (419.450 + 13.256) / 486.539}
+        # k_ss_dots / k_ss_update of the block at k = 48 of a 1024^2 FP64 GMRES(100) s-step cycle (S = 4):
+        # 53 vectors read (889.19 MB); the update also writes the 4 block vectors (956.30 MB in all),
+        # which are still in L2 when the kernel ends
+        ncu_ratio = {"dots": (889.266 + 3.859) / 889.192, "axpy": (889.219 + 16.487) / 956.301}
     else:
         ncu_ratio = {"dots": (536.904 + 4.625) / 536.871, "axpy": (536.961 + 8.369) / 570.425}
     launches = max(1, dom[1].get("launches", 0))
@@ -554,7 +557,7 @@ def main():
             "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind,
             "traffic": round(traffic) if traffic else None, "traffic_unit": "bytes/launch",
             "traffic_source": ("ncu capture of the same kernel of this solve (delayed CGS2: step 30, s-step: the "
-                               "block at k = 20), its DRAM bytes / algorithmic bytes ratio applied to this "
+                               "block at k = 48), its DRAM bytes / algorithmic bytes ratio applied to this "
                                "run's mean launch"),
             "algorithmic_bytes_per_launch": round(alg_per_launch),
             "phases": {k: {"share": round(v["ms"] / tot_ms, 4), "gbs": round(v["gbs"], 1),
