@@ -1230,10 +1230,9 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             }
             CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, b * S, q));
             for (int pass = 0; pass < 2; pass++) {
-                CG_LAUNCH(launch_ss_dots(prec, c->V, n, kp, S, nss, q));
+                // the dot pass's last block also runs the pass's Cholesky
+                CG_LAUNCH(launch_ss_dots(prec, c->V, n, kp, S, nss, pass, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, b * S, q));
-                CG_LAUNCH(launch_ss_chol(kp, S, pass, q));
-                CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, b * S, q));
                 CG_LAUNCH(launch_ss_update(prec, c->V, n, kp, S, nss, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, b * S, q));
             }

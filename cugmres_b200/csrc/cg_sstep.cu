@@ -110,13 +110,130 @@ template <int V> __device__ __forceinline__ double warp_sum_scatter(double (&v)[
 // lanes that write a scattered total: one per value index
 template <int V> __device__ __forceinline__ bool scatter_writer(int lane) { return (lane & ((32 / V) - 1)) == 0; }
 
+// ------------------------------------------------------------ Cholesky
+// One block of SS_THREADS threads (the last block of the dot pass, once C and
+// G are summed): Gp = G - C^H C (S x S), Gp = R^H R, A = R^-1, B = C R^-1, and
+// the running totals Ct = Ct + C Rt, Rt = R Rt (Rt = I, Ct = 0 before pass 0).
+// A failed factorisation (a pivot not above 1e-26 of the block's scale, or
+// not finite) ends the cycle at the columns already finished.
+template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, int pass) {
+    DevState *st = kp.st;
+    const int k = st->k;
+    const int nq = k + 1;
+    const SsLayout L(kp.mcap);
+    const double2 *C = kp.ss + L.C;
+    double2 *Ct = kp.ss + L.Ct;
+    double2 *Bc = kp.ss + L.Bc;
+    const double2 *G = kp.ss + L.G;
+    double2 *Rt = kp.ss + L.Rt;
+    double2 *Ai = kp.ss + L.Ai;
+    __shared__ double2 gp[S][S];
+    __shared__ double2 rr[S][S];
+    __shared__ double2 ai[S][S];
+    __shared__ double2 rt_old[S][S];
+    __shared__ double red[SS_WARPS][2];
+    __shared__ int ok;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // C^H C, one entry per warp round: sum over the nq rows
+    for (int e = 0; e < S * S; e++) {
+        const int i = e / S, l = e % S;
+        if (l < i) continue;
+        double sr = 0.0, si = 0.0;
+        for (int j = tid; j < nq; j += SS_THREADS) {
+            const double2 a = C[j * SS_MAX + i], b = C[j * SS_MAX + l];
+            sr += a.x * b.x + a.y * b.y;
+            si += a.x * b.y - a.y * b.x;
+        }
+        sr = warp_sum(sr);
+        si = warp_sum(si);
+        if (lane == 0) red[warp][0] = sr, red[warp][1] = si;
+        __syncthreads();
+        if (tid == 0) {
+            double tr = 0.0, ti = 0.0;
+            for (int w = 0; w < SS_WARPS; w++) tr += red[w][0], ti += red[w][1];
+            const double2 g = G[i * SS_MAX + l];
+            gp[i][l] = make_double2(g.x - tr, g.y - ti);
+        }
+        __syncthreads();
+    }
+    if (tid == 0) {
+        for (int i = 0; i < S; i++)
+            for (int l = 0; l < i; l++) gp[i][l] = cconj(gp[l][i]);
+        double scale = 0.0;
+        for (int i = 0; i < S; i++) scale = fmax(scale, G[i * SS_MAX + i].x);
+        int good = isfinite(scale) && scale > 0.0;
+        // Cholesky gp = R^H R (R upper), row by row
+        for (int i = 0; i < S && good; i++) {
+            double d = gp[i][i].x;
+            for (int p = 0; p < i; p++) d -= rr[p][i].x * rr[p][i].x + rr[p][i].y * rr[p][i].y;
+            if (!(d > 1e-26 * scale) || !isfinite(d)) {
+                good = 0;
+                break;
+            }
+            const double rii = sqrt(d);
+            rr[i][i] = make_double2(rii, 0.0);
+            for (int l = i + 1; l < S; l++) {
+                double2 v = gp[i][l];
+                for (int p = 0; p < i; p++) v = csub(v, cmul(cconj(rr[p][i]), rr[p][l]));
+                rr[i][l] = make_double2(v.x / rii, v.y / rii);
+            }
+            for (int l = 0; l < i; l++) rr[i][l] = make_double2(0.0, 0.0);
+        }
+        if (good) {
+            // A = R^-1 (upper), column by column
+            for (int l = 0; l < S; l++) {
+                for (int i = S - 1; i >= 0; i--) {
+                    double2 v = make_double2(i == l ? 1.0 : 0.0, 0.0);
+                    for (int p = i + 1; p < S; p++) v = csub(v, cmul(rr[i][p], ai[p][l]));
+                    const double inv = 1.0 / rr[i][i].x;
+                    ai[i][l] = make_double2(v.x * inv, v.y * inv);
+                }
+            }
+            for (int i = 0; i < S; i++)
+                for (int l = 0; l < S; l++) {
+                    rt_old[i][l] = pass == 0 ? make_double2(i == l ? 1.0 : 0.0, 0.0) : Rt[i * SS_MAX + l];
+                    Ai[i * SS_MAX + l] = ai[i][l];
+                }
+        }
+        ok = good;
+    }
+    __syncthreads();
+    if (!ok) {
+        if (tid == 0) {
+            // end the cycle with the finished columns; none finished: no progress possible
+            if (k == 0) st->brk = 1;
+            st->stop = 1;
+        }
+        return;
+    }
+    // B = C R^-1 and Ct += C Rt_old (rows j = 0..k)
+    for (int e = tid; e < nq * S; e += SS_THREADS) {
+        const int j = e / S, l = e % S;
+        double2 b = make_double2(0.0, 0.0), c = make_double2(0.0, 0.0);
+        for (int i = 0; i < S; i++) {
+            const double2 cji = C[j * SS_MAX + i];
+            b = cadd(b, cmul(cji, ai[i][l]));
+            c = cadd(c, cmul(cji, rt_old[i][l]));
+        }
+        Bc[j * SS_MAX + l] = b;
+        Ct[j * SS_MAX + l] = pass == 0 ? c : cadd(Ct[j * SS_MAX + l], c);
+    }
+    if (tid < S * S) {
+        const int i = tid / S, l = tid % S;
+        double2 v = make_double2(0.0, 0.0);
+        for (int p = 0; p < S; p++) v = cadd(v, cmul(rr[i][p], rt_old[p][l]));
+        Rt[i * SS_MAX + l] = v;
+    }
+}
+
 // ------------------------------------------------------------ block dots
 // C[j][i] = <q_j, w_i> (j = 0..k, i < S), G[i][l] = <w_i, w_l>; tile-major:
 // every warp keeps its tile of the S block vectors in registers and streams
 // the basis over it.  Per-block partial rows part[b][2 S (k+1) + 2 S S] are
 // summed in two fixed-order levels (groups of 16 blocks, then the groups).
 template <typename CV, int S, int U>
-__global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp,
+                                                                       int pass) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
     if (st->stop) return;
@@ -247,122 +364,9 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
             G[2 * (i * SS_MAX + l) + (r & 1)] = s;
         }
     }
-}
-
-// ------------------------------------------------------------ Cholesky
-// One block: Gp = G - C^H C (S x S), Gp = R^H R, A = R^-1, B = C R^-1, and the
-// running totals Ct = Ct + C Rt, Rt = R Rt (Rt = I, Ct = 0 before pass 0).
-// A failed factorisation (a pivot not above 1e-26 of the block's scale, or
-// not finite) ends the cycle at the columns already finished.
-template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_chol(KrylovPtrs kp, int pass) {
-    DevState *st = kp.st;
-    if (st->stop) return;
-    const int k = st->k;
-    const int nq = k + 1;
-    const SsLayout L(kp.mcap);
-    const double2 *C = kp.ss + L.C;
-    double2 *Ct = kp.ss + L.Ct;
-    double2 *Bc = kp.ss + L.Bc;
-    const double2 *G = kp.ss + L.G;
-    double2 *Rt = kp.ss + L.Rt;
-    double2 *Ai = kp.ss + L.Ai;
-    __shared__ double2 gp[S][S];
-    __shared__ double2 rr[S][S];
-    __shared__ double2 ai[S][S];
-    __shared__ double2 rt_old[S][S];
-    __shared__ double red[SS_WARPS][2];
-    __shared__ int ok;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    // C^H C, one entry per warp round: sum over the nq rows
-    for (int e = 0; e < S * S; e++) {
-        const int i = e / S, l = e % S;
-        if (l < i) continue;
-        double sr = 0.0, si = 0.0;
-        for (int j = tid; j < nq; j += SS_THREADS) {
-            const double2 a = C[j * SS_MAX + i], b = C[j * SS_MAX + l];
-            sr += a.x * b.x + a.y * b.y;
-            si += a.x * b.y - a.y * b.x;
-        }
-        sr = warp_sum(sr);
-        si = warp_sum(si);
-        if (lane == 0) red[warp][0] = sr, red[warp][1] = si;
-        __syncthreads();
-        if (tid == 0) {
-            double tr = 0.0, ti = 0.0;
-            for (int w = 0; w < SS_WARPS; w++) tr += red[w][0], ti += red[w][1];
-            const double2 g = G[i * SS_MAX + l];
-            gp[i][l] = make_double2(g.x - tr, g.y - ti);
-        }
-        __syncthreads();
-    }
-    if (tid == 0) {
-        for (int i = 0; i < S; i++)
-            for (int l = 0; l < i; l++) gp[i][l] = cconj(gp[l][i]);
-        double scale = 0.0;
-        for (int i = 0; i < S; i++) scale = fmax(scale, G[i * SS_MAX + i].x);
-        int good = isfinite(scale) && scale > 0.0;
-        // Cholesky gp = R^H R (R upper), row by row
-        for (int i = 0; i < S && good; i++) {
-            double d = gp[i][i].x;
-            for (int p = 0; p < i; p++) d -= rr[p][i].x * rr[p][i].x + rr[p][i].y * rr[p][i].y;
-            if (!(d > 1e-26 * scale) || !isfinite(d)) {
-                good = 0;
-                break;
-            }
-            const double rii = sqrt(d);
-            rr[i][i] = make_double2(rii, 0.0);
-            for (int l = i + 1; l < S; l++) {
-                double2 v = gp[i][l];
-                for (int p = 0; p < i; p++) v = csub(v, cmul(cconj(rr[p][i]), rr[p][l]));
-                rr[i][l] = make_double2(v.x / rii, v.y / rii);
-            }
-            for (int l = 0; l < i; l++) rr[i][l] = make_double2(0.0, 0.0);
-        }
-        if (good) {
-            // A = R^-1 (upper), column by column
-            for (int l = 0; l < S; l++) {
-                for (int i = S - 1; i >= 0; i--) {
-                    double2 v = make_double2(i == l ? 1.0 : 0.0, 0.0);
-                    for (int p = i + 1; p < S; p++) v = csub(v, cmul(rr[i][p], ai[p][l]));
-                    const double inv = 1.0 / rr[i][i].x;
-                    ai[i][l] = make_double2(v.x * inv, v.y * inv);
-                }
-            }
-            for (int i = 0; i < S; i++)
-                for (int l = 0; l < S; l++) {
-                    rt_old[i][l] = pass == 0 ? make_double2(i == l ? 1.0 : 0.0, 0.0) : Rt[i * SS_MAX + l];
-                    Ai[i * SS_MAX + l] = ai[i][l];
-                }
-        }
-        ok = good;
-    }
+    // the last block goes on with the pass's Cholesky (C and G are complete)
     __syncthreads();
-    if (!ok) {
-        if (tid == 0) {
-            // end the cycle with the finished columns; none finished: no progress possible
-            if (k == 0) st->brk = 1;
-            st->stop = 1;
-        }
-        return;
-    }
-    // B = C R^-1 and Ct += C Rt_old (rows j = 0..k)
-    for (int e = tid; e < nq * S; e += SS_THREADS) {
-        const int j = e / S, l = e % S;
-        double2 b = make_double2(0.0, 0.0), c = make_double2(0.0, 0.0);
-        for (int i = 0; i < S; i++) {
-            const double2 cji = C[j * SS_MAX + i];
-            b = cadd(b, cmul(cji, ai[i][l]));
-            c = cadd(c, cmul(cji, rt_old[i][l]));
-        }
-        Bc[j * SS_MAX + l] = b;
-        Ct[j * SS_MAX + l] = pass == 0 ? c : cadd(Ct[j * SS_MAX + l], c);
-    }
-    if (tid < S * S) {
-        const int i = tid / S, l = tid % S;
-        double2 v = make_double2(0.0, 0.0);
-        for (int p = 0; p < S; p++) v = cadd(v, cmul(rr[i][p], rt_old[p][l]));
-        Rt[i * SS_MAX + l] = v;
-    }
+    ss_chol<S>(kp, pass);
 }
 
 // ------------------------------------------------------------ update
@@ -512,16 +516,32 @@ template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovP
         const int i = r - k - 1;
         return i <= c - 1 ? Rt[i * SS_MAX + (c - 1)] : make_double2(0.0, 0.0);
     };
-    // M = Rall T - [H_old C''; 0]
-    for (int e = tid; e < nr * S; e += SS_THREADS) {
-        const int r = e / S, j = e % S;
-        double2 v = cadd(cmul(rall(r, j), Th[j]), rall(r, j + 1));
-        if (r <= k && j >= 1) {
-            double2 h = make_double2(0.0, 0.0);
-            for (int l = (r > 0 ? r - 1 : 0); l < k; l++) h = cadd(h, cmul(kp.Hm[(size_t)r * ld + l], Ct[l * SS_MAX + (j - 1)]));
-            v = csub(v, h);
-        }
-        M[e] = v;
+    // M = Rall T - [H_old C''; 0]: one warp per row r, its lanes over the
+    // columns l of H_old (upper Hessenberg: l >= r - 1), fixed-order warp sums
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int r = warp; r < nr; r += SS_WARPS) {
+        double hs[2 * (S - 1) > 0 ? 2 * (S - 1) : 1];
+#pragma unroll
+        for (int q = 0; q < 2 * (S - 1); q++) hs[q] = 0.0;
+        if (r <= k)
+            for (int l = (r > 0 ? r - 1 : 0) + lane; l < k; l += 32) {
+                const double2 hv = kp.Hm[(size_t)r * ld + l];
+#pragma unroll
+                for (int jj = 0; jj < S - 1; jj++) {
+                    const double2 p = cmul(hv, Ct[l * SS_MAX + jj]);
+                    hs[2 * jj] += p.x;
+                    hs[2 * jj + 1] += p.y;
+                }
+            }
+#pragma unroll
+        for (int q = 0; q < 2 * (S - 1); q++) hs[q] = warp_sum(hs[q]);
+#pragma unroll
+        for (int j = 0; j < S; j++)
+            if (lane == j) {
+                double2 v = cadd(cmul(rall(r, j), Th[j]), rall(r, j + 1));
+                if (r <= k && j >= 1) v = csub(v, make_double2(hs[2 * (j - 1)], hs[2 * (j - 1) + 1]));
+                M[r * S + j] = v;
+            }
     }
     if (tid < S * S) {
         const int r = tid / S, c = tid % S;
@@ -555,12 +575,24 @@ template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovP
     if (tid < cols) {
         const int c = tid;
         double2 carry = M[0 * S + c];
-        for (int j = 0; j < k; j++) {
-            const double2 cj = kp.cs[j];
-            const double sj = kp.sn[j];
-            const double2 nx = M[(j + 1) * S + c];
-            kp.Rm[(size_t)(k + c) * ld + j] = cadd(cmul(cconj(cj), carry), cscale(nx, sj));
-            carry = csub(cmul(cj, nx), cscale(carry, sj));
+        // the loads do not depend on the carry: fetch 8 rotations ahead of the chain
+        constexpr int RC = 8;
+        for (int j0 = 0; j0 < k; j0 += RC) {
+            double2 cj[RC], nx[RC];
+            double sj[RC];
+#pragma unroll
+            for (int u = 0; u < RC; u++)
+                if (j0 + u < k) {
+                    cj[u] = kp.cs[j0 + u];
+                    sj[u] = kp.sn[j0 + u];
+                    nx[u] = M[(j0 + u + 1) * S + c];
+                }
+#pragma unroll
+            for (int u = 0; u < RC; u++)
+                if (j0 + u < k) {
+                    kp.Rm[(size_t)(k + c) * ld + j0 + u] = cadd(cmul(cconj(cj[u]), carry), cscale(nx[u], sj[u]));
+                    carry = csub(cmul(cj[u], nx[u]), cscale(carry, sj[u]));
+                }
         }
         M[k * S + c] = carry;
     }
@@ -636,17 +668,17 @@ template <typename K> static int ss_smem(K kern, size_t bytes) {
 
 static constexpr int SS_U32 = 8;  // tile width used to size the grid
 
-template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int nblk,
+template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int nblk, int pass,
                                       cudaStream_t s) {
     const size_t smem = sizeof(double) * ((size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)SS_WARPS * 2 * S * S);
     if (prec == 0) {
         auto kern = k_ss_dots<double2, S, ss_u64<S>()>;
         if (int e = ss_smem(kern, smem)) return e;
-        kern<<<nblk, SS_THREADS, smem, s>>>((const double2 *)V, n, kp);
+        kern<<<nblk, SS_THREADS, smem, s>>>((const double2 *)V, n, kp, pass);
     } else {
         auto kern = k_ss_dots<float2, S, ss_u32<S>()>;
         if (int e = ss_smem(kern, smem)) return e;
-        kern<<<nblk, SS_THREADS, smem, s>>>((const float2 *)V, n, kp);
+        kern<<<nblk, SS_THREADS, smem, s>>>((const float2 *)V, n, kp, pass);
     }
     return (int)cudaGetLastError();
 }
@@ -681,14 +713,9 @@ int sstep_blocks(int sms, long long n) {
     return (int)(g < 1 ? 1 : g);
 }
 
-int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int nblk, cudaStream_t s) {
-#define CALL(S_) ss_dots_t<S_>(prec, V, n, kp, nblk, s)
-    SS_DISPATCH(S, CALL)
-#undef CALL
-}
-
-int launch_ss_chol(const KrylovPtrs &kp, int S, int pass, cudaStream_t s) {
-#define CALL(S_) (k_ss_chol<S_><<<1, SS_THREADS, 0, s>>>(kp, pass), (int)cudaGetLastError())
+int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int nblk, int pass,
+                   cudaStream_t s) {
+#define CALL(S_) ss_dots_t<S_>(prec, V, n, kp, nblk, pass, s)
     SS_DISPATCH(S, CALL)
 #undef CALL
 }
