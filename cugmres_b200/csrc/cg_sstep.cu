@@ -45,6 +45,22 @@ template <int S> constexpr int ss_u32() { return 32 / S > 8 ? 8 : (32 / S > 1 ? 
 // with 8 points and one block of 8 warps (4.9 against 4.0 TB/s)
 template <int S> constexpr int ss_u64_upd() { return 16 / S > 4 ? 4 : (16 / S > 1 ? 16 / S : 1); }
 template <typename CV> constexpr int ss_minb() { return sizeof(CV) == 16 ? 1 : 2; }
+// stages of a warp's private basis-tile ring in the dot pass (cp.async, one
+// commit group per basis vector, each lane copying and reading its own points)
+static constexpr int SS_NST = 4;
+
+static __device__ __forceinline__ void cp_async_cv(double2 *dst, const double2 *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+static __device__ __forceinline__ void cp_async_cv(float2 *dst, const float2 *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+static __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> static __device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // offsets (in double2) of the s-step scratch arrays in kp.ss; M1 = mcap + 1
 struct SsLayout {
@@ -241,10 +257,13 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
     const int nq = k + 1;
     const CV *W = V + (long long)(k + 1) * n;
     const int pld = ss_pld(kp.mcap);
-    extern __shared__ double sacc[];  // [SS_WARPS][SS_CHUNK][2 S], then [SS_WARPS][2 S S]
+    // [SS_WARPS][SS_CHUNK][2 S] and [SS_WARPS][2 S S] doubles, then the rings [SS_WARPS][SS_NST][U][32]
+    extern __shared__ __align__(16) double sacc[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double *my = sacc + (size_t)warp * SS_CHUNK * 2 * S;
     double *myg = sacc + (size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)warp * 2 * S * S;
+    CV *ring = reinterpret_cast<CV *>(sacc + (size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)SS_WARPS * 2 * S * S) +
+               (size_t)warp * SS_NST * U * 32;
     const long long TILE = 32LL * U;
     const long long ntile = (n + TILE - 1) / TILE;
     const long long nw = (long long)gridDim.x * SS_WARPS;
@@ -285,22 +304,30 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
                         }
                     }
             }
-            CV a[U];
-#pragma unroll
-            for (int t = 0; t < U; t++) {
-                const long long e = e0 + 32 * t;
-                a[t] = (full || e < n) ? __ldcs(V + (long long)jc * n + e) : czero<CV>();
-            }
-            for (int j = 0; j < nj; j++) {
-                // the next basis vector's tile in flight during this one's products and reduction
-                CV an[U];
-                if (j + 1 < nj) {
-                    const CV *qn = V + (long long)(jc + j + 1) * n;
+            // basis tiles stream through the warp's ring, SS_NST - 1 vectors ahead
+            auto issue = [&](int jj) {
+                if (jj < nj) {
+                    const CV *q = V + (long long)(jc + jj) * n;
+                    CV *slot = ring + (size_t)(jj % SS_NST) * U * 32;
 #pragma unroll
                     for (int t = 0; t < U; t++) {
                         const long long e = e0 + 32 * t;
-                        an[t] = (full || e < n) ? __ldcs(qn + e) : czero<CV>();
+                        if (full || e < n) cp_async_cv(slot + t * 32 + lane, q + e);
                     }
+                }
+                cp_async_commit();
+            };
+#pragma unroll
+            for (int jj = 0; jj < SS_NST - 1; jj++) issue(jj);
+            for (int j = 0; j < nj; j++) {
+                issue(j + SS_NST - 1);
+                cp_async_wait<SS_NST - 1>();  // this lane's copies of vector j have landed
+                CV a[U];
+                const CV *slot = ring + (size_t)(j % SS_NST) * U * 32;
+#pragma unroll
+                for (int t = 0; t < U; t++) {
+                    const long long e = e0 + 32 * t;
+                    a[t] = (full || e < n) ? slot[t * 32 + lane] : czero<CV>();
                 }
                 double d[2 * S];
 #pragma unroll
@@ -317,10 +344,6 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
                 }
                 const double tot = warp_sum_scatter<2 * S>(d, lane);
                 if (scatter_writer<2 * S>(lane)) my[2 * S * j + scatter_index<2 * S>(lane)] += tot;
-                if (j + 1 < nj) {
-#pragma unroll
-                    for (int t = 0; t < U; t++) a[t] = an[t];
-                }
             }
         }
         gram_done = true;
@@ -387,6 +410,8 @@ __global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V,
         sa[e / S][e % S] = mk<CV>((R)a.x, (R)a.y);
     }
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    extern __shared__ __align__(16) unsigned char ss_upd_smem[];  // rings [SS_WARPS][SS_NST][U][32]
+    CV *ring = reinterpret_cast<CV *>(ss_upd_smem) + (size_t)warp * SS_NST * U * 32;
     const long long TILE = 32LL * U;
     const long long ntile = (n + TILE - 1) / TILE;
     const long long nw = (long long)gridDim.x * SS_WARPS;
@@ -435,31 +460,36 @@ __global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V,
             }
             __syncthreads();
             if (live) {
-                CV a[U];
-#pragma unroll
-                for (int t = 0; t < U; t++) {
-                    const long long e = e0 + 32 * t;
-                    a[t] = (full || e < n) ? __ldcs(V + (long long)jc * n + e) : czero<CV>();
-                }
-                for (int j = 0; j < nj; j++) {
-                    CV an[U];  // the next basis vector's tile in flight
-                    if (j + 1 < nj) {
-                        const CV *qn = V + (long long)(jc + j + 1) * n;
+                // basis tiles stream through the warp's ring, SS_NST - 1 vectors ahead
+                auto issue = [&](int jj) {
+                    if (jj < nj) {
+                        const CV *q = V + (long long)(jc + jj) * n;
+                        CV *slot = ring + (size_t)(jj % SS_NST) * U * 32;
 #pragma unroll
                         for (int t = 0; t < U; t++) {
                             const long long e = e0 + 32 * t;
-                            an[t] = (full || e < n) ? __ldcs(qn + e) : czero<CV>();
+                            if (full || e < n) cp_async_cv(slot + t * 32 + lane, q + e);
                         }
+                    }
+                    cp_async_commit();
+                };
+#pragma unroll
+                for (int jj = 0; jj < SS_NST - 1; jj++) issue(jj);
+                for (int j = 0; j < nj; j++) {
+                    issue(j + SS_NST - 1);
+                    cp_async_wait<SS_NST - 1>();  // this lane's copies of vector j have landed
+                    CV a[U];
+                    const CV *slot = ring + (size_t)(j % SS_NST) * U * 32;
+#pragma unroll
+                    for (int t = 0; t < U; t++) {
+                        const long long e = e0 + 32 * t;
+                        a[t] = (full || e < n) ? slot[t * 32 + lane] : czero<CV>();
                     }
 #pragma unroll
                     for (int l = 0; l < S; l++) {
                         const CV b = sb[j][l];
 #pragma unroll
                         for (int t = 0; t < U; t++) acc[l][t] = cfms(acc[l][t], a[t], b);
-                    }
-                    if (j + 1 < nj) {
-#pragma unroll
-                        for (int t = 0; t < U; t++) a[t] = an[t];
                     }
                 }
             }
@@ -670,12 +700,14 @@ static constexpr int SS_U32 = 8;  // tile width used to size the grid
 
 template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int nblk, int pass,
                                       cudaStream_t s) {
-    const size_t smem = sizeof(double) * ((size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)SS_WARPS * 2 * S * S);
+    const size_t acc = sizeof(double) * ((size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)SS_WARPS * 2 * S * S);
     if (prec == 0) {
+        const size_t smem = acc + sizeof(double2) * (size_t)SS_WARPS * SS_NST * ss_u64<S>() * 32;
         auto kern = k_ss_dots<double2, S, ss_u64<S>()>;
         if (int e = ss_smem(kern, smem)) return e;
         kern<<<nblk, SS_THREADS, smem, s>>>((const double2 *)V, n, kp, pass);
     } else {
+        const size_t smem = acc + sizeof(float2) * (size_t)SS_WARPS * SS_NST * ss_u32<S>() * 32;
         auto kern = k_ss_dots<float2, S, ss_u32<S>()>;
         if (int e = ss_smem(kern, smem)) return e;
         kern<<<nblk, SS_THREADS, smem, s>>>((const float2 *)V, n, kp, pass);
@@ -685,8 +717,17 @@ template <int S> static int ss_dots_t(int prec, const void *V, long long n, cons
 
 template <int S> static int ss_update_t(int prec, void *V, long long n, const KrylovPtrs &kp, int nblk,
                                         cudaStream_t s) {
-    if (prec == 0) k_ss_update<double2, S, ss_u64_upd<S>()><<<nblk, SS_THREADS, 0, s>>>((double2 *)V, n, kp);
-    else k_ss_update<float2, S, ss_u32<S>()><<<nblk, SS_THREADS, 0, s>>>((float2 *)V, n, kp);
+    if (prec == 0) {
+        const size_t smem = sizeof(double2) * (size_t)SS_WARPS * SS_NST * ss_u64_upd<S>() * 32;
+        auto kern = k_ss_update<double2, S, ss_u64_upd<S>()>;
+        if (int e = ss_smem(kern, smem)) return e;
+        kern<<<nblk, SS_THREADS, smem, s>>>((double2 *)V, n, kp);
+    } else {
+        const size_t smem = sizeof(float2) * (size_t)SS_WARPS * SS_NST * ss_u32<S>() * 32;
+        auto kern = k_ss_update<float2, S, ss_u32<S>()>;
+        if (int e = ss_smem(kern, smem)) return e;
+        kern<<<nblk, SS_THREADS, smem, s>>>((float2 *)V, n, kp);
+    }
     return (int)cudaGetLastError();
 }
 
