@@ -294,7 +294,7 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes, int extra = 0)
         const size_t part_cgs2 = 2 * (size_t)dot_blocks(c) * (mc + 1);
         const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) *
                                   (size_t)dots2_part_ld(mc);
-        const size_t nss = (size_t)sstep_blocks(c->sms, n);  // grid of the s-step block passes
+        const size_t nss = (size_t)sstep_blocks(c->sms, n);  // most blocks of the s-step dot pass (its partial rows)
         const size_t part_ss = nss * (size_t)sstep_part_ld(mc);
         CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(std::max(part_cgs2, part_dcgs2), part_ss)));
         const size_t ng2 = ((size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) + 15) / 16;
@@ -1231,9 +1231,9 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, b * S, q));
             for (int pass = 0; pass < 2; pass++) {
                 // the dot pass's last block also runs the pass's Cholesky
-                CG_LAUNCH(launch_ss_dots(prec, c->V, n, kp, S, nss, pass, q));
+                CG_LAUNCH(launch_ss_dots(prec, c->V, n, kp, S, c->sms, pass, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, b * S, q));
-                CG_LAUNCH(launch_ss_update(prec, c->V, n, kp, S, nss, q));
+                CG_LAUNCH(launch_ss_update(prec, c->V, n, kp, S, c->sms, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, b * S, q));
             }
             CG_LAUNCH(launch_ss_hess(kp, S, q));

@@ -189,10 +189,11 @@ long long sstep_scratch_elems(int mcap);  // double2 entries of KrylovPtrs::ss
 int sstep_part_ld(int mcap);              // partials per block of the block dot pass
 int sstep_blocks(int sms, long long n);   // grid of the block dot and update passes
 int launch_ss_norm0(int prec, void *V, long long n, const KrylovPtrs &kp, cudaStream_t s);
-// block dots of pass `pass` (0 or 1); the last block also runs the pass's Cholesky
-int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int nblk, int pass,
+// block dots of pass `pass` (0 or 1); the last block also runs the pass's Cholesky.
+// The dot and update passes size their grids from the SM count (sms).
+int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int sms, int pass,
                    cudaStream_t s);
-int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int nblk, cudaStream_t s);
+int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int sms, cudaStream_t s);
 int launch_ss_hess(const KrylovPtrs &kp, int S, cudaStream_t s);
 int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
                  cudaStream_t s);

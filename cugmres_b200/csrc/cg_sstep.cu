@@ -698,35 +698,57 @@ template <typename K> static int ss_smem(K kern, size_t bytes) {
 
 static constexpr int SS_U32 = 8;  // tile width used to size the grid
 
-template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int nblk, int pass,
+// Grid of a tile-major pass: the fewest rounds of warp tiles the resident
+// blocks allow (`per_sm` blocks of SS_WARPS warps on each of `sms` SMs), then
+// the fewest blocks that still finish in that many rounds, so every warp gets
+// the same number of tiles (1024^2 FP64 dots: 4096 tiles -> 128 blocks of 4
+// rounds, where 148 resident blocks would leave the fourth round 46 % full);
+// at most `cap` blocks (the rows of the partial buffers).
+static int ss_grid(long long ntile, int sms, int per_sm, int cap) {
+    const long long resident = (long long)sms * per_sm * SS_WARPS;
+    const long long rounds = (ntile + resident - 1) / resident;
+    long long g = (ntile + rounds * SS_WARPS - 1) / (rounds * SS_WARPS);
+    if (g > cap) g = cap;
+    return (int)(g < 1 ? 1 : g);
+}
+
+template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int sms, int pass,
                                       cudaStream_t s) {
     const size_t acc = sizeof(double) * ((size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)SS_WARPS * 2 * S * S);
+    const int cap = sstep_blocks(sms, n);
     if (prec == 0) {
-        const size_t smem = acc + sizeof(double2) * (size_t)SS_WARPS * SS_NST * ss_u64<S>() * 32;
-        auto kern = k_ss_dots<double2, S, ss_u64<S>()>;
+        constexpr int U = ss_u64<S>();
+        const size_t smem = acc + sizeof(double2) * (size_t)SS_WARPS * SS_NST * U * 32;
+        auto kern = k_ss_dots<double2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
+        const int nblk = ss_grid((n + 32 * U - 1) / (32 * U), sms, ss_minb<double2>(), cap);
         kern<<<nblk, SS_THREADS, smem, s>>>((const double2 *)V, n, kp, pass);
     } else {
-        const size_t smem = acc + sizeof(float2) * (size_t)SS_WARPS * SS_NST * ss_u32<S>() * 32;
-        auto kern = k_ss_dots<float2, S, ss_u32<S>()>;
+        constexpr int U = ss_u32<S>();
+        const size_t smem = acc + sizeof(float2) * (size_t)SS_WARPS * SS_NST * U * 32;
+        auto kern = k_ss_dots<float2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
+        const int nblk = ss_grid((n + 32 * U - 1) / (32 * U), sms, ss_minb<float2>(), cap);
         kern<<<nblk, SS_THREADS, smem, s>>>((const float2 *)V, n, kp, pass);
     }
     return (int)cudaGetLastError();
 }
 
-template <int S> static int ss_update_t(int prec, void *V, long long n, const KrylovPtrs &kp, int nblk,
+template <int S> static int ss_update_t(int prec, void *V, long long n, const KrylovPtrs &kp, int sms,
                                         cudaStream_t s) {
+    const int cap = 2 * sms;  // the update writes no partial rows: the cap is occupancy only
     if (prec == 0) {
-        const size_t smem = sizeof(double2) * (size_t)SS_WARPS * SS_NST * ss_u64_upd<S>() * 32;
-        auto kern = k_ss_update<double2, S, ss_u64_upd<S>()>;
+        constexpr int U = ss_u64_upd<S>();
+        const size_t smem = sizeof(double2) * (size_t)SS_WARPS * SS_NST * U * 32;
+        auto kern = k_ss_update<double2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
-        kern<<<nblk, SS_THREADS, smem, s>>>((double2 *)V, n, kp);
+        kern<<<ss_grid((n + 32 * U - 1) / (32 * U), sms, 2, cap), SS_THREADS, smem, s>>>((double2 *)V, n, kp);
     } else {
-        const size_t smem = sizeof(float2) * (size_t)SS_WARPS * SS_NST * ss_u32<S>() * 32;
-        auto kern = k_ss_update<float2, S, ss_u32<S>()>;
+        constexpr int U = ss_u32<S>();
+        const size_t smem = sizeof(float2) * (size_t)SS_WARPS * SS_NST * U * 32;
+        auto kern = k_ss_update<float2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
-        kern<<<nblk, SS_THREADS, smem, s>>>((float2 *)V, n, kp);
+        kern<<<ss_grid((n + 32 * U - 1) / (32 * U), sms, 2, cap), SS_THREADS, smem, s>>>((float2 *)V, n, kp);
     }
     return (int)cudaGetLastError();
 }
@@ -754,15 +776,15 @@ int sstep_blocks(int sms, long long n) {
     return (int)(g < 1 ? 1 : g);
 }
 
-int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int nblk, int pass,
+int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int sms, int pass,
                    cudaStream_t s) {
-#define CALL(S_) ss_dots_t<S_>(prec, V, n, kp, nblk, pass, s)
+#define CALL(S_) ss_dots_t<S_>(prec, V, n, kp, sms, pass, s)
     SS_DISPATCH(S, CALL)
 #undef CALL
 }
 
-int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int nblk, cudaStream_t s) {
-#define CALL(S_) ss_update_t<S_>(prec, V, n, kp, nblk, s)
+int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int sms, cudaStream_t s) {
+#define CALL(S_) ss_update_t<S_>(prec, V, n, kp, sms, s)
     SS_DISPATCH(S, CALL)
 #undef CALL
 }
