@@ -67,6 +67,33 @@ def test_sstep_matches_dcgs2_on_the_benchmark_system(solver, S):
     assert abs(ib["rel_residual_true"] - ia["rel_residual_true"]) <= 1e-8 * ia["rel_residual_true"]
 
 
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_sstep_partial_tiles_on_an_odd_grid(solver, oracle, precision):
+    """N = 45: n = 2025 points is odd and no multiple of a pass's tile, so the
+    last tile of every dot and update pass (and of every warp's copy ring) is
+    partial.  FP64: three whole GMRES(20) cycles give the oracle's iterate and
+    residual estimates; both precisions converge to 1e-10 like the oracle."""
+    N = 45
+    pr = P.helmholtz(N, 4.0, seed=7)  # GMRES(20): 140 steps in 7 cycles
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    chi = pr["chi"] * pr["chi_scale"]
+    if precision == "fp64":
+        x, info = solver.solve(pr["b"], restart=20, max_iter=60, tol=0.0, ortho="sstep", sstep=4)
+        o = oracle.gmres(gh, chi, pr["b"], restart=20, maxiter=60, tol=0.0)
+        assert info["iterations"] == o["iterations"] == 60 and info["cycles"] == 3
+        assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
+        assert np.allclose(info["res_hist"][1:], o["res_hist"][1:], rtol=1e-7)
+    x, info = solver.solve(pr["b"], restart=20, max_iter=3000, tol=1e-10, precision=precision, ortho="sstep", sstep=4)
+    o = oracle.gmres(gh, chi, pr["b"], restart=20, maxiter=3000, tol=1e-10)
+    assert info["status"] == 0 and o["status"] == 0 and info["cycles"] > 1
+    assert info["rel_residual_true"] <= 1e-10
+    t = oracle.gmres(gh, chi, pr["b"], restart=20, maxiter=6000, tol=1e-13)
+    assert np.linalg.norm(x - t["x"]) / np.linalg.norm(t["x"]) < 1e-8
+    if precision == "fp64":
+        assert abs(info["iterations"] - o["iterations"]) <= 2, (info["iterations"], o["iterations"])
+
+
 def test_sstep_mixed_precision(solver):
     N = 96
     pr = P.helmholtz(N, 2.25, seed=31)
