@@ -974,6 +974,7 @@ struct cg_fno {
     int *err = nullptr;
     // workspace
     long long cap_cells = 0, cap_lines = 0, cap_part = 0, cap_spec = 0;
+    long long cap_vt = 0;  // cells of vT (0: not allocated; only W = 1024 grids use it)
     int cap_B = 0;
     unsigned char *ws = nullptr;
     __nv_bfloat16 *act[LAYERS + 1] = {}, *zpre[LAYERS - 1] = {}, *zq = nullptr, *dz[2] = {}, *dzq = nullptr;
@@ -1047,16 +1048,21 @@ int ensure_ws(cg_fno *f, int B, int H, int W) {
     const long long hp = (long long)B * HC * K1N * NJ;
     const int nred = reduction_blocks(f, cells);
     const long long part = std::max<long long>((long long)nred * (HID * C + HID), 2LL * nred + 16);
-    if (cells <= f->cap_cells && lines <= f->cap_lines && B <= f->cap_B && hp <= f->cap_spec && part <= f->cap_part)
+    // the channel-major copy feeds the tensor-core column DFT, which only W = 1024 grids run
+    const long long vt = W == 1024 ? cells : 0;
+    if (cells <= f->cap_cells && lines <= f->cap_lines && B <= f->cap_B && hp <= f->cap_spec && part <= f->cap_part &&
+        vt <= f->cap_vt)
         return CG_OK;
     const long long nc = std::max(cells, f->cap_cells), nl = std::max(lines, f->cap_lines);
+    const long long nvt = std::max(vt, f->cap_vt);
     const int nb = std::max(B, f->cap_B);
     const long long nh = std::max(hp, f->cap_spec), np = std::max(part, f->cap_part);
     size_t off = 0;
     std::vector<std::pair<void **, size_t>> plan;
     auto add = [&](void **ptr, size_t bytes) { plan.push_back({ptr, bytes}); };
     for (int l = 0; l <= LAYERS; l++) add((void **)&f->act[l], (size_t)nc * C * 2);
-    add((void **)&f->vT, (size_t)nc * C * 2);
+    f->vT = nullptr;
+    if (nvt > 0) add((void **)&f->vT, (size_t)nvt * C * 2);
     for (int l = 0; l < LAYERS - 1; l++) add((void **)&f->zpre[l], (size_t)nc * C * 2);
     add((void **)&f->zq, (size_t)nc * HID * 2);
     add((void **)&f->dz[0], (size_t)nc * C * 2);
@@ -1089,7 +1095,8 @@ int ensure_ws(cg_fno *f, int B, int H, int W) {
     if (cudaMalloc(&base, off) != cudaSuccess) {
         cudaGetLastError();
         f->cap_cells = f->cap_lines = f->cap_B = 0;
-        f->cap_spec = f->cap_part = 0;
+        f->cap_spec = f->cap_part = f->cap_vt = 0;
+        f->vT = nullptr;
         return CG_ERR_OOM;
     }
     f->ws = base;
@@ -1103,6 +1110,7 @@ int ensure_ws(cg_fno *f, int B, int H, int W) {
     f->cap_B = nb;
     f->cap_spec = nh;
     f->cap_part = np;
+    f->cap_vt = nvt;
     f->map_cells = -1;
     return CG_OK;
 }
@@ -1114,7 +1122,8 @@ int ensure_maps(cg_fno *f, long long cells) {
     for (int q = 0; q < 2; q++)
         if (make_map(&f->mapDZ[q], f->dz[q], cells, C, umma::TILE_M)) return CG_ERR_CUDA;
     if (make_map(&f->mapDZQ, f->dzq, cells, HID, umma::TILE_M)) return CG_ERR_CUDA;
-    if (make_map(&f->mapVT, f->vT, cells, C, umma::TILE_M)) return CG_ERR_CUDA;  // rows (line, c, w1) x 32 w2
+    // rows (line, c, w1) x 32 w2; only where the W = 1024 workspace holds vT for these cells
+    if (f->vT && f->cap_vt >= cells && make_map(&f->mapVT, f->vT, cells, C, umma::TILE_M)) return CG_ERR_CUDA;
     f->map_cells = cells;
     return CG_OK;
 }
@@ -1144,7 +1153,7 @@ bool tc_dft(const cg_fno *f, int W) {
         const char *e = getenv("CUGMRES_FNO_TC_DFT");
         return !(e && e[0] == '0');
     }();
-    return on && W == 1024 && f->twb != nullptr;
+    return on && W == 1024 && f->twb != nullptr && f->vT != nullptr;
 }
 
 int ensure_tc_dft(cg_fno *f) {
