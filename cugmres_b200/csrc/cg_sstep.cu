@@ -131,7 +131,9 @@ template <int V> __device__ __forceinline__ bool scatter_writer(int lane) { retu
 // G are summed): Gp = G - C^H C (S x S), Gp = R^H R, A = R^-1, B = C R^-1, and
 // the running totals Ct = Ct + C Rt, Rt = R Rt (Rt = I, Ct = 0 before pass 0).
 // A failed factorisation (a pivot not above 1e-26 of the block's scale, or
-// not finite) ends the cycle at the columns already finished.
+// not finite) in the second pass ends the cycle at the columns already
+// finished; in the first pass the block is projected without normalisation
+// (R = I) and the second pass factors it.
 template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, int pass) {
     DevState *st = kp.st;
     const int k = st->k;
@@ -194,6 +196,21 @@ template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, i
                 rr[i][l] = make_double2(v.x / rii, v.y / rii);
             }
             for (int l = 0; l < i; l++) rr[i][l] = make_double2(0.0, 0.0);
+        }
+        if (!good && pass == 0 && isfinite(scale) && scale > 0.0) {
+            // The Pythagorean update G - C^H C cancelled: the block lies almost in
+            // the basis.  Take R = I for this pass, so that its update only projects
+            // (W <- W - Q C) and the second pass factors the Gram matrix of the
+            // projected block, where nothing cancels; the running totals come out
+            // as Ct = C1 + C2, Rt = R2.  Non-finite coefficients still end the cycle.
+            bool fin = true;
+            for (int i = 0; i < S; i++)
+                for (int l = 0; l < S; l++) fin = fin && isfinite(gp[i][l].x) && isfinite(gp[i][l].y);
+            if (fin) {
+                for (int i = 0; i < S; i++)
+                    for (int l = 0; l < S; l++) rr[i][l] = make_double2(i == l ? 1.0 : 0.0, 0.0);
+                good = 1;
+            }
         }
         if (good) {
             // A = R^-1 (upper), column by column
