@@ -543,7 +543,7 @@ __global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V,
 // One block: the S new columns k..k+S-1 of H (rows 0..k+S) from the block's
 // coefficients (Ct, Rt), the shifts and the earlier columns of H, then their
 // Givens rotations, residual estimates and the stop decision.
-template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovPtrs kp) {
+template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovPtrs kp, int m_in_smem) {
     DevState *st = kp.st;
     if (st->stop) return;
     const int k = st->k;
@@ -553,7 +553,10 @@ template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovP
     const double2 *Rt = kp.ss + L.Rt;
     const double2 *Th = kp.ss + L.Th;
     const int tid = threadIdx.x;
-    double2 *M = kp.ss + L.Mh;  // [(k + S + 1) * S], row-major (global: long cycles do not fit shared memory)
+    // work rows [(k + S + 1) * S], row-major: in shared memory when the launch
+    // provides (mcap + SS_MAX + 1) * S of them, else in the global scratch (long cycles)
+    extern __shared__ double2 ss_hess_smem[];
+    double2 *M = m_in_smem ? ss_hess_smem : kp.ss + L.Mh;
     __shared__ double2 rh[S][S];  // Rhat
     const int nr = k + S + 1;
     // Rall[r][c], c = 0..S: column 0 = e_k; column c >= 1: Ct(:, c-1) on rows <= k, Rt(:, c-1) below
@@ -771,7 +774,9 @@ template <int S> static int ss_update_t(int prec, void *V, long long n, const Kr
 }
 
 template <int S> static int ss_hess_t(const KrylovPtrs &kp, cudaStream_t s) {
-    k_ss_hess<S><<<1, SS_THREADS, 0, s>>>(kp);
+    const size_t smem = sizeof(double2) * (size_t)(kp.mcap + SS_MAX + 1) * S;
+    const bool in_smem = smem <= 48 * 1024;
+    k_ss_hess<S><<<1, SS_THREADS, in_smem ? smem : 0, s>>>(kp, in_smem ? 1 : 0);
     return (int)cudaGetLastError();
 }
 
