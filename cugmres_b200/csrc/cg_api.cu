@@ -558,11 +558,21 @@ int prof_mark(cg_ctx *c, CycleProf &cp, int phase, int iter, cudaStream_t s) {
 // the block's ss matvecs and iter is the block's first basis index.
 int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed, int ss = 0) {
     if (c->prof && cp.used >= 2) {
+        // s-step: a block that skipped its second Gram-Schmidt pass moved no bytes in
+        // its second dot and update launches (the second of each per block start k)
+        std::vector<int> skipped;
+        std::map<int, int> seen_dots, seen_axpy;
+        if (ss > 0) CG_TRY(sstep_skipped(c->kp, c->mcap / ss + 1, skipped, c->stream));
         for (int i = 0; i + 1 < cp.used; i++) {
             float ms = 0.f;
             CG_CU(cudaEventElapsedTime(&ms, c->evpool[i], c->evpool[i + 1]));
             const int t = cp.tag[i], k = cp.iter[i];
-            const bool live = k < steps_done;
+            bool live = k < steps_done;
+            if (ss > 0 && k >= 0 && (t == CG_PHASE_DOTS || t == CG_PHASE_AXPY)) {
+                const int nth = (t == CG_PHASE_DOTS ? seen_dots : seen_axpy)[k]++;
+                const int blk = k / ss;
+                if (nth == 1 && blk < (int)skipped.size() && skipped[blk]) live = false;
+            }
             double bytes = 0.0;
             switch (ss > 0 ? -t - 100 : t) {
                 case CG_PHASE_MATVEC: bytes = live ? 16.0 * n * e : 0.0; break;
@@ -1233,7 +1243,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
                 // the dot pass's last block also runs the pass's Cholesky
                 CG_LAUNCH(launch_ss_dots(prec, c->V, n, kp, S, c->sms, pass, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_DOTS, b * S, q));
-                CG_LAUNCH(launch_ss_update(prec, c->V, n, kp, S, c->sms, q));
+                CG_LAUNCH(launch_ss_update(prec, c->V, n, kp, S, c->sms, pass, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, b * S, q));
             }
             CG_LAUNCH(launch_ss_hess(kp, S, q));

@@ -6,6 +6,8 @@
 #include <stddef.h>
 #include <stdint.h>
 
+#include <vector>
+
 struct cg_ctx;  // solver context (cg_api.cu)
 
 namespace cg {
@@ -38,6 +40,7 @@ struct DevState {
     double2 du;       //   u_{k+1} = cw w + du u - sum S_j q_j
     double2 delta;    // q_k^H w of the current delayed CGS2 step
     unsigned int counter[8];  // tickets of the last-block reductions
+    int ss_one;               // s-step: the block's first Gram-Schmidt pass was enough (second pass skipped)
 };
 
 // Device workspace of one Krylov cycle (restart m, budget maxit).
@@ -188,12 +191,13 @@ int sstep_supported(int S);
 long long sstep_scratch_elems(int mcap);  // double2 entries of KrylovPtrs::ss
 int sstep_part_ld(int mcap);              // partials per block of the block dot pass
 int sstep_blocks(int sms, long long n);   // grid of the block dot and update passes
+int sstep_skipped(const KrylovPtrs &kp, int nblocks, std::vector<int> &flags, cudaStream_t s);
 int launch_ss_norm0(int prec, void *V, long long n, const KrylovPtrs &kp, cudaStream_t s);
 // block dots of pass `pass` (0 or 1); the last block also runs the pass's Cholesky.
 // The dot and update passes size their grids from the SM count (sms).
 int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int sms, int pass,
                    cudaStream_t s);
-int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int sms, cudaStream_t s);
+int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int sms, int pass, cudaStream_t s);
 int launch_ss_hess(const KrylovPtrs &kp, int S, cudaStream_t s);
 int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
                  cudaStream_t s);

@@ -27,6 +27,8 @@
 // Numbers, layout and reductions follow the rest of the library: the basis is
 // q_j normalised at V + j n, FP64 (or FP32 in mixed precision) complex,
 // reductions in fixed order (two-level over blocks, as cg_dcgs2.cu).
+#include <vector>
+
 #include "cg_common.cuh"
 #include "cg_internal.h"
 
@@ -48,6 +50,13 @@ template <typename CV> constexpr int ss_minb() { return sizeof(CV) == 16 ? 1 : 2
 // stages of a warp's private basis-tile ring in the dot pass (cp.async, one
 // commit group per basis vector, each lane copying and reading its own points)
 static constexpr int SS_NST = 4;
+// An FP64 block whose first pass keeps more than this fraction of every
+// vector's squared norm skips the second pass: the first pass then leaves the
+// block orthogonal to about eps / fraction (2e-15).  Measured: the 1024^2
+// GMRES(100) blocks keep 0.1 to 0.3, and the 64^2 solves keep their step counts
+// (699, 699, 673 with S = 2, 4, 8), which a 1e-2 threshold did not (711 with S = 2).
+// Complex64 blocks always take both passes (eps = 6e-8).
+static constexpr double SS_ONE_PASS = 0.1;
 
 static __device__ __forceinline__ void cp_async_cv(double2 *dst, const double2 *src) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
@@ -64,7 +73,7 @@ template <int N> static __device__ __forceinline__ void cp_async_wait() {
 
 // offsets (in double2) of the s-step scratch arrays in kp.ss; M1 = mcap + 1
 struct SsLayout {
-    long long C, Ct, Bc, G, Rt, Ai, Th, Mh, end;
+    long long C, Ct, Bc, G, Rt, Ai, Th, Mh, Sk, end;
     __host__ __device__ explicit SsLayout(int mcap) {
         const long long M1 = mcap + 1;
         C = 0;
@@ -75,11 +84,26 @@ struct SsLayout {
         Ai = Rt + SS_MAX * SS_MAX;
         Th = Ai + SS_MAX * SS_MAX;
         Mh = Th + SS_MAX;                        // [(mcap + SS_MAX + 1) * SS_MAX] work rows of k_ss_hess
-        end = Mh + (M1 + SS_MAX) * SS_MAX;
+        Sk = Mh + (M1 + SS_MAX) * SS_MAX;        // [M1] per block of the cycle: .x = 1 if its second pass was skipped
+        end = Sk + M1;
     }
 };
 
 long long sstep_scratch_elems(int mcap) { return SsLayout(mcap).end; }
+
+// Which blocks of the last s-step cycle skipped their second pass (flags[b] for
+// the block starting at column b S, nblocks of them); synchronises the stream.
+int sstep_skipped(const KrylovPtrs &kp, int nblocks, std::vector<int> &flags, cudaStream_t s) {
+    const SsLayout L(kp.mcap);
+    std::vector<double2> h((size_t)nblocks);
+    flags.assign((size_t)nblocks, 0);
+    if (nblocks <= 0) return 0;
+    if (int e = (int)cudaMemcpyAsync(h.data(), kp.ss + L.Sk, sizeof(double2) * h.size(), cudaMemcpyDeviceToHost, s))
+        return e;
+    if (int e = (int)cudaStreamSynchronize(s)) return e;
+    for (int b = 0; b < nblocks; b++) flags[b] = h[b].x != 0.0;
+    return 0;
+}
 static __host__ __device__ __forceinline__ int ss_pld(int mcap) { return 2 * SS_MAX * (mcap + 1) + 2 * SS_MAX * SS_MAX; }
 int sstep_part_ld(int mcap) { return ss_pld(mcap); }
 
@@ -134,7 +158,7 @@ template <int V> __device__ __forceinline__ bool scatter_writer(int lane) { retu
 // not finite) in the second pass ends the cycle at the columns already
 // finished; in the first pass the block is projected without normalisation
 // (R = I) and the second pass factors it.
-template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, int pass) {
+template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, int pass, double tau) {
     DevState *st = kp.st;
     const int k = st->k;
     const int nq = k + 1;
@@ -197,6 +221,7 @@ template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, i
             }
             for (int l = 0; l < i; l++) rr[i][l] = make_double2(0.0, 0.0);
         }
+        int fallback = 0;
         if (!good && pass == 0 && isfinite(scale) && scale > 0.0) {
             // The Pythagorean update G - C^H C cancelled: the block lies almost in
             // the basis.  Take R = I for this pass, so that its update only projects
@@ -210,7 +235,19 @@ template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, i
                 for (int i = 0; i < S; i++)
                     for (int l = 0; l < S; l++) rr[i][l] = make_double2(i == l ? 1.0 : 0.0, 0.0);
                 good = 1;
+                fallback = 1;
             }
+        }
+        if (pass == 0) {
+            // One pass is enough when the projection cancelled little: the lost
+            // orthogonality of a Pythagorean Cholesky pass is about eps * G_ii / R_ii^2
+            // (the squared ratio of a block vector's norm to what stays of it after
+            // projection and after the block's earlier vectors); when every
+            // R_ii^2 / G_ii exceeds tau the second pass is skipped.
+            double q = (good && !fallback) ? 1e300 : 0.0;
+            for (int i = 0; i < S && good && !fallback; i++) q = fmin(q, (rr[i][i].x * rr[i][i].x) / G[i * SS_MAX + i].x);
+            st->ss_one = q > tau ? 1 : 0;
+            kp.ss[L.Sk + k / S] = make_double2((double)st->ss_one, 0.0);  // for the byte count of the profile
         }
         if (good) {
             // A = R^-1 (upper), column by column
@@ -269,7 +306,7 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
                                                                        int pass) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
-    if (st->stop) return;
+    if (st->stop || (pass == 1 && st->ss_one)) return;
     const int k = st->k;
     const int nq = k + 1;
     const CV *W = V + (long long)(k + 1) * n;
@@ -406,16 +443,16 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
     }
     // the last block goes on with the pass's Cholesky (C and G are complete)
     __syncthreads();
-    ss_chol<S>(kp, pass);
+    ss_chol<S>(kp, pass, sizeof(CV) == 16 ? SS_ONE_PASS : 2.0);  // q <= 1: complex64 never skips
 }
 
 // ------------------------------------------------------------ update
 // W <- W A - Q B in place (A = R^-1 of the pass, B = C R^-1); tile-major.
 template <typename CV, int S, int U>
-__global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp) {
+__global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V, long long n, KrylovPtrs kp, int pass) {
     typedef typename real_of<CV>::type R;
     DevState *st = kp.st;
-    if (st->stop) return;
+    if (st->stop || (pass == 1 && st->ss_one)) return;
     const int k = st->k;
     const int nq = k + 1;
     CV *W = V + (long long)(k + 1) * n;
@@ -754,7 +791,7 @@ template <int S> static int ss_dots_t(int prec, const void *V, long long n, cons
     return (int)cudaGetLastError();
 }
 
-template <int S> static int ss_update_t(int prec, void *V, long long n, const KrylovPtrs &kp, int sms,
+template <int S> static int ss_update_t(int prec, void *V, long long n, const KrylovPtrs &kp, int sms, int pass,
                                         cudaStream_t s) {
     const int cap = 2 * sms;  // the update writes no partial rows: the cap is occupancy only
     if (prec == 0) {
@@ -762,13 +799,13 @@ template <int S> static int ss_update_t(int prec, void *V, long long n, const Kr
         const size_t smem = sizeof(double2) * (size_t)SS_WARPS * SS_NST * U * 32;
         auto kern = k_ss_update<double2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
-        kern<<<ss_grid((n + 32 * U - 1) / (32 * U), sms, 2, cap), SS_THREADS, smem, s>>>((double2 *)V, n, kp);
+        kern<<<ss_grid((n + 32 * U - 1) / (32 * U), sms, 2, cap), SS_THREADS, smem, s>>>((double2 *)V, n, kp, pass);
     } else {
         constexpr int U = ss_u32<S>();
         const size_t smem = sizeof(float2) * (size_t)SS_WARPS * SS_NST * U * 32;
         auto kern = k_ss_update<float2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
-        kern<<<ss_grid((n + 32 * U - 1) / (32 * U), sms, 2, cap), SS_THREADS, smem, s>>>((float2 *)V, n, kp);
+        kern<<<ss_grid((n + 32 * U - 1) / (32 * U), sms, 2, cap), SS_THREADS, smem, s>>>((float2 *)V, n, kp, pass);
     }
     return (int)cudaGetLastError();
 }
@@ -805,8 +842,8 @@ int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, i
 #undef CALL
 }
 
-int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int sms, cudaStream_t s) {
-#define CALL(S_) ss_update_t<S_>(prec, V, n, kp, sms, s)
+int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int sms, int pass, cudaStream_t s) {
+#define CALL(S_) ss_update_t<S_>(prec, V, n, kp, sms, pass, s)
     SS_DISPATCH(S, CALL)
 #undef CALL
 }
