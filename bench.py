@@ -550,15 +550,20 @@ def main():
         ncu_ratio = {"dots": (889.260 + 4.386) / 889.192, "axpy": (889.234 + 55.452) / 956.301}
     else:
         ncu_ratio = {"dots": (536.904 + 4.625) / 536.871, "axpy": (536.961 + 8.369) / 570.425}
+    # the three FFT passes of one FP64 matvec at 1024^2 (the same capture's DRAM read + write of
+    # k_rows_forward, k_cols_convolve_pipe, k_rows_inverse) against the 16 n e model (268.44 MB):
+    # replayed with flushed caches, each pass reads its inputs from DRAM while the intermediate
+    # it writes is still in L2 when it ends
+    ncu_ratio["matvec"] = (25.189 + 0.139 + 50.408 + 0.139 + 50.363 + 0.473) / 268.435
     launches = max(1, dom[1].get("launches", 0))
     alg_per_launch = dom[1].get("bytes", 0.0) / launches
     traffic = ncu_ratio[dom[0]] * alg_per_launch if dom[0] in ncu_ratio and alg_per_launch > 0 else None
     roof = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1]["gbs"], 1), "peak": hbm, "unit": "GB/s",
             "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind,
             "traffic": round(traffic) if traffic else None, "traffic_unit": "bytes/launch",
-            "traffic_source": ("ncu capture of the same kernel of this solve (delayed CGS2: step 30, s-step: the "
-                               "block at k = 48), its DRAM bytes / algorithmic bytes ratio applied to this "
-                               "run's mean launch"),
+            "traffic_source": ("ncu capture of the same kernels of this solve (matvec: its three FFT passes; "
+                               "delayed CGS2: step 30; s-step: the block at k = 48), their DRAM bytes / "
+                               "algorithmic bytes ratio applied to this run's mean launch"),
             "algorithmic_bytes_per_launch": round(alg_per_launch),
             "phases": {k: {"share": round(v["ms"] / tot_ms, 4), "gbs": round(v["gbs"], 1),
                            "ms": round(v["ms"], 3)} for k, v in phases.items()}}
