@@ -557,10 +557,15 @@ def main():
     ncu_ratio["matvec"] = (25.189 + 0.139 + 50.408 + 0.139 + 50.363 + 0.473) / 268.435
     launches = max(1, dom[1].get("launches", 0))
     alg_per_launch = dom[1].get("bytes", 0.0) / launches
+    if dom[0] == "matvec":
+        # per operator application (its three FFT passes): a profile interval of an s-step block
+        # holds S of them, so the phase's mean interval is not one application
+        alg_per_launch = 16.0 * args.N * args.N * (16 if args.precision == "fp64" else 8)
     traffic = ncu_ratio[dom[0]] * alg_per_launch if dom[0] in ncu_ratio and alg_per_launch > 0 else None
     roof = {"bound": "hbm", "kernel": dom[0], "achieved": round(dom[1]["gbs"], 1), "peak": hbm, "unit": "GB/s",
             "frac": round(dom[1]["gbs"] / hbm, 4), "peak_kind": peak_kind,
-            "traffic": round(traffic) if traffic else None, "traffic_unit": "bytes/launch",
+            "traffic": round(traffic) if traffic else None,
+            "traffic_unit": "bytes/matvec (three FFT launches)" if dom[0] == "matvec" else "bytes/launch",
             "traffic_source": ("ncu capture of the same kernels of this solve (matvec: its three FFT passes; "
                                "delayed CGS2: step 30; s-step: the block at k = 48), their DRAM bytes / "
                                "algorithmic bytes ratio applied to this run's mean launch"),
