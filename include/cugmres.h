@@ -41,7 +41,7 @@ enum {
     CG_ERR_BREAKDOWN = 4,       /* Arnoldi breakdown without convergence                */
     CG_ERR_NONFINITE = 5,       /* NaN or Inf met in the input or during the iteration  */
     CG_ERR_TIMEOUT = 6,         /* opts.timeout_s elapsed                               */
-    CG_ERR_NOT_IMPLEMENTED = 7, /* size or mode this build does not support             */
+    CG_ERR_NOT_IMPLEMENTED = 7, /* size or mode the library does not support            */
     CG_ERR_NO_OPERATOR = 8,     /* cugmres_set_operator has not been called             */
     CG_ERR_OOM = 9              /* device allocation failed                             */
 };
