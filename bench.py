@@ -593,10 +593,11 @@ def main():
     # cycle return at once): the norm of b, the first residual (3 passes) and cycle set-up; per
     # delayed-CGS2 cycle 6 per step (3 matvec passes, dots, step, axpy) for restart+1 steps, then
     # back-solve, update, 3 residual passes and the cycle set-up; an s-step cycle instead runs q_0's
-    # normalisation, per block of S steps 3 S matvec passes, 2 x (dots with the Cholesky in their last
-    # block, update) and the Hessenberg/Givens kernel, then the same 6
+    # normalisation, per block of S steps 2 S + 1 matvec passes (the inverse row pass of each chained
+    # matvec but the last also runs the next forward row pass), 2 x (dots with the Cholesky in their
+    # last block, update) and the Hessenberg/Givens kernel, then the same 6
     per_dcgs2 = 6 * (args.restart + 1) + 6
-    per_ss = 1 + -(-args.restart // args.sstep) * (3 * args.sstep + 5) + 6
+    per_ss = 1 + -(-args.restart // args.sstep) * (2 * args.sstep + 6) + 6
     cyc = last["cycles"]
     per_solve = 5 + (per_dcgs2 + (cyc - 1) * per_ss if args.ortho == "sstep" else cyc * per_dcgs2)
     line["gpu_launches"] = int(args.steps * per_solve)

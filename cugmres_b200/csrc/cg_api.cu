@@ -556,7 +556,8 @@ int prof_mark(cg_ctx *c, CycleProf &cp, int phase, int iter, cudaStream_t s) {
 // off on device and move no bytes); e: element bytes of the cycle precision.
 // ss > 0: the cycle ran s-step blocks of ss steps; a MATVEC interval then holds
 // the block's ss matvecs and iter is the block's first basis index.
-int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed, int ss = 0) {
+int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed, int ss = 0,
+                 bool chained = false) {
     if (c->prof && cp.used >= 2) {
         // s-step: a block that skipped its second Gram-Schmidt pass moved no bytes in
         // its second dot and update launches (the second of each per block start k)
@@ -578,7 +579,10 @@ int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, b
                 case CG_PHASE_MATVEC: bytes = live ? 16.0 * n * e : 0.0; break;
                 case CG_PHASE_DOTS: bytes = live ? (k + 2.0) * n * e : 0.0; break;
                 case CG_PHASE_AXPY: bytes = live ? (k + (delayed ? 4.0 : 3.0)) * n * e : 0.0; break;
-                case -CG_PHASE_MATVEC - 100: bytes = live ? ss * 16.0 * n * e : 0.0; break;
+                case -CG_PHASE_MATVEC - 100:
+                    // a fused chain does not read w_1 .. w_{S-1} back: one vector less per chained matvec
+                    bytes = live ? (16.0 * ss - (chained ? ss - 1.0 : 0.0)) * n * e : 0.0;
+                    break;
                 case -CG_PHASE_DOTS - 100: bytes = live ? (k + 1.0 + ss) * n * e : 0.0; break;  // Q^H W and W^H W
                 case -CG_PHASE_AXPY - 100: bytes = live ? (k + 1.0 + 2.0 * ss) * n * e : 0.0; break;  // W <- W A - Q B
                 case -CG_PHASE_UPDATE - 100: bytes = steps_done * n * e + 2.0 * n * 16.0; break;
@@ -1229,14 +1233,20 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_LAUNCH(launch_ss_norm0(prec, c->V, n, kp, q));
         CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
         for (int b = 0; b * S < m; b++) {
+            // Newton chain w_{i+1} = (A - theta_i) w_i: the inverse row pass of each
+            // matvec but the last also runs the next one's forward row pass
+            const bool chain = !o.transpose;
             for (int i = 0; i < S; i++) {
                 VecSel vin = vk, vout = vk;
                 vin.koff = i;
                 vout.koff = i + 1;
-                CG_LAUNCH(launch_rows_forward(prec, ap, vin, nullptr, c->st, GATE_STOP, q));
+                if (i == 0 || !chain) CG_LAUNCH(launch_rows_forward(prec, ap, vin, nullptr, c->st, GATE_STOP, q));
                 CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, q));
-                CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vin, nullptr, nullptr, vout, nullptr, c->st, GATE_STOP,
-                                              q, shifts[i]));
+                if (chain && i + 1 < S)
+                    CG_LAUNCH(launch_rows_inv_fwd(prec, ap, vin, vout, c->st, GATE_STOP, q, shifts[i]));
+                else
+                    CG_LAUNCH(launch_rows_inverse(prec, 0, prec, ap, vin, nullptr, nullptr, vout, nullptr, c->st,
+                                                  GATE_STOP, q, shifts[i]));
             }
             CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, b * S, q));
             for (int pass = 0; pass < 2; pass++) {
@@ -1337,7 +1347,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_CU(cudaEventSynchronize(c->ev));
         const DevState hs = *c->st_host;
         CG_TRY(prof_collect(c, cp, nd, esz_d, hs.it - it_prev + (delayed && !ss_on ? 1 : 0), delayed && !ss_on,
-                            ss_on ? S : 0));
+                            ss_on ? S : 0, ss_on && !o.transpose));
         const int cycle_steps = hs.it - it_prev;
         it_prev = hs.it;
         // the first cycle has ended and the second begun: its Hessenberg gives the shifts

@@ -135,6 +135,10 @@ int launch_rows_forward(int prec, const MatvecArgs &a, VecSel x, const double *x
 int launch_cols_convolve(int prec, const MatvecArgs &a, const DevState *st, int gate, cudaStream_t s);
 // mode 0: y = s (1 - shift) x - conv = (A - shift) (s x);  mode 1: y = b - x + conv
 // (y may be float2 while the matvec is double2: out_prec)
+// Pass 3 of a matvec y = (A - shift) x fused with pass 1 of the next matvec on y
+// (same precision, plain operator): y is stored and c y transformed into T.
+int launch_rows_inv_fwd(int prec, const MatvecArgs &a, VecSel x, VecSel y, const DevState *st, int gate,
+                        cudaStream_t s, double2 shift);
 int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, VecSel x, const double *xscale_base,
                         const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s,
                         double2 shift = double2{0.0, 0.0});

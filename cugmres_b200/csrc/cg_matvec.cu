@@ -544,6 +544,74 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
     }
 }
 
+// Pass 3 of one matvec fused with pass 1 of the next, for chains y_{i+1} =
+// (A - shift) y_i (the s-step Newton basis): per row, the inverse transform of
+// T, the crop and y_{i+1} = (1 - shift) y_i - G c y_i stored as in
+// k_rows_inverse (MODE 0, no scaling, no contrast at the crop), then c y_{i+1}
+// zero-padded and transformed forward and stored back into the same row of T
+// as k_rows_forward would.  The cropped outputs y_{i+1}[t + p TPR] (p < E/2) are
+// already in the forward transform's input layout, so y_{i+1} is not read back
+// from HBM.  Each block owns its rows of T, which it reads before it writes.
+template <typename C, int L, typename SH>
+__global__ void __launch_bounds__(RowCfg<L, SH>::THREADS, SH::MINB)
+k_rows_inv_fwd(C *__restrict__ T, VecSel xs, VecSel ys, const typename real_of<C>::type *__restrict__ cdiag,
+               const C *__restrict__ tw, int N, const DevState *st, int gate, SysSel sy, double2 shift) {
+    typedef typename real_of<C>::type R;
+    typedef Plan<L, SH::E> P;
+    constexpr int E = P::E, TPR = P::TPR;
+    st = sys_move_bytes(st, sy.ws);
+    if (gated(st, gate)) return;
+    T += (long long)blockIdx.y * sy.T;
+    cdiag += (long long)blockIdx.y * sy.c;
+    extern __shared__ __align__(16) unsigned char smraw[];
+    const int lr = threadIdx.x / TPR, t = threadIdx.x % TPR;
+    C *sm = reinterpret_cast<C *>(smraw) + lr * P::SMEM_ELEMS;
+    const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
+    const bool live = row < N;
+    C reg[E];
+    const long long kx = sel_index(st, xs.koff);
+    const long long ky = sel_index(st, ys.koff);
+    const C *x = reinterpret_cast<const C *>(xs.base) + kx * xs.stride + (long long)blockIdx.y * xs.sys;
+    C *y = reinterpret_cast<C *>(ys.base) + ky * ys.stride + (long long)blockIdx.y * ys.sys;
+    const size_t rb = (size_t)row * (size_t)N;
+    C xv[E / 2];
+    R cv[E / 2];
+#pragma unroll
+    for (int p = 0; p < E / 2; p++) {
+        const int idx = t + p * TPR;
+        const bool ok = live && idx < N;
+        xv[p] = ok ? x[rb + idx] : czero<C>();
+        cv[p] = ok ? cdiag[rb + idx] : (R)0;
+    }
+    C *trow = T + (size_t)row * L;
+    if (live) {
+#pragma unroll
+        for (int p = 0; p < E; p++) reg[p] = trow[t + p * TPR];
+    } else {
+#pragma unroll
+        for (int p = 0; p < E; p++) reg[p] = czero<C>();
+    }
+    fft_run<L, SH::E, true, false>(reg, sm, tw, t);
+    const C sc = mk<C>((R)(1.0 - shift.x), (R)(-shift.y));
+#pragma unroll
+    for (int p = 0; p < E / 2; p++) {
+        const int idx = t + p * TPR;
+        C o = czero<C>();
+        if (live && idx < N) {
+            o = csub(cmul(xv[p], sc), reg[p]);
+            y[rb + idx] = o;
+        }
+        reg[p] = cscale(o, cv[p]);
+    }
+#pragma unroll
+    for (int p = E / 2; p < E; p++) reg[p] = czero<C>();
+    fft_run<L, SH::E, false, true>(reg, sm, tw, t);
+    if (live) {
+#pragma unroll
+        for (int p = 0; p < E; p++) trow[t + p * TPR] = reg[p];
+    }
+}
+
 // ------------------------------------------------- full transforms (setup)
 template <int L>
 __global__ void __launch_bounds__(RowCfg<L, MvV0>::THREADS)
@@ -709,6 +777,24 @@ template <typename SH0, int L> struct Passes {
         if (mode == 0) return inv_t<float2, float2, 0>(a, x, xs, b, y, npart, st, gate, s, sh);
         return inv_t<float2, float2, 1>(a, x, xs, b, y, npart, st, gate, s, sh);
     }
+    template <typename C>
+    static int inv_fwd_t(const MatvecArgs &a, VecSel x, VecSel y, const DevState *st, int gate, cudaStream_t s,
+                         double2 shift) {
+        typedef RowCfg<L, SH> Q;
+        typedef typename real_of<C>::type R;
+        const size_t smem = (size_t)Q::SMEM_ELEMS * sizeof(C);
+        auto kern = k_rows_inv_fwd<C, L, SH>;
+        int e = set_smem(kern, smem);
+        if (e) return e;
+        const int grid = (a.N + Q::RPC - 1) / Q::RPC;
+        kern<<<dim3(grid, a.nsys), Q::THREADS, smem, s>>>((C *)a.T, x, y, (const R *)a.cdiag, (const C *)a.tw, a.N, st,
+                                                            gate, sys_sel(a), shift);
+        return (int)cudaGetLastError();
+    }
+    static int inv_fwd(int prec, const MatvecArgs &a, VecSel x, VecSel y, const DevState *st, int gate,
+                       cudaStream_t s, double2 sh) {
+        return prec == 0 ? inv_fwd_t<double2>(a, x, y, st, gate, s, sh) : inv_fwd_t<float2>(a, x, y, st, gate, s, sh);
+    }
     static int rpc() { return RowCfg<L, SH>::RPC; }
 };
 
@@ -764,6 +850,12 @@ template <typename PS> struct InvF {
         return PS::inv(prec, mode, out_prec, *a, x, xs, b, y, npart, st, gate, s, sh);
     }
 };
+template <typename PS> struct InvFwdF {
+    static int run(int prec, const MatvecArgs *a, VecSel x, VecSel y, const DevState *st, int gate, cudaStream_t s,
+                   double2 sh) {
+        return PS::inv_fwd(prec, *a, x, y, st, gate, s, sh);
+    }
+};
 template <typename PS> struct RpcF {
     static int run() { return PS::rpc(); }
 };
@@ -791,6 +883,12 @@ int launch_rows_inverse(int prec, int mode, int out_prec, const MatvecArgs &a, V
                         const void *b, VecSel y, double *npart, const DevState *st, int gate, cudaStream_t s,
                         double2 shift) {
     return dispatch<InvF>(a.vinv, a.L, prec, mode, out_prec, &a, x, xs, b, y, npart, st, gate, s, shift);
+}
+
+int launch_rows_inv_fwd(int prec, const MatvecArgs &a, VecSel x, VecSel y, const DevState *st, int gate,
+                        cudaStream_t s, double2 shift) {
+    if (a.transpose || !a.cdiag) return (int)cudaErrorInvalidValue;  // chains of the plain operator only
+    return dispatch<InvFwdF>(a.vinv, a.L, prec, &a, x, y, st, gate, s, shift);
 }
 
 template <int L> static int fft2d_full_t(double2 *A, const double2 *tw, cudaStream_t s) {
