@@ -77,6 +77,10 @@ struct cg_ctx {
     cg_phase_stats stats[CG_NPHASES] = {};
     // CUDA graph of one restart cycle (replayed with one launch per cycle)
     cudaStream_t cap_stream = nullptr;  // capture only; the graph is launched on `stream`
+    // s-step cycles: the Hessenberg kernel of a block runs on a side stream next to
+    // the next block's Newton chain (fork and join events)
+    cudaStream_t side_stream = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t gexec = nullptr;
     unsigned char gkey[256] = {0};
     // learned preconditioner (flexible GMRES)
@@ -789,6 +793,9 @@ int cugmres_destroy(cg_ctx *c) {
     for (cudaEvent_t e : c->evpool) cudaEventDestroy(e);
     free_graph(c);
     if (c->cap_stream) cudaStreamDestroy(c->cap_stream);
+    if (c->side_stream) cudaStreamDestroy(c->side_stream);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CG_OK;
@@ -1232,14 +1239,30 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     auto enqueue_cycle_ss = [&](cudaStream_t q) -> int {
         CG_LAUNCH(launch_ss_norm0(prec, c->V, n, kp, q));
         CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
+        // The Hessenberg / Givens kernel of block b (one block of threads) runs on a
+        // side stream while block b + 1's Newton chain runs: the chain addresses its
+        // rows absolutely (block b starts at column b S) instead of through st->k,
+        // and the join precedes block b + 1's dot pass, the first kernel that reads
+        // what the Hessenberg kernel writes.  A cycle that the Hessenberg kernel
+        // stops lets the chain finish on rows the cycle no longer uses; every later
+        // kernel sees the stop.  Profiled cycles keep one stream (exact phase times).
+        const bool overlap = !c->prof;
+        if (overlap && !c->side_stream) {
+            CG_CU(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+            CG_CU(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+            CG_CU(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+        }
+        bool pending = false;
         for (int b = 0; b * S < m; b++) {
+            const bool last_block = (b + 1) * S >= m;
             // Newton chain w_{i+1} = (A - theta_i) w_i: the inverse row pass of each
             // matvec but the last also runs the next one's forward row pass
             const bool chain = !o.transpose;
             for (int i = 0; i < S; i++) {
                 VecSel vin = vk, vout = vk;
-                vin.koff = i;
-                vout.koff = i + 1;
+                vin.koff = b * S + i;
+                vout.koff = b * S + i + 1;
+                vin.abs = vout.abs = 1;
                 if (i == 0 || !chain) CG_LAUNCH(launch_rows_forward(prec, ap, vin, nullptr, c->st, GATE_STOP, q));
                 CG_LAUNCH(launch_cols_convolve(prec, ap, c->st, GATE_STOP, q));
                 if (chain && i + 1 < S)
@@ -1249,6 +1272,10 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
                                                   GATE_STOP, q, shifts[i]));
             }
             CG_TRY(prof_mark(c, cp, CG_PHASE_MATVEC, b * S, q));
+            if (pending) {
+                CG_CU(cudaStreamWaitEvent(q, c->ev_join, 0));
+                pending = false;
+            }
             for (int pass = 0; pass < 2; pass++) {
                 // the dot pass's last block also runs the pass's Cholesky
                 CG_LAUNCH(launch_ss_dots(prec, c->V, n, kp, S, c->sms, pass, q));
@@ -1256,8 +1283,16 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
                 CG_LAUNCH(launch_ss_update(prec, c->V, n, kp, S, c->sms, pass, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_AXPY, b * S, q));
             }
-            CG_LAUNCH(launch_ss_hess(kp, S, q));
-            CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, b * S, q));
+            if (overlap && !last_block) {
+                CG_CU(cudaEventRecord(c->ev_fork, q));
+                CG_CU(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
+                CG_LAUNCH(launch_ss_hess(kp, S, c->side_stream));
+                CG_CU(cudaEventRecord(c->ev_join, c->side_stream));
+                pending = true;
+            } else {
+                CG_LAUNCH(launch_ss_hess(kp, S, q));
+                CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, b * S, q));
+            }
         }
         CG_LAUNCH(launch_backsolve(kp, q));
         CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));

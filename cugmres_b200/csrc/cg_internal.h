@@ -127,6 +127,7 @@ struct VecSel {
     long long stride;
     int koff;
     long long sys = 0;  // elements between the vectors of consecutive systems of a bucket
+    int abs = 0;        // 1: vector koff itself; 0: vector st->k + koff (the cycle's current column)
 };
 
 // kernel launchers (cg_matvec.cu)

@@ -37,8 +37,9 @@ static __device__ __forceinline__ bool gated(const DevState *st, int gate) {
     return gate == GATE_STOP && st != nullptr && st->stop != 0;
 }
 
-static __device__ __forceinline__ long long sel_index(const DevState *st, int koff) {
-    return st ? (long long)(st->k + koff) : 0;
+static __device__ __forceinline__ long long sel_index(const DevState *st, const VecSel &v) {
+    if (v.abs) return (long long)v.koff;
+    return st ? (long long)(st->k + v.koff) : 0;
 }
 
 // E: points per thread; ROWT: target threads per row block; COLT64 / COLT32:
@@ -110,7 +111,7 @@ k_rows_forward(VecSel xs, const double *__restrict__ xscale, const typename real
     const int lr = threadIdx.x / TPR, t = threadIdx.x % TPR;
     C *sm = reinterpret_cast<C *>(smraw) + lr * P::SMEM_ELEMS;
     const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
-    const long long ks = sel_index(st, xs.koff);
+    const long long ks = sel_index(st, xs);
     const C *x = reinterpret_cast<const C *>(xs.base) + ks * xs.stride + (long long)blockIdx.y * xs.sys;
     const R s = xscale ? (R)xscale[ks] : (R)1;
     C reg[E];
@@ -416,7 +417,7 @@ k_rows_forward_pipe(VecSel xs, const double *__restrict__ xscale, const typename
     unsigned char *gb = smraw + (size_t)g * G::GROUP_BYTES;
     C *sm = reinterpret_cast<C *>(gb);
     unsigned char *slots = gb + (size_t)P::SMEM_ELEMS * sizeof(C);
-    const long long ks = sel_index(st, xs.koff);
+    const long long ks = sel_index(st, xs);
     const C *x = reinterpret_cast<const C *>(xs.base) + ks * xs.stride + (long long)blockIdx.y * xs.sys;
     const R s = xscale ? (R)xscale[ks] : (R)1;
     const int W = gridDim.x * G::G;
@@ -485,8 +486,8 @@ k_rows_inverse(const C *__restrict__ T, VecSel xs, const double *__restrict__ xs
     const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
     const bool live = row < N;
     C reg[E];
-    const long long kx = sel_index(st, xs.koff);
-    const long long ky = sel_index(st, ys.koff);
+    const long long kx = sel_index(st, xs);
+    const long long ky = sel_index(st, ys);
     const C *x = reinterpret_cast<const C *>(xs.base) + kx * xs.stride + (long long)blockIdx.y * xs.sys;
     CO *y = reinterpret_cast<CO *>(ys.base) + ky * ys.stride + (long long)blockIdx.y * ys.sys;
     const R s = xscale ? (R)xscale[kx] : (R)1;
@@ -569,8 +570,8 @@ k_rows_inv_fwd(C *__restrict__ T, VecSel xs, VecSel ys, const typename real_of<C
     const int row = blockIdx.x * RowCfg<L, SH>::RPC + lr;
     const bool live = row < N;
     C reg[E];
-    const long long kx = sel_index(st, xs.koff);
-    const long long ky = sel_index(st, ys.koff);
+    const long long kx = sel_index(st, xs);
+    const long long ky = sel_index(st, ys);
     const C *x = reinterpret_cast<const C *>(xs.base) + kx * xs.stride + (long long)blockIdx.y * xs.sys;
     C *y = reinterpret_cast<C *>(ys.base) + ky * ys.stride + (long long)blockIdx.y * ys.sys;
     const size_t rb = (size_t)row * (size_t)N;
