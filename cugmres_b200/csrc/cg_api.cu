@@ -87,6 +87,9 @@ struct cg_ctx {
     cg_fno *net = nullptr;
     double k0h = 0.0;
     void *Z = nullptr;  // preconditioned basis z_j = M(v_j), restart + 1 vectors
+    // s-step solves: the short delayed-CGS2 run that gives the Newton shifts
+    double2 *probe_x = nullptr;  // its (discarded) iterate, N^2 values
+    bool in_probe = false;       // that run is in progress (no graphs, no nested probe)
     size_t zcap_bytes = 0;
 };
 
@@ -560,6 +563,9 @@ int prof_mark(cg_ctx *c, CycleProf &cp, int phase, int iter, cudaStream_t s) {
 // off on device and move no bytes); e: element bytes of the cycle precision.
 // ss > 0: the cycle ran s-step blocks of ss steps; a MATVEC interval then holds
 // the block's ss matvecs and iter is the block's first basis index.
+// Arnoldi steps of the run that gives an s-step solve its Newton shifts
+constexpr int SS_PROBE_STEPS = 24;
+
 int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed, int ss = 0,
                  bool chained = false) {
     if (c->prof && cp.used >= 2) {
@@ -796,6 +802,7 @@ int cugmres_destroy(cg_ctx *c) {
     if (c->side_stream) cudaStreamDestroy(c->side_stream);
     if (c->ev_fork) cudaEventDestroy(c->ev_fork);
     if (c->ev_join) cudaEventDestroy(c->ev_join);
+    dfree_t(c->probe_x);
     if (c->own_stream && c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return CG_OK;
@@ -1110,6 +1117,49 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     }
     if (o.zero_x0) CG_CU(cudaMemsetAsync(xp, 0, bytes, s));
 
+    // s-step: the Newton shifts are the Leja-ordered Ritz values of a short
+    // delayed-CGS2 run from b (the outer Ritz values, which Arnoldi finds first),
+    // made before the solve and not counted in it, so every restart cycle of the
+    // solve runs s-step blocks; without enough columns the first cycle of the
+    // solve runs delayed CGS2 and gives them instead
+    double2 shifts_probe[SS_MAX];
+    bool probe_ok = false;
+    if (sstep && !c->in_probe) {
+        const int p = std::min(m, SS_PROBE_STEPS);
+        if (!c->probe_x) CG_CU(cudaMalloc((void **)&c->probe_x, bytes));
+        cg_opts po = o;
+        po.ortho = CG_ORTHO_DCGS2;
+        po.precision = CG_PREC_FP64;
+        po.restart = p;
+        po.max_iter = p;
+        po.tol = 0.0;
+        po.zero_x0 = 1;
+        po.fixed_iterations = 0;
+        po.preconditioner = CG_PRECOND_NONE;
+        po.timeout_s = 0.0;
+        cg_result pres;
+        c->in_probe = true;
+        const int pe = cugmres_solve(c, (const cg_c128 *)bp, (cg_c128 *)c->probe_x, &po, nullptr, 0, &pres);
+        c->in_probe = false;
+        if (pe != CG_OK && pe != CG_ERR_NOT_CONVERGED) return pe;
+        const int ncol = std::min(pres.iterations, p);
+        if (ncol >= S) {
+            const int ld = c->mcap + 1;
+            std::vector<double2> hm((size_t)ncol * ld);
+            CG_CU(cudaMemcpyAsync(hm.data(), c->kp.Hm, sizeof(double2) * hm.size(), cudaMemcpyDeviceToHost, s));
+            CG_CU(cudaStreamSynchronize(s));
+            const std::vector<std::complex<double>> ritz = hessenberg_eigenvalues(hm, ncol, ld);
+            bool fin = true;
+            for (const auto &z : ritz) fin = fin && std::isfinite(z.real()) && std::isfinite(z.imag());
+            if (fin) {
+                const std::vector<std::complex<double>> th = leja_points(ritz, S);
+                for (int i = 0; i < SS_MAX; i++)
+                    shifts_probe[i] = i < S ? make_double2(th[i].real(), th[i].imag()) : make_double2(0.0, 0.0);
+                probe_ok = true;
+            }
+        }
+    }
+
     // device state
     DevState h;
     memset(&h, 0, sizeof(h));
@@ -1322,10 +1372,18 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         ss_on = true;
         return CG_OK;
     };
+    if (probe_ok) {
+        for (int i = 0; i < SS_MAX; i++) shifts[i] = shifts_probe[i];
+        // the Hessenberg kernel reads them from the scratch (offset of SsLayout::Th)
+        const long long M1 = c->mcap + 1;
+        const long long th_off = 3 * M1 * SS_MAX + 3 * SS_MAX * SS_MAX;
+        CG_CU(cudaMemcpyAsync(kp.ss + th_off, shifts, sizeof(double2) * SS_MAX, cudaMemcpyHostToDevice, s));
+        ss_on = true;
+    }
     // Graph replay of [cycle + next residual/decisions] when nothing in it
     // changes between cycles (not while profiling, not with the network).
     // (flexible GMRES: plain cycles after the probe only)
-    const bool graphs = !c->prof && graphs_enabled();
+    const bool graphs = !c->prof && !c->in_probe && graphs_enabled();
     unsigned char key[256];
     // key of the cycle about to be replayed (the scheme can change between cycles)
     auto make_key = [&]() {
