@@ -33,11 +33,12 @@ budget-capped solve (max_iter / restart).  Warm-up steps run a 5-step sample.
 --profile-case: a fixed launch sequence for profiler captures (no timing, no
 JSON): three FP64 and three FP32 matvecs of the 1024^2 system, then one solve of
 exactly --case-steps Arnoldi steps (tolerance 1e-14, so it never stops early) in
-cycles of min(--restart, --case-steps) steps.  Its first cycle is delayed CGS2:
-per step [k_rows_forward, k_cols_convolve, k_rows_inverse, k_dots2, k_dcgs2_step,
-k_axpy2], so `ncu -k regex:k_dots2 -s 30 -c 1` picks the dot pass of step 30; with
---case-steps 200 the second cycle runs s-step blocks (--sstep), whose passes are
-k_ss_dots and k_ss_update.
+cycles of min(--restart, --case-steps) steps.  With --ortho dcgs2 every step is
+[k_rows_forward, k_cols_convolve, k_rows_inverse, k_dots2, k_dcgs2_step, k_axpy2],
+so `ncu -k regex:k_dots2 -s 30 -c 1` picks the dot pass of step 30; with the
+default s-step scheme a 24-step delayed-CGS2 run gives the shifts first, then
+every cycle runs s-step blocks (--sstep), whose passes are k_ss_dots and
+k_ss_update.
 """
 import argparse
 import json
@@ -69,7 +70,7 @@ def parse():
     ap.add_argument("--max-iter", type=int, default=1000)
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--ortho", default="sstep", choices=["sstep", "dcgs2", "cgs2"],
-                    help="Arnoldi scheme of the timed solve (s-step blocks after a first delayed-CGS2 cycle)")
+                    help="Arnoldi scheme of the timed solve (s-step blocks, shifts from a short delayed-CGS2 run)")
     ap.add_argument("--sstep", type=int, default=4, help="steps per s-step block")
     ap.add_argument("--inner-tol", type=float, default=1e-5, help="mixed: a complex64 cycle ends when its estimate fell by this")
     ap.add_argument("--profile-case", action="store_true", help="fixed launch sequence for profiler captures")

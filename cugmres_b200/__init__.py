@@ -185,8 +185,8 @@ class Solver:
         preconditioner="learned": flexible GMRES with the attached network
         (learned_x0: also start from x0 = M(b) when x0 is None).
         transpose=True solves A^T x = b (the adjoint system of the gradient path).
-        ortho="sstep": s-step Arnoldi, `sstep` (2, 4 or 8) steps per block after a
-        first delayed-CGS2 cycle that gives the Newton shifts."""
+        ortho="sstep": s-step Arnoldi, `sstep` (2, 4 or 8) steps per block; the
+        Newton shifts come from a 24-step delayed-CGS2 run made before the solve."""
         o = _lib.CgOpts()
         _lib.lib().cugmres_default_opts(ctypes.byref(o))
         o.restart = int(restart)

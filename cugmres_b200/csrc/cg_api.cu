@@ -1070,7 +1070,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         (o.preconditioner != CG_PRECOND_NONE && o.preconditioner != CG_PRECOND_LEARNED))
         return CG_ERR_INVALID;
     const bool learned = o.preconditioner == CG_PRECOND_LEARNED;
-    // s-step Arnoldi: S steps per block after a first delayed-CGS2 cycle (its Ritz values are the shifts)
+    // s-step Arnoldi: S steps per block; the shifts are Ritz values of a short delayed-CGS2 run
     const bool sstep = o.ortho == CG_ORTHO_SSTEP;
     const int S = sstep ? (o.sstep > 0 ? o.sstep : 4) : 0;
     if (sstep && (!sstep_supported(S) || learned || o.fixed_iterations || o.givens != CG_GIVENS_UNITARY ||
@@ -1279,7 +1279,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, q));
         return CG_OK;
     };
-    // s-step cycles (after the first, delayed-CGS2 cycle): ceil(m / S) blocks of
+    // s-step cycles: ceil(m / S) blocks of
     // S shifted matvecs, two block Gram-Schmidt passes and the Hessenberg /
     // Givens kernel, then the back-solve and the update
     bool ss_on = false;
@@ -1350,9 +1350,9 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         CG_TRY(prof_mark(c, cp, CG_PHASE_UPDATE, -1, q));
         return CG_OK;
     };
-    // The first cycle's Hessenberg (delayed CGS2 keeps it unrotated in Hm)
-    // gives the shifts: Leja-ordered Ritz values.  Returns false (s-step stays
-    // off) when the cycle had fewer than S columns.
+    // Fallback when the probe before the solve gave no shifts: the solve's first
+    // cycle runs delayed CGS2 and its Hessenberg (unrotated in Hm) gives them,
+    // Leja-ordered Ritz values; s-step stays off when that cycle had fewer than S columns.
     auto setup_shifts = [&](int ncol1) -> int {
         if (ncol1 < S) return CG_OK;
         const int ld = c->mcap + 1;
@@ -1491,7 +1491,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             if (d != delayed) CG_LAUNCH(launch_set_ortho(kp, d ? 0 : 1, s));
             delayed = d;
         }
-        // s-step, first cycle: delayed CGS2 for the shifts, at most 64 steps when the
+        // s-step without probe shifts, first cycle: delayed CGS2 for the shifts, at most 64 steps when the
         // restart is long (an unrestarted solve would otherwise spend its whole
         // budget before the s-step blocks start); restarts up to 128 keep their
         // full first cycle, so GMRES(m) iterates are those of the other schemes

@@ -64,8 +64,9 @@ enum {
     CG_ORTHO_DCGS2 = 0, /* classical Gram-Schmidt, reorthogonalisation delayed one step: 2 passes over the basis per step */
     CG_ORTHO_CGS2 = 1,  /* classical Gram-Schmidt with one immediate reorthogonalisation: 4 passes per step            */
     CG_ORTHO_SSTEP = 2  /* s-step: opts->sstep Arnoldi steps per block (a Newton basis of sstep matvecs, block
-                           Gram-Schmidt twice with Pythagorean Cholesky): 4 passes over the basis per block; the
-                           first cycle runs CG_ORTHO_DCGS2 and gives the Newton shifts (its Ritz values)        */
+                           Gram-Schmidt with Pythagorean Cholesky, the second pass only where the first
+                           cancelled): 2 to 4 passes over the basis per block; the Newton shifts are the Ritz
+                           values of a 24-step CG_ORTHO_DCGS2 run from b made before the solve               */
 };
 
 /* Green's-function constructions for cugmres_green_block */

@@ -41,8 +41,9 @@ def test_sstep_converges_like_oracle(solver, oracle, S):
 
 
 def test_sstep_fixed_budget_iterates_match_oracle(solver, oracle):
-    """Three whole GMRES(20) cycles (the first delayed CGS2, then s-step): the
-    iterate and the residual estimates agree with the oracle's MGS GMRES."""
+    """Three whole GMRES(20) cycles of s-step blocks (shifts from the 20-step
+    delayed-CGS2 probe): the iterate and the residual estimates agree with the
+    oracle's MGS GMRES."""
     N = 48
     pr = P.helmholtz(N, 2.25, seed=21)
     solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
