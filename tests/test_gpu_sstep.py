@@ -112,3 +112,41 @@ def test_sstep_rejects_unsupported_options(solver):
     for kw in (dict(sstep=3), dict(sstep=8, restart=4), dict(givens="reference"), dict(fixed_iterations=True)):
         with pytest.raises(cg.CugmresError):
             solver.solve(pr["b"], ortho="sstep", **{"restart": 20, **kw})
+
+
+def test_sstep_partial_last_block_and_initial_guess(solver, oracle):
+    """GMRES(30) with blocks of 4 (each cycle ends with a block of 2 columns) from
+    a non-zero x0: the oracle's iterate after three whole cycles and the same
+    converged solve."""
+    N = 64
+    pr = P.helmholtz(N, 2.25, seed=9)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    chi = pr["chi"] * pr["chi_scale"]
+    x0 = 0.5 * pr["b"]
+    x, info = solver.solve(pr["b"], x0=x0, restart=30, max_iter=90, tol=0.0, ortho="sstep", sstep=4)
+    o = oracle.gmres(gh, chi, pr["b"], x0=x0, restart=30, maxiter=90, tol=0.0)
+    assert info["iterations"] == o["iterations"] == 90 and info["cycles"] == 3
+    assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
+    x, info = solver.solve(pr["b"], x0=x0, restart=30, max_iter=3000, tol=1e-10, ortho="sstep", sstep=4)
+    o = oracle.gmres(gh, chi, pr["b"], x0=x0, restart=30, maxiter=3000, tol=1e-10)
+    assert info["status"] == 0 and abs(info["iterations"] - o["iterations"]) <= 2
+    assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
+
+
+def test_sstep_transposed_operator(solver, oracle):
+    """A^T x = b (the gradient system) by s-step blocks, whose Newton chain then
+    runs the three row passes separately: the transposed residual reaches 1e-10
+    and the solution is the delayed-CGS2 one."""
+    N = 48
+    pr = P.helmholtz(N, 4.0, seed=4)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    chi = pr["chi"] * pr["chi_scale"]
+    x, info = solver.solve(pr["b"], restart=40, max_iter=4000, tol=1e-10, ortho="sstep", sstep=4, transpose=True)
+    xd, idd = solver.solve(pr["b"], restart=40, max_iter=4000, tol=1e-10, transpose=True)
+    assert info["status"] == 0 and idd["status"] == 0
+    r = pr["b"] - oracle.matvec_transpose(gh, chi, x)
+    assert np.linalg.norm(r) / np.linalg.norm(pr["b"]) <= 1.1e-10
+    assert abs(info["iterations"] - idd["iterations"]) <= 2, (info["iterations"], idd["iterations"])
+    assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-8
