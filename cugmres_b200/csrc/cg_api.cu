@@ -89,6 +89,7 @@ struct cg_ctx {
     void *Z = nullptr;  // preconditioned basis z_j = M(v_j), restart + 1 vectors
     // s-step solves: the short delayed-CGS2 run that gives the Newton shifts
     double2 *probe_x = nullptr;  // its (discarded) iterate, N^2 values
+    size_t probe_cap_bytes = 0;  // allocated bytes of probe_x (the grid side can change between solves)
     bool in_probe = false;       // that run is in progress (no graphs, no nested probe)
     size_t zcap_bytes = 0;
 };
@@ -563,7 +564,10 @@ int prof_mark(cg_ctx *c, CycleProf &cp, int phase, int iter, cudaStream_t s) {
 // off on device and move no bytes); e: element bytes of the cycle precision.
 // ss > 0: the cycle ran s-step blocks of ss steps; a MATVEC interval then holds
 // the block's ss matvecs and iter is the block's first basis index.
-// Arnoldi steps of the run that gives an s-step solve its Newton shifts
+// Arnoldi steps of the run that gives an s-step solve its Newton shifts.  Measured on
+// the 1024^2 GMRES(100) solve (s, S = 4 / 8): 8 steps 0.175 / 0.217, 12 steps
+// 0.166 / 0.202, 16 steps 0.162 / 0.185, 24 steps 0.164 / 0.178 (shorter runs give
+// rougher shifts, worse-conditioned Newton blocks and more second passes).
 constexpr int SS_PROBE_STEPS = 24;
 
 int prof_collect(cg_ctx *c, CycleProf &cp, double n, double e, int steps_done, bool delayed, int ss = 0,
@@ -1126,7 +1130,12 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     bool probe_ok = false;
     if (sstep && !c->in_probe) {
         const int p = std::min(m, SS_PROBE_STEPS);
-        if (!c->probe_x) CG_CU(cudaMalloc((void **)&c->probe_x, bytes));
+        if (c->probe_cap_bytes < bytes) {
+            dfree_t(c->probe_x);
+            c->probe_cap_bytes = 0;
+            CG_CU(cudaMalloc((void **)&c->probe_x, bytes));
+            c->probe_cap_bytes = bytes;
+        }
         cg_opts po = o;
         po.ortho = CG_ORTHO_DCGS2;
         po.precision = CG_PREC_FP64;

@@ -150,3 +150,17 @@ def test_sstep_transposed_operator(solver, oracle):
     assert np.linalg.norm(r) / np.linalg.norm(pr["b"]) <= 1.1e-10
     assert abs(info["iterations"] - idd["iterations"]) <= 2, (info["iterations"], idd["iterations"])
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-8
+
+
+def test_sstep_context_reused_across_grid_sizes(solver, oracle):
+    """One context solves a 32^2 and then a larger 96^2 system with s-step blocks:
+    the buffers of the shift probe follow the grid size (each solve matches the
+    oracle)."""
+    for N in (32, 96):
+        pr = P.helmholtz(N, 2.25, seed=N)
+        solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+        x, info = solver.solve(pr["b"], restart=40, max_iter=3000, tol=1e-10, ortho="sstep", sstep=4)
+        o = oracle.gmres(oracle.spectrum(pr["g_block"], solver.L), pr["chi"] * pr["chi_scale"], pr["b"], restart=40,
+                         maxiter=3000, tol=1e-10)
+        assert info["status"] == 0 and abs(info["iterations"] - o["iterations"]) <= 2
+        assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
