@@ -56,6 +56,7 @@ def sweep_stats(records, wall_s):
     conv = sum(1 for r in records if r["status"] == 0)
     return {"systems": len(records), "converged": conv, "wall_s": wall_s,
             "solves_per_s": len(records) / wall_s if wall_s > 0 else None,
+            "converged_per_s": conv / wall_s if wall_s > 0 else None,
             "latency_p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
             "latency_p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
             "iterations_total": int(sum(r["iterations"] for r in records))}
