@@ -303,12 +303,15 @@ def side_measurements(args, stream):
         s.set_operator(prn["g_block"], prn["chi"], prn["chi_scale"])
         bn = torch.from_numpy(prn["b"]).cuda()
         xref = tight_reference(s, bn, restart=R, max_iter=2 * R)
-        for prec in ("fp64", "mixed"):
-            kwn = dict(restart=R, max_iter=3 * R, tol=args.tol, precision=prec, inner_tol=1e-7)
+        # delayed CGS2 in FP64 and mixed precision, and s-step blocks of 4 in FP64
+        # (shifts refreshed every 100 steps of the long cycle)
+        for name, prec, extra in (("fp64", "fp64", {}), ("mixed", "mixed", {}),
+                                  ("sstep_fp64", "fp64", dict(ortho="sstep", sstep=4))):
+            kwn = dict(restart=R, max_iter=3 * R, tol=args.tol, precision=prec, inner_tol=1e-7, **extra)
             for _ in range(reps):  # warm-up solve (the 512^2 ones are timed cold: graphs are built in their first cycle)
                 s.solve(bn, **kwn)
             ms, info, x = timed_solves(s, bn, kwn, 1, stream)
-            out[f"time_to_tol_{N}_unrestarted_{prec}"] = {
+            out[f"time_to_tol_{N}_unrestarted_{name}"] = {
                 "s": ms / 1e3, "steps": info["iterations"], "cycles": info["cycles"], "status": info["status_text"],
                 "rel_residual_true": info["rel_residual_true"], "err_vs_fp64_tol1e-13": rel_err(x, xref)}
         s.close()

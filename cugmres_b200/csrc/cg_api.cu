@@ -1294,10 +1294,28 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
     bool ss_on = false;
     double2 shifts[SS_MAX];
     for (int i = 0; i < SS_MAX; i++) shifts[i] = make_double2(0.0, 0.0);
+    // Long s-step cycles (restart above SS_REFRESH_MIN) are enqueued in segments
+    // of SS_REFRESH_STEPS steps; after each, the Newton shifts become the
+    // Leja-ordered Ritz values of the trailing SS_REFRESH_WINDOW columns of H.
+    // The probe's shifts follow the outer spectrum that Arnoldi finds first; a
+    // basis of thousands of vectors has left it behind, and with those shifts a
+    // block's later vectors kept almost nothing outside the basis, so its
+    // Cholesky failed and the cycle restarted (512^2, eps_r = 4, restart 4500:
+    // 7 cycles and 12 000 steps without reaching 1e-10).  With the refresh the
+    // first cycle runs 3981 steps (delayed CGS2: 3979) and a second of 1663
+    // removes the 1e-8 its Hessenberg reconstruction left.  Each cycle starts
+    // again from the probe's shifts.
+    constexpr int SS_REFRESH_MIN = 256, SS_REFRESH_STEPS = 100, SS_REFRESH_WINDOW = 32;
+    const bool ss_segments = m > SS_REFRESH_MIN;
+    const int ss_nblk = S > 0 ? (m + S - 1) / S : 0;  // blocks of a full s-step cycle
+    double2 shifts0[SS_MAX];
+    for (int i = 0; i < SS_MAX; i++) shifts0[i] = make_double2(0.0, 0.0);
     const int nss = sstep_blocks(c->sms, n);
-    auto enqueue_cycle_ss = [&](cudaStream_t q) -> int {
-        CG_LAUNCH(launch_ss_norm0(prec, c->V, n, kp, q));
-        CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
+    auto enqueue_cycle_ss = [&](cudaStream_t q, int b0, int b1, bool finish) -> int {
+        if (b0 == 0) {
+            CG_LAUNCH(launch_ss_norm0(prec, c->V, n, kp, q));
+            CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
+        }
         // The Hessenberg / Givens kernel of block b (one block of threads) runs on a
         // side stream while block b + 1's Newton chain runs: the chain addresses its
         // rows absolutely (block b starts at column b S) instead of through st->k,
@@ -1312,8 +1330,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             CG_CU(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
         }
         bool pending = false;
-        for (int b = 0; b * S < m; b++) {
-            const bool last_block = (b + 1) * S >= m;
+        for (int b = b0; b < b1 && b * S < m; b++) {
+            const bool last_block = (b + 1) * S >= m || b + 1 >= b1;
             // Newton chain w_{i+1} = (A - theta_i) w_i: the inverse row pass of each
             // matvec but the last also runs the next one's forward row pass
             const bool chain = !o.transpose;
@@ -1345,14 +1363,15 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             if (overlap && !last_block) {
                 CG_CU(cudaEventRecord(c->ev_fork, q));
                 CG_CU(cudaStreamWaitEvent(c->side_stream, c->ev_fork, 0));
-                CG_LAUNCH(launch_ss_hess(kp, S, c->side_stream));
+                CG_LAUNCH(launch_ss_hess(kp, S, b * S, c->side_stream));
                 CG_CU(cudaEventRecord(c->ev_join, c->side_stream));
                 pending = true;
             } else {
-                CG_LAUNCH(launch_ss_hess(kp, S, q));
+                CG_LAUNCH(launch_ss_hess(kp, S, b * S, q));
                 CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, b * S, q));
             }
         }
+        if (!finish) return CG_OK;
         CG_LAUNCH(launch_backsolve(kp, q));
         CG_TRY(prof_mark(c, cp, CG_PHASE_SMALL, -1, q));
         CG_LAUNCH(launch_axpy(prec, 0, c->V, n, kp, kp.y, 1.0, NJ_NCOL, xs, 0, 1, nax, GATE_NONE, q));
@@ -1373,6 +1392,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             if (!std::isfinite(z.real()) || !std::isfinite(z.imag())) return CG_OK;
         const std::vector<std::complex<double>> th = leja_points(ritz, S);
         for (int i = 0; i < S; i++) shifts[i] = make_double2(th[i].real(), th[i].imag());
+        for (int i = 0; i < SS_MAX; i++) shifts0[i] = shifts[i];
         // the Hessenberg kernel reads them from the scratch (offset of SsLayout::Th)
         const long long M1 = c->mcap + 1;
         const long long th_off = 3 * M1 * SS_MAX + 3 * SS_MAX * SS_MAX;
@@ -1382,7 +1402,7 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
         return CG_OK;
     };
     if (probe_ok) {
-        for (int i = 0; i < SS_MAX; i++) shifts[i] = shifts_probe[i];
+        for (int i = 0; i < SS_MAX; i++) shifts[i] = shifts0[i] = shifts_probe[i];
         // the Hessenberg kernel reads them from the scratch (offset of SsLayout::Th)
         const long long M1 = c->mcap + 1;
         const long long th_off = 3 * M1 * SS_MAX + 3 * SS_MAX * SS_MAX;
@@ -1421,7 +1441,8 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             if (!c->cap_stream) CG_CU(cudaStreamCreateWithFlags(&c->cap_stream, cudaStreamNonBlocking));
             cudaGraph_t g = nullptr;
             CG_CU(cudaStreamBeginCapture(c->cap_stream, cudaStreamCaptureModeThreadLocal));
-            int e1 = ss_on ? enqueue_cycle_ss(c->cap_stream) : enqueue_cycle(m + (delayed ? 1 : 0), c->cap_stream);
+            int e1 = ss_on ? enqueue_cycle_ss(c->cap_stream, 0, ss_nblk, true)
+                           : enqueue_cycle(m + (delayed ? 1 : 0), c->cap_stream);
             int e2 = e1 == CG_OK ? enqueue_begin(c->cap_stream) : e1;
             cudaError_t ce = cudaStreamEndCapture(c->cap_stream, &g);
             if (e2 != CG_OK || ce != cudaSuccess) {
@@ -1510,10 +1531,45 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
             CG_TRY(enqueue_cycle(len + 1, s));
             CG_TRY(prof_mark(c, cp, -1, -1, s));
             CG_TRY(enqueue_begin(s));
-        } else if (graphs && !use_prec && !(learned && rate_plain < 0.0)) {
+        } else if (graphs && !use_prec && !(learned && rate_plain < 0.0) && !(ss_on && ss_segments)) {
             CG_TRY(launch_cycle_graph());
+        } else if (ss_on && ss_segments) {
+            const long long th_off = 3 * (long long)(c->mcap + 1) * SS_MAX + 3 * SS_MAX * SS_MAX;  // SsLayout::Th
+            for (int i = 0; i < SS_MAX; i++) shifts[i] = shifts0[i];
+            CG_CU(cudaMemcpyAsync(kp.ss + th_off, shifts, sizeof(double2) * SS_MAX, cudaMemcpyHostToDevice, s));
+            const int segb = (SS_REFRESH_STEPS + S - 1) / S;
+            int b0 = 0;
+            for (;;) {
+                CG_TRY(enqueue_cycle_ss(s, b0, b0 + segb, false));
+                b0 += segb;
+                if (b0 >= ss_nblk) break;
+                DevState sd;
+                CG_CU(cudaMemcpyAsync(&sd, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
+                CG_CU(cudaStreamSynchronize(s));
+                if (sd.stop) break;
+                const int k = sd.k, W = std::min(SS_REFRESH_WINDOW, k);
+                if (W >= S) {
+                    const int ld = c->mcap + 1;
+                    std::vector<double2> hw((size_t)W * W);
+                    CG_CU(cudaMemcpy2DAsync(hw.data(), sizeof(double2) * W, kp.Hm + (size_t)(k - W) * ld + (k - W),
+                                            sizeof(double2) * ld, sizeof(double2) * W, W, cudaMemcpyDeviceToHost, s));
+                    CG_CU(cudaStreamSynchronize(s));
+                    const std::vector<std::complex<double>> ritz = hessenberg_eigenvalues(hw, W, W);
+                    bool fin = true;
+                    for (const auto &z : ritz) fin = fin && std::isfinite(z.real()) && std::isfinite(z.imag());
+                    if (fin) {
+                        const std::vector<std::complex<double>> th = leja_points(ritz, S);
+                        for (int i = 0; i < S; i++) shifts[i] = make_double2(th[i].real(), th[i].imag());
+                        // the next segment's Hessenberg kernels read them there
+                        CG_CU(cudaMemcpyAsync(kp.ss + th_off, shifts, sizeof(double2) * SS_MAX, cudaMemcpyHostToDevice, s));
+                    }
+                }
+            }
+            CG_TRY(enqueue_cycle_ss(s, ss_nblk, ss_nblk, true));  // the back-solve and the update
+            CG_TRY(prof_mark(c, cp, -1, -1, s));
+            CG_TRY(enqueue_begin(s));
         } else if (ss_on) {
-            CG_TRY(enqueue_cycle_ss(s));
+            CG_TRY(enqueue_cycle_ss(s, 0, ss_nblk, true));
             CG_TRY(prof_mark(c, cp, -1, -1, s));
             CG_TRY(enqueue_begin(s));
         } else {

@@ -203,7 +203,9 @@ int launch_ss_norm0(int prec, void *V, long long n, const KrylovPtrs &kp, cudaSt
 int launch_ss_dots(int prec, const void *V, long long n, const KrylovPtrs &kp, int S, int sms, int pass,
                    cudaStream_t s);
 int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S, int sms, int pass, cudaStream_t s);
-int launch_ss_hess(const KrylovPtrs &kp, int S, cudaStream_t s);
+// k: the basis size the block starts at (b S), which picks the many-block
+// H_old C'' product for long cycles
+int launch_ss_hess(const KrylovPtrs &kp, int S, int k, cudaStream_t s);
 int launch_norm2(int prec, const void *v, long long n, double *npart, unsigned int *counter, double *out, int nblk,
                  cudaStream_t s);
 int launch_convert(int from_prec, int to_prec, const void *src, void *dst, long long n, cudaStream_t s);

@@ -73,7 +73,7 @@ template <int N> static __device__ __forceinline__ void cp_async_wait() {
 
 // offsets (in double2) of the s-step scratch arrays in kp.ss; M1 = mcap + 1
 struct SsLayout {
-    long long C, Ct, Bc, G, Rt, Ai, Th, Mh, Sk, end;
+    long long C, Ct, Bc, G, Rt, Ai, Th, Mh, Sk, Ph, end;
     __host__ __device__ explicit SsLayout(int mcap) {
         const long long M1 = mcap + 1;
         C = 0;
@@ -85,7 +85,8 @@ struct SsLayout {
         Th = Ai + SS_MAX * SS_MAX;
         Mh = Th + SS_MAX;                        // [(mcap + SS_MAX + 1) * SS_MAX] work rows of k_ss_hess
         Sk = Mh + (M1 + SS_MAX) * SS_MAX;        // [M1] per block of the cycle: .x = 1 if its second pass was skipped
-        end = Sk + M1;
+        Ph = Sk + M1;                            // [M1][SS_MAX] rows of H_old C'' from k_ss_hprod (long cycles)
+        end = Ph + M1 * SS_MAX;
     }
 };
 
@@ -577,10 +578,56 @@ __global__ void __launch_bounds__(SS_THREADS, 2) k_ss_update(CV *__restrict__ V,
 }
 
 // ------------------------------------------------------------ Hessenberg + Givens
+// Row r of H_old C'' (r = 0..k): sum over the columns l = max(r-1, 0)..k-1 of
+// the upper Hessenberg H_old of H[r][l] Ct[l][j], j < S - 1, lanes strided over
+// l and a fixed-order warp sum.  Shared by the one-block Hessenberg kernel and
+// the many-block product that long cycles launch before it (the same sum in
+// the same order, so both give the same bits).
+template <int S>
+__device__ __forceinline__ void ss_hrow(const KrylovPtrs &kp, const double2 *Ct, int r, int k, int ld, int lane,
+                                        double (&hs)[2 * (S - 1) > 0 ? 2 * (S - 1) : 1]) {
+#pragma unroll
+    for (int q = 0; q < 2 * (S - 1); q++) hs[q] = 0.0;
+    for (int l = (r > 0 ? r - 1 : 0) + lane; l < k; l += 32) {
+        const double2 hv = kp.Hm[(size_t)r * ld + l];
+#pragma unroll
+        for (int jj = 0; jj < S - 1; jj++) {
+            const double2 p = cmul(hv, Ct[l * SS_MAX + jj]);
+            hs[2 * jj] += p.x;
+            hs[2 * jj + 1] += p.y;
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 2 * (S - 1); q++) hs[q] = warp_sum(hs[q]);
+}
+
+// H_old C'' over many blocks, one warp per row, into the Ph rows: at a basis of
+// k vectors the product reads k^2 / 2 entries of H (128 MB at k = 4000), which
+// one block of threads would stream at a single SM's bandwidth.
+template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hprod(KrylovPtrs kp) {
+    DevState *st = kp.st;
+    if (st->stop) return;
+    const int k = st->k;
+    const int ld = kp.mcap + 1;
+    const SsLayout L(kp.mcap);
+    const double2 *Ct = kp.ss + L.Ct;
+    double2 *P = kp.ss + L.Ph;
+    const int lane = threadIdx.x & 31;
+    const int nw = gridDim.x * SS_WARPS;
+    for (int r = blockIdx.x * SS_WARPS + (threadIdx.x >> 5); r <= k; r += nw) {
+        double hs[2 * (S - 1) > 0 ? 2 * (S - 1) : 1];
+        ss_hrow<S>(kp, Ct, r, k, ld, lane, hs);
+#pragma unroll
+        for (int jj = 0; jj < S - 1; jj++)
+            if (lane == jj) P[(size_t)r * SS_MAX + jj] = make_double2(hs[2 * jj], hs[2 * jj + 1]);
+    }
+}
+
 // One block: the S new columns k..k+S-1 of H (rows 0..k+S) from the block's
 // coefficients (Ct, Rt), the shifts and the earlier columns of H, then their
-// Givens rotations, residual estimates and the stop decision.
-template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovPtrs kp, int m_in_smem) {
+// Givens rotations, residual estimates and the stop decision.  p_ready: the
+// rows of H_old C'' are in Ph (k_ss_hprod ran first).
+template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovPtrs kp, int m_in_smem, int p_ready) {
     DevState *st = kp.st;
     if (st->stop) return;
     const int k = st->k;
@@ -606,22 +653,23 @@ template <int S> __global__ void __launch_bounds__(SS_THREADS) k_ss_hess(KrylovP
     // M = Rall T - [H_old C''; 0]: one warp per row r, its lanes over the
     // columns l of H_old (upper Hessenberg: l >= r - 1), fixed-order warp sums
     const int warp = tid >> 5, lane = tid & 31;
+    const double2 *P = kp.ss + L.Ph;
     for (int r = warp; r < nr; r += SS_WARPS) {
         double hs[2 * (S - 1) > 0 ? 2 * (S - 1) : 1];
 #pragma unroll
         for (int q = 0; q < 2 * (S - 1); q++) hs[q] = 0.0;
-        if (r <= k)
-            for (int l = (r > 0 ? r - 1 : 0) + lane; l < k; l += 32) {
-                const double2 hv = kp.Hm[(size_t)r * ld + l];
+        if (r <= k) {
+            if (p_ready) {
 #pragma unroll
                 for (int jj = 0; jj < S - 1; jj++) {
-                    const double2 p = cmul(hv, Ct[l * SS_MAX + jj]);
-                    hs[2 * jj] += p.x;
-                    hs[2 * jj + 1] += p.y;
+                    const double2 pv = P[(size_t)r * SS_MAX + jj];
+                    hs[2 * jj] = pv.x;
+                    hs[2 * jj + 1] = pv.y;
                 }
+            } else {
+                ss_hrow<S>(kp, Ct, r, k, ld, lane, hs);
             }
-#pragma unroll
-        for (int q = 0; q < 2 * (S - 1); q++) hs[q] = warp_sum(hs[q]);
+        }
 #pragma unroll
         for (int j = 0; j < S; j++)
             if (lane == j) {
@@ -810,10 +858,21 @@ template <int S> static int ss_update_t(int prec, void *V, long long n, const Kr
     return (int)cudaGetLastError();
 }
 
-template <int S> static int ss_hess_t(const KrylovPtrs &kp, cudaStream_t s) {
+// Blocks from this basis size on get the many-block H_old C'' first: below it
+// the one-block product costs less than the extra launch (restart-100 cycles
+// never reach it).
+static constexpr int SS_HPROD_MIN = 512;
+
+template <int S> static int ss_hess_t(const KrylovPtrs &kp, int k, cudaStream_t s) {
     const size_t smem = sizeof(double2) * (size_t)(kp.mcap + SS_MAX + 1) * S;
     const bool in_smem = smem <= 48 * 1024;
-    k_ss_hess<S><<<1, SS_THREADS, in_smem ? smem : 0, s>>>(kp, in_smem ? 1 : 0);
+    const bool many = k >= SS_HPROD_MIN;
+    if (many) {
+        int g = (k + 1 + SS_WARPS - 1) / SS_WARPS;  // one warp per row
+        if (g > 1184) g = 1184;
+        k_ss_hprod<S><<<g, SS_THREADS, 0, s>>>(kp);
+    }
+    k_ss_hess<S><<<1, SS_THREADS, in_smem ? smem : 0, s>>>(kp, in_smem ? 1 : 0, many ? 1 : 0);
     return (int)cudaGetLastError();
 }
 
@@ -848,8 +907,8 @@ int launch_ss_update(int prec, void *V, long long n, const KrylovPtrs &kp, int S
 #undef CALL
 }
 
-int launch_ss_hess(const KrylovPtrs &kp, int S, cudaStream_t s) {
-#define CALL(S_) ss_hess_t<S_>(kp, s)
+int launch_ss_hess(const KrylovPtrs &kp, int S, int k, cudaStream_t s) {
+#define CALL(S_) ss_hess_t<S_>(kp, k, s)
     SS_DISPATCH(S, CALL)
 #undef CALL
 }

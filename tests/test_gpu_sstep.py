@@ -164,3 +164,43 @@ def test_sstep_context_reused_across_grid_sizes(solver, oracle):
                          maxiter=3000, tol=1e-10)
         assert info["status"] == 0 and abs(info["iterations"] - o["iterations"]) <= 2
         assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-9
+
+
+def test_sstep_long_cycle_refreshed_shifts_match_oracle(solver, oracle):
+    """A cycle longer than 256 steps is run in segments of 100, each after the
+    first with Newton shifts from the Ritz values of the latest Hessenberg
+    columns: 300 steps of one GMRES(400) cycle on 128^2 (three refreshes) give
+    the oracle's iterate and residual history."""
+    N = 128
+    pr = P.helmholtz(N, 4.0, seed=0)
+    solver.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+    x, info = solver.solve(pr["b"], restart=400, max_iter=300, tol=0.0, ortho="sstep", sstep=4)
+    gh = oracle.spectrum(pr["g_block"], solver.L)
+    o = oracle.gmres(gh, pr["chi"] * pr["chi_scale"], pr["b"], restart=400, maxiter=300, tol=0.0)
+    assert info["iterations"] == o["iterations"] == 300 and info["cycles"] == o["cycles"] == 1
+    assert np.linalg.norm(x - o["x"]) / np.linalg.norm(o["x"]) < 1e-8
+    # The residual falls from 0.7 to 2e-11 in these 300 steps, so the late
+    # Newton blocks keep little outside the basis and their rounding moves the
+    # Krylov space slightly: measured, the estimates differ by at most 2.8e-2
+    # (relative, step 247, estimate 3.4e-5) and meet again at the end
+    hs, ho = info["res_hist"][1:], o["res_hist"][1:]
+    assert np.allclose(hs, ho, rtol=5e-2)
+    assert abs(hs[-1] - ho[-1]) <= 1e-13
+
+
+def test_sstep_unrestarted_512_converges(cuda_device):
+    """512^2, eps_r = 4, one cycle of up to 4500 steps.  With the probe's
+    shifts alone the late blocks lost rank and the solve restarted seven times
+    without reaching 1e-10 in 12 000 steps; with refreshed shifts the first
+    cycle follows delayed CGS2 (3981 steps) and a second, shorter cycle
+    removes what the first one's rounding left (the s-step Hessenberg holds
+    its Arnoldi relation to about 1e-8 here)."""
+    N = 512
+    pr = P.helmholtz(N, 4.0, seed=0)
+    with cg.Solver(cuda_device) as s:
+        s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+        x, info = s.solve(pr["b"], restart=4500, max_iter=8000, tol=1e-10, ortho="sstep", sstep=4)
+        assert info["status"] == 0 and info["cycles"] <= 3, (info["status_text"], info["cycles"])
+        assert info["iterations"] <= 6500, info["iterations"]
+        r = pr["b"] - s.matvec(x)
+        assert np.linalg.norm(r) / np.linalg.norm(pr["b"]) <= 1.2e-10
