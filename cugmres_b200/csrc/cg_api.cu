@@ -302,7 +302,7 @@ int ensure_krylov(cg_ctx *c, int m, int maxit, size_t elem_bytes, int extra = 0)
         const size_t part_cgs2 = 2 * (size_t)dot_blocks(c) * (mc + 1);
         const size_t part_dcgs2 = 4 * (size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) *
                                   (size_t)dots2_part_ld(mc);
-        const size_t nss = (size_t)sstep_blocks(c->sms, n);  // most blocks of the s-step dot pass (its partial rows)
+        const size_t nss = (size_t)sstep_part_rows(c->sms);  // most blocks of the s-step dot pass (its partial rows)
         const size_t part_ss = nss * (size_t)sstep_part_ld(mc);
         CG_CU(cudaMalloc((void **)&c->kp.part, sizeof(double) * std::max(std::max(part_cgs2, part_dcgs2), part_ss)));
         const size_t ng2 = ((size_t)std::max(dots2_blocks(0, c->sms, mc, n), dots2_blocks(1, c->sms, mc, n)) + 15) / 16;

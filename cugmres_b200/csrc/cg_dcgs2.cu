@@ -1015,18 +1015,18 @@ typedef void (*DotsVecK)(const float4 *, long long, KrylovPtrs);
 typedef void (*AxpyVecK)(float4 *, long long, KrylovPtrs);
 static DotsVecK dots2_vec_kernel(int v, size_t smem) {
     DotsVecK kern = v == 11 ? k_dots2t<float4, 8> : k_dots2t<float4, 7>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_optin(kern, smem);
     return kern;
 }
 static AxpyVecK axpy2_vec_kernel(int v, size_t smem) {
     AxpyVecK kern = v == 9 ? k_axpy2t<float4, 4> : k_axpy2t<float4, 7>;
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_optin(kern, smem);
     return kern;
 }
 
 template <typename CV, bool COMP> static typename Dots2Table<CV, COMP>::K dots2_kernel(int v, size_t smem) {
     typename Dots2Table<CV, COMP>::K kern = Dots2Table<CV, COMP>::get(v);
-    if (smem > 48 * 1024) cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    smem_optin(kern, smem);
     return kern;
 }
 
@@ -1074,19 +1074,13 @@ int launch_dots2(int prec_v, const void *V, long long n, const KrylovPtrs &kp, i
 int launch_dcgs2_step(const KrylovPtrs &kp, cudaStream_t s) {
     const size_t smem = (size_t)(kp.mcap + 2) * sizeof(double2) + (size_t)(kp.mcap + 1) * sizeof(double2) +
                         (size_t)(kp.mcap + 1) * sizeof(double);
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(k_dcgs2_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return (int)e;
-    }
+    if (int e = smem_optin(k_dcgs2_step, smem)) return e;
     k_dcgs2_step<<<dim3(1, kp.nsys), STEP_THREADS, smem, s>>>(kp);
     return (int)cudaGetLastError();
 }
 
 template <typename CV> static int axpy2_prepare(int v, size_t smem) {
-    if (smem > 48 * 1024)
-        return (int)cudaFuncSetAttribute(Axpy2Table<CV>::get(v), cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
-    return 0;
+    return smem_optin(Axpy2Table<CV>::get(v), smem);
 }
 
 // Dynamic shared memory of the axpy-pass shapes: P, S coefficients, plus the

@@ -12,6 +12,19 @@ struct cg_ctx;  // solver context (cg_api.cu)
 
 namespace cg {
 
+// Opt `kern` in to `dyn` bytes of dynamic shared memory when its static shared
+// memory and `dyn` together pass the 48 KB that a launch may use without
+// opting in.  Comparing `dyn` alone let kernels with static arrays fail to
+// launch just below the threshold (the delayed-CGS2 step kernel, 6.4 KB
+// static, at restarts of about 1070 to 1230).
+template <typename K> inline int smem_optin(K kern, size_t dyn) {
+    cudaFuncAttributes a;
+    cudaError_t e = cudaFuncGetAttributes(&a, kern);
+    if (e != cudaSuccess) return (int)e;
+    if (a.sharedSizeBytes + dyn <= 48 * 1024) return 0;
+    return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+}
+
 // Solver state kept in device memory so that no host synchronisation is
 // needed per Arnoldi step (the reference copies Jtotal(i+1,0) to the host and
 // the residual back every iteration, CUDA_GMRES/GMRES.cuh:369-371).
@@ -196,6 +209,7 @@ int sstep_supported(int S);
 long long sstep_scratch_elems(int mcap);  // double2 entries of KrylovPtrs::ss
 int sstep_part_ld(int mcap);              // partials per block of the block dot pass
 int sstep_blocks(int sms, long long n);   // grid of the block dot and update passes
+int sstep_part_rows(int sms);              // partial rows of the dot pass, basis slices included
 int sstep_skipped(const KrylovPtrs &kp, int nblocks, std::vector<int> &flags, cudaStream_t s);
 int launch_ss_norm0(int prec, void *V, long long n, const KrylovPtrs &kp, cudaStream_t s);
 // block dots of pass `pass` (0 or 1); the last block also runs the pass's Cholesky.

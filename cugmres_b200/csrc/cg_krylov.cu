@@ -409,10 +409,7 @@ int launch_dots(int prec_v, const void *V, long long n, const KrylovPtrs &kp, Ve
     return (int)cudaGetLastError();
 }
 
-template <typename K> static int smem_attr(K kern, size_t smem) {
-    if (smem <= 48 * 1024) return 0;
-    return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-}
+template <typename K> static int smem_attr(K kern, size_t smem) { return smem_optin(kern, smem); }
 
 int launch_axpy(int prec_v, int prec_w, const void *V, long long n, const KrylovPtrs &kp, const double2 *src,
                 double sign, int nj_mode, VecSel w, int want_norm, int ctr, int nblk, int gate, cudaStream_t s) {

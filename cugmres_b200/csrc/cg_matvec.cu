@@ -653,13 +653,7 @@ k_cols_fft_full(double2 *__restrict__ A, const double2 *__restrict__ tw) {
 }
 
 // ---------------------------------------------------------------- launchers
-template <typename K> static int set_smem(K kern, size_t bytes) {
-    if (bytes > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-        if (e != cudaSuccess) return (int)e;
-    }
-    return 0;
-}
+template <typename K> static int set_smem(K kern, size_t bytes) { return smem_optin(kern, bytes); }
 
 // The three passes for one launch shape SH and one embedding size L.
 // The row passes do not depend on the column fields (COLT64, COLT32, PIPE):

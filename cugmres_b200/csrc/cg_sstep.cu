@@ -302,6 +302,11 @@ template <int S> __device__ __forceinline__ void ss_chol(const KrylovPtrs &kp, i
 // every warp keeps its tile of the S block vectors in registers and streams
 // the basis over it.  Per-block partial rows part[b][2 S (k+1) + 2 S S] are
 // summed in two fixed-order levels (groups of 16 blocks, then the groups).
+// On short vectors the grid's second dimension splits the basis: slice y of
+// gridDim.y takes the chunks of SS_CHUNK vectors with index = y mod gridDim.y
+// and writes zeros in its rows for the others; the Gram matrix comes from
+// slice 0.  (256^2: 256 tiles keep 32 blocks busy, each streaming the whole
+// basis; four slices give 128.)
 template <typename CV, int S, int U>
 __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV *__restrict__ V, long long n, KrylovPtrs kp,
                                                                        int pass) {
@@ -323,10 +328,16 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
     const long long ntile = (n + TILE - 1) / TILE;
     const long long nw = (long long)gridDim.x * SS_WARPS;
     for (int q = lane; q < 2 * S * S; q += 32) myg[q] = 0.0;
-    double *part = kp.part + (size_t)blockIdx.x * pld;
-    bool gram_done = false;
+    const int bflat = blockIdx.y * gridDim.x + blockIdx.x;
+    double *part = kp.part + (size_t)bflat * pld;
+    bool gram_done = blockIdx.y != 0;
     for (int jc = 0; jc < nq; jc += SS_CHUNK) {
         const int nj = nq - jc < SS_CHUNK ? nq - jc : SS_CHUNK;
+        if ((int)((jc / SS_CHUNK) % gridDim.y) != (int)blockIdx.y) {
+            // another slice's chunk (block-uniform): this block adds nothing to it
+            for (int q = threadIdx.x; q < nj * 2 * S; q += blockDim.x) part[2 * S * jc + q] = 0.0;
+            continue;
+        }
         for (int q = lane; q < nj * 2 * S; q += 32) my[q] = 0.0;
         __syncwarp();
         for (long long tile = (long long)blockIdx.x * SS_WARPS + warp; tile < ntile; tile += nw) {
@@ -417,8 +428,8 @@ __global__ void __launch_bounds__(SS_THREADS, ss_minb<CV>()) k_ss_dots(const CV 
     }
     // two-level fixed-order sum of the block rows
     const int nvals = 2 * S * nq + 2 * S * S;
-    const int nb = gridDim.x, ng = (nb + 15) / 16;
-    const int g = blockIdx.x / 16;
+    const int nb = gridDim.x * gridDim.y, ng = (nb + 15) / 16;
+    const int g = bflat / 16;
     const int gsz = nb - g * 16 < 16 ? nb - g * 16 : 16;
     if (!ss_last_of(&kp.tickets[g], (unsigned int)gsz)) return;
     for (int q = threadIdx.x; q < nvals; q += blockDim.x) {
@@ -797,8 +808,7 @@ template <typename CV> __global__ void k_ss_norm0(CV *__restrict__ V, long long 
 
 // ------------------------------------------------------------ launchers
 template <typename K> static int ss_smem(K kern, size_t bytes) {
-    if (bytes > 48 * 1024) return (int)cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-    return 0;
+    return smem_optin(kern, bytes);
 }
 
 static constexpr int SS_U32 = 8;  // tile width used to size the grid
@@ -817,24 +827,37 @@ static int ss_grid(long long ntile, int sms, int per_sm, int cap) {
     return (int)(g < 1 ? 1 : g);
 }
 
+// Basis slices of the dot pass (its grid's second dimension): as many as fill
+// `per_sm` blocks on every SM next to the `nblk` blocks that the tiles keep
+// busy, at most 8, within the partial rows of the buffer.
+static int ss_slices(int nblk, int sms, int per_sm, int rows) {
+    int y = (sms * per_sm) / nblk;
+    if (y > 8) y = 8;
+    while (y > 1 && (long long)y * nblk > rows) y--;
+    return y < 1 ? 1 : y;
+}
+
 template <int S> static int ss_dots_t(int prec, const void *V, long long n, const KrylovPtrs &kp, int sms, int pass,
                                       cudaStream_t s) {
     const size_t acc = sizeof(double) * ((size_t)SS_WARPS * SS_CHUNK * 2 * S + (size_t)SS_WARPS * 2 * S * S);
     const int cap = sstep_blocks(sms, n);
+    const int rows = sstep_part_rows(sms);
     if (prec == 0) {
         constexpr int U = ss_u64<S>();
         const size_t smem = acc + sizeof(double2) * (size_t)SS_WARPS * SS_NST * U * 32;
         auto kern = k_ss_dots<double2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
         const int nblk = ss_grid((n + 32 * U - 1) / (32 * U), sms, ss_minb<double2>(), cap);
-        kern<<<nblk, SS_THREADS, smem, s>>>((const double2 *)V, n, kp, pass);
+        const dim3 grid(nblk, ss_slices(nblk, sms, ss_minb<double2>(), rows));
+        kern<<<grid, SS_THREADS, smem, s>>>((const double2 *)V, n, kp, pass);
     } else {
         constexpr int U = ss_u32<S>();
         const size_t smem = acc + sizeof(float2) * (size_t)SS_WARPS * SS_NST * U * 32;
         auto kern = k_ss_dots<float2, S, U>;
         if (int e = ss_smem(kern, smem)) return e;
         const int nblk = ss_grid((n + 32 * U - 1) / (32 * U), sms, ss_minb<float2>(), cap);
-        kern<<<nblk, SS_THREADS, smem, s>>>((const float2 *)V, n, kp, pass);
+        const dim3 grid(nblk, ss_slices(nblk, sms, ss_minb<float2>(), rows));
+        kern<<<grid, SS_THREADS, smem, s>>>((const float2 *)V, n, kp, pass);
     }
     return (int)cudaGetLastError();
 }
@@ -872,6 +895,8 @@ template <int S> static int ss_hess_t(const KrylovPtrs &kp, int k, cudaStream_t 
         if (g > 1184) g = 1184;
         k_ss_hprod<S><<<g, SS_THREADS, 0, s>>>(kp);
     }
+    if (in_smem)
+        if (int e = smem_optin(k_ss_hess<S>, smem)) return e;
     k_ss_hess<S><<<1, SS_THREADS, in_smem ? smem : 0, s>>>(kp, in_smem ? 1 : 0, many ? 1 : 0);
     return (int)cudaGetLastError();
 }
@@ -885,6 +910,8 @@ template <int S> static int ss_hess_t(const KrylovPtrs &kp, int k, cudaStream_t 
     }
 
 int sstep_supported(int S) { return S == 2 || S == 4 || S == 8; }
+
+int sstep_part_rows(int sms) { return 2 * sms; }
 
 int sstep_blocks(int sms, long long n) {
     const long long tiles = (n + 32 * SS_U32 - 1) / (32 * SS_U32);
