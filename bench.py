@@ -266,8 +266,9 @@ def tight_reference(s, b, restart=2500, max_iter=5000):
 def side_measurements(args, stream):
     """Mixed precision on the same capped solve; time-to-1e-10 where GMRES
     converges: the 256^2 and 512^2 systems of the same construction
-    (unrestarted; mixed = complex64 cycles that end when their estimate fell by
-    1e-7, FP64 refinement); the config-3 grid (2048^2, eps_r = 12.25, restart
+    (unrestarted, by delayed CGS2 in FP64 and mixed precision, and by s-step
+    blocks of 4 in FP64; mixed = complex64 cycles that end when their estimate
+    fell by 1e-7, FP64 refinement); the config-3 grid (2048^2, eps_r = 12.25, restart
     50) within a budget of 1000 steps, FP64 and mixed."""
     import torch
     import cugmres_b200 as cg
