@@ -25,6 +25,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <cstddef>
 #include <vector>
 
 #include "../../include/cugmres.h"
@@ -1547,6 +1548,14 @@ int cugmres_solve(cg_ctx *c, const cg_c128 *b, cg_c128 *x, const cg_opts *opts_i
                 CG_CU(cudaMemcpyAsync(&sd, c->st, sizeof(DevState), cudaMemcpyDeviceToHost, s));
                 CG_CU(cudaStreamSynchronize(s));
                 if (sd.stop) break;
+                if (o.timeout_s > 0.0 && now_s() - t0 > o.timeout_s) {
+                    // end the cycle at the finished columns (nothing is in flight); the
+                    // check after the cycle then returns CG_ERR_TIMEOUT
+                    const int one = 1;
+                    CG_CU(cudaMemcpyAsync(reinterpret_cast<char *>(c->st) + offsetof(DevState, stop), &one, sizeof(int),
+                                          cudaMemcpyHostToDevice, s));
+                    break;
+                }
                 const int k = sd.k, W = std::min(SS_REFRESH_WINDOW, k);
                 if (W >= S) {
                     const int ld = c->mcap + 1;

@@ -204,3 +204,22 @@ def test_sstep_unrestarted_512_converges(cuda_device):
         assert info["iterations"] <= 6500, info["iterations"]
         r = pr["b"] - s.matvec(x)
         assert np.linalg.norm(r) / np.linalg.norm(pr["b"]) <= 1.2e-10
+
+
+def test_sstep_long_cycle_honours_the_timeout(cuda_device):
+    """A long s-step cycle checks the timeout between its 100-step segments:
+    512^2 with restart 4500 and an unreachable tolerance (a full cycle takes
+    several seconds) returns CG_ERR_TIMEOUT soon after 0.3 s, with the steps
+    finished so far applied to x."""
+    import time
+    N = 512
+    pr = P.helmholtz(N, 4.0, seed=0)
+    with cg.Solver(cuda_device) as s:
+        s.set_operator(pr["g_block"], pr["chi"], pr["chi_scale"])
+        s.solve(pr["b"], restart=4500, max_iter=200, tol=1e-30, ortho="sstep", sstep=4)  # allocation, tuning
+        t = time.perf_counter()
+        x, info = s.solve(pr["b"], restart=4500, max_iter=12000, tol=1e-30, ortho="sstep", sstep=4, timeout_s=0.3)
+        dt = time.perf_counter() - t
+        assert info["status"] == cg._lib.CG_ERR_TIMEOUT, info["status_text"]
+        assert dt < 1.5 and 0 < info["iterations"] < 4500, (dt, info["iterations"])
+        assert info["rel_residual_true"] < 0.5
